@@ -1,0 +1,264 @@
+/*
+ * cutcell_b200.h -- C ABI of libcutcell_b200.so, the sm_100a backend for the
+ * `update_cache!` hot path of CutCellMethods.jl (v0.3.0).
+ *
+ * Every entry point takes plain pointers and sizes. Cell columns, nodal phi,
+ * PLIC plane arrays and tree leaf arrays are DEVICE pointers owned by the
+ * caller (a Julia CuArray, a torch tensor): the library never frees them.
+ * The library owns only its own scratch (the marching-cubes tiling table,
+ * reduction partials, work lists), behind an opaque `cc_handle` that the
+ * caller creates at allocate_cache time and destroys in a finalizer.
+ *
+ * Memory layout written (the reference's StructArray of CutCellData, one
+ * plain array per field, column-major over grid.n with x fastest):
+ *   kind                int8  [ncell]
+ *   ambiguous           uint8 [ncell]          (Julia Bool)
+ *   volume_fraction     T     [ncell]
+ *   centroid            T     [D*ncell]        (D contiguous per cell)
+ *   face_fraction       T     [2D*ncell]       (-x,+x,-y,+y,-z,+z per cell)
+ *   face_centroid_local T     [2D*(D-1)*ncell] (per direction, in-plane axes
+ *                                               in increasing order)
+ *   interface_centroid  T     [D*ncell]
+ *   phi                 T     [prod(n+1)]      (nodal block, x fastest)
+ * (reference: src/cut_cell.jl:112-120, src/cache.jl:101-105,
+ *  src/marching_squares/cache.jl:41-47, src/marching_cubes/cache.jl:30-36)
+ *
+ * All update entry points are asynchronous on `stream` (a cudaStream_t, or
+ * NULL for the legacy default stream); the Julia/Python shims synchronize
+ * before returning, as the reference's update_cache! does
+ * (src/marching_squares/cache.jl:62).
+ */
+#ifndef CUTCELL_B200_H
+#define CUTCELL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------
+ * Mirrors the reference's host-side validation:
+ *   CC_DIM_MISMATCH      DimensionMismatch, src/cache.jl:107-121,
+ *                        src/marching_squares/cache.jl:140-147
+ *   CC_ANISOTROPIC       ArgumentError, src/plic/surface.jl:41-45
+ *   CC_BACKEND_MISMATCH  ArgumentError, src/marching_squares/cache.jl:119-121
+ */
+typedef enum {
+  CC_OK = 0,
+  CC_DIM_MISMATCH = 1,
+  CC_ANISOTROPIC = 2,
+  CC_BACKEND_MISMATCH = 3,
+  CC_BAD_TAPE = 4,
+  CC_DEVICE_TIMEOUT = 5,
+  CC_CUDA_ERR = 6,
+  CC_BAD_ARG = 7,
+  CC_BAD_TABLE = 8,
+  CC_NO_TABLE = 9,
+  CC_TOO_LARGE = 10
+} cc_status;
+
+/* Precision of a cache: the element type T of its columns. CC_MIXED stores
+ * Float32 columns and evaluates in Float32 with Float64 islands (edge roots of
+ * nearly equal corner values, the asymptotic face decider). */
+typedef enum { CC_F32 = 0, CC_F64 = 1, CC_MIXED = 2 } cc_prec;
+
+/* Methods (the reference's stateless method tags). */
+typedef enum {
+  CC_MARCHING_SQUARES = 0, /* src/marching_squares/marching_squares.jl:68 */
+  CC_MARCHING_CUBES = 1,   /* src/marching_cubes/marching_cubes.jl:53    */
+  CC_PLIC = 2              /* src/plic/plic.jl:30                         */
+} cc_method;
+
+/* A CartesianGrid{D}: origin x0, cell size d, cells per axis n. Node i (0-based)
+ * along axis a sits at  T(x0[a]) + T(i) * T(d[a])  with no FMA contraction
+ * (the get_node expression; the grid is narrowed to T once, as
+ * `convert(CartesianGrid{D,T}, grid)` at src/marching_squares/cache.jl:58). */
+typedef struct {
+  int32_t dim; /* 2 or 3 */
+  int32_t pad_;
+  double x0[3];
+  double d[3];
+  int64_t n[3]; /* cells per axis; n[2] = 1 in 2D */
+} cc_grid;
+
+/* Column pointers of a cache (device). Unused in a call may be NULL only
+ * where the entry point says so. */
+typedef struct {
+  int8_t* kind;
+  uint8_t* ambiguous;
+  void* volume_fraction;
+  void* centroid;
+  void* face_fraction;
+  void* face_centroid_local;
+  void* interface_centroid;
+} cc_cells;
+
+/* ---- the body: a CSG tree flattened to a postfix op-tape -----------------
+ * Each op evaluates a primitive at the sample point (or, for CC_OP_NONE,
+ * pops the stack) and combines the value into the stack:
+ *   PUSH  push v                MIN   top = (v < top) ? v : top
+ *   MAX   top = (v > top)? v:top   SMIN top = polynomial smooth-min(top, v, k)
+ *   SUB   top = max(top, -v)    NEG   top = -top (CC_OP_NONE only, no pop)
+ * Parameters are doubles in `params`, narrowed to the cache's T at launch.
+ * Stands in for SDFLibrary.jl's sdf_value/get_sdf (called at
+ * src/marching_squares/cache.jl:69, src/plic/plic.jl:74). */
+enum {
+  CC_OP_NONE = 0,   /* no primitive: pop v, then combine                    */
+  CC_OP_SPHERE = 1, /* D=3: cx cy cz r  | D=2 (circle): cx cy r           */
+  CC_OP_BOX = 2,    /* c[D] h[D] (half extents, axis aligned)              */
+  CC_OP_TORUS = 3,  /* D=3: c[3] R[9] (row major, local = R*(x-c)) Rmaj rmin */
+  CC_OP_PLANE = 4,  /* p[D] n[D]: dot(n, x - p)                            */
+  CC_OP_TRIG = 5,   /* a k[D] c: a * prod_i sin(k_i x_i) + c               */
+  CC_OP_CONST = 6,  /* v (SDFLibrary's EmptyGeo(v))                        */
+  CC_OP_STAR = 7,   /* D=2: cx cy r0 a[5] ph[5]: |x-c| - (r0 + sum_k a_k cos(k th + ph_k)), k=2..6 */
+  CC_OP_COUNT = 8
+};
+enum {
+  CC_COMB_PUSH = 0,
+  CC_COMB_MIN = 1,
+  CC_COMB_MAX = 2,
+  CC_COMB_SMIN = 3,
+  CC_COMB_SUB = 4,
+  CC_COMB_NEG = 5
+};
+#define CC_TAPE_MAX_OPS 256
+#define CC_TAPE_MAX_PARAMS 1024
+#define CC_TAPE_MAX_STACK 8
+
+typedef struct {
+  uint8_t opcode;  /* CC_OP_* */
+  uint8_t combine; /* CC_COMB_* */
+  uint16_t poff;   /* first parameter of the primitive */
+  uint16_t kparam; /* parameter index of k for CC_COMB_SMIN */
+  uint16_t reserved;
+} cc_op;
+
+typedef struct {
+  const cc_op* ops; /* host pointer */
+  int32_t n_ops;
+  int32_t n_params;
+  const double* params; /* host pointer */
+} cc_optape;
+
+/* ---- marching-cubes tiling table ------------------------------------------
+ * A flat, position-independent blob that encodes the per-cube Lewiner
+ * dispatch of src/marching_cubes/marching_cubes.jl:538-651: per lookup index
+ * (bit p set when corner p+1 is outside, src/marching_cubes/marching_cubes.jl:343-349)
+ * the case number, up to six signed face tests (the asymptotic decider,
+ * :401-406), one outcome per combination of test results, each naming an
+ * optional interior test (:427-504) and the tiling(s) it selects. The Julia
+ * shim encodes MarchingCubes.jl's own tables into it; the package can also
+ * generate a project-designed tiling in the same format.
+ *
+ *   header  : cc_mc_table_header
+ *   luts    : cc_mc_lut[256]
+ *   outcomes: cc_mc_outcome[n_outcomes]
+ *   tiles   : cc_mc_tile[n_tiles]
+ *   codes   : uint8_t[n_codes]   (edge codes 1..13, three per triangle)
+ */
+#define CC_MC_TABLE_MAGIC 0x544D4343u /* 'CCMT' */
+typedef struct {
+  uint32_t magic;
+  uint32_t version; /* 1 */
+  uint32_t n_outcomes;
+  uint32_t n_tiles;
+  uint32_t n_codes;
+  uint32_t total_bytes;
+} cc_mc_table_header;
+typedef struct {
+  uint8_t lcase;  /* MarchingCubes.cases[lut][1]: 1..15 */
+  uint8_t ntests; /* 0..6 face tests */
+  int8_t face[6]; /* signed face codes, MarchingCubes.jl face numbering */
+  uint16_t outcome_base;
+  uint16_t pad_;
+} cc_mc_lut;
+enum { CC_MC_INTERIOR_NONE = 0, CC_MC_INTERIOR_CASE4_10 = 1, CC_MC_INTERIOR_EDGE = 2 };
+typedef struct {
+  uint8_t itype; /* CC_MC_INTERIOR_* */
+  uint8_t edge;  /* 0-based reference edge for CC_MC_INTERIOR_EDGE */
+  int8_t s;      /* sign handed to the interior test */
+  uint8_t pad_;
+  uint16_t tile_true;  /* tiling when there is no interior test, or it holds */
+  uint16_t tile_false; /* tiling when the interior test fails */
+} cc_mc_outcome;
+typedef struct {
+  uint16_t code_off;
+  uint8_t ntris;
+  uint8_t pad_;
+} cc_mc_tile;
+
+/* ---- handle -------------------------------------------------------------- */
+typedef struct cc_handle cc_handle;
+
+/* Create the library-side state for one cache (the reference's
+ * allocate_cache, src/cache.jl:29). `n` is cells per axis. Allocates the
+ * handle's device scratch on `device`. */
+cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t prec,
+                           const int64_t n[3], cc_handle** out);
+cc_status cc_handle_destroy(cc_handle* h);
+/* Upload a marching-cubes tiling table blob (validated) into the handle. */
+cc_status cc_handle_set_mc_table(cc_handle* h, const void* blob, size_t nbytes);
+
+/* Marching cubes, fused: sample phi at every node from the op-tape and build
+ * every cell's CutCellData{3,T,6,2} (src/marching_cubes/cache.jl:38-39 ->
+ * src/marching_squares/cache.jl:55-78). phi is T[prod(n+1)]. */
+cc_status cc_mc_update(cc_handle* h, const cc_grid* g, const cc_optape* body, void* phi,
+                       const cc_cells* cells, void* stream);
+/* Marching cubes from a caller-supplied nodal field (the cell pass alone,
+ * src/marching_squares/cache.jl:75-78): phi is read, not written. */
+cc_status cc_mc_cells_from_phi(cc_handle* h, const cc_grid* g, const void* phi,
+                               const cc_cells* cells, void* stream);
+
+/* Marching squares on a CartesianGrid{2} (src/marching_squares/cache.jl:49-78). */
+cc_status cc_ms_update(cc_handle* h, const cc_grid* g, const cc_optape* body, void* phi,
+                       const cc_cells* cells, void* stream);
+cc_status cc_ms_cells_from_phi(cc_handle* h, const cc_grid* g, const void* phi,
+                               const cc_cells* cells, void* stream);
+
+/* Marching squares on the leaves of an AdaptiveMesh{2}
+ * (src/marching_squares/cache.jl:115-137). Leaf i has `level[i]` and integer
+ * coordinates (coord[2i], coord[2i+1]) at that level; its size is
+ * base_d / 2^level and its corners x0 + T(coord + bit) * h
+ * (src/marching_squares/marching_squares.jl:113-121). level/coord are device
+ * int32 arrays; phi4 is T[4*nleaves] (MS_NODE_BITS order per leaf). */
+typedef struct {
+  double x0[2];
+  double base_d[2];
+  int64_t nleaves;
+  const int32_t* level;
+  const int32_t* coord;
+} cc_tree;
+cc_status cc_ms_tree_update(cc_handle* h, const cc_tree* t, const cc_optape* body, void* phi4,
+                            const cc_cells* cells, void* stream);
+
+/* PLIC (src/plic/cache.jl:77-162): the fit pass writes normals (D*T per cell),
+ * intercepts, is_valid, volume_fraction and kind; the face pass writes the
+ * resolved face_fraction. centroid / face_centroid_local / interface_centroid
+ * / ambiguous are not touched (NaN / false from allocation). */
+cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body,
+                         const cc_cells* cells, void* normals, void* intercepts,
+                         uint8_t* is_valid, void* stream);
+
+/* calc_volume (src/volume.jl:29-40): sum over cells of the PLIC solid
+ * fraction times prod(d), accumulated on the device in compensated Float64.
+ * Blocking; writes the result to *out. */
+cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, double* out,
+                         void* stream);
+
+/* cut_cell_report (src/cut_cell.jl:302-319) over a cache's columns.
+ * Blocking. counts = {n, cut, inside, outside, ambiguous}. */
+cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8_t* ambiguous,
+                    const void* volume_fraction, int64_t counts[5],
+                    double* min_volume_fraction, void* stream);
+
+/* Library version string. */
+const char* cc_version(void);
+/* Last CUDA error text seen by the library on this thread ("" if none). */
+const char* cc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUTCELL_B200_H */

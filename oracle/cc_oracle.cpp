@@ -1,0 +1,1170 @@
+// =====================================================================================
+// cc_oracle.cpp -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+//
+// A CPU restatement of CutCellMethods.jl's `update_cache!` hot path (MarchingSquaresCutCell,
+// MarchingCubesCutCell, PLICCutCell, calc_volume), used only by tests/, by
+// __graft_entry__.smoke() and by bench.py's CPU baseline leg as the checker. Nothing in the
+// product links or calls it.
+//
+// Every construction follows the reference's expression order (StaticArrays left folds,
+// elementwise division, no FMA contraction: build with -ffp-contract=off -fno-fast-math), so
+// that a device kernel compiled with --fmad=false can be compared bit for bit.
+//
+// What this file cannot restate bit-exactly, because the code is absent from the reference
+// checkout (third-party packages pinned in Manifest.toml but not vendored):
+//   * SDFLibrary 0.10.5 `sdf_value` / `get_sdf`: replaced by the op-tape primitives defined in
+//     include/cutcell_b200.h, written from each body's mathematics. The PLIC normal is the
+//     forward-mode gradient of the same expression.
+//   * CartesianMeshes 0.2.3 `get_node` / `get_elem_centroid` / `get_volume_fraction`: node
+//     coordinates are taken as x0 + T(i)*d (0-based i), centroids as x0 + T(i + 0.5)*d, and the
+//     plane-cube clip is the analytic formula of Scardovelli & Zaleski (2000).
+//   * MarchingCubes.jl 0.1.11 Lewiner tables: the per-cube dispatch of
+//     src/marching_cubes/marching_cubes.jl:538-651 is restated here over a table blob passed in by
+//     the caller (the format of include/cutcell_b200.h); the tests pass a project-designed tiling.
+// Parity of these pieces against the reference is therefore "unpinned" here; everything else is
+// pinned against the reference tests' golden values (tests/test_oracle_*.py).
+// =====================================================================================
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+#include <algorithm>
+#include <thread>
+#include <atomic>
+#include "../include/cutcell_b200.h"
+
+namespace oc {
+
+// ----------------------------------------------------------------------------------
+// Host threading: a static split of [0, n) over std::threads (the toolchain here has no OpenMP
+// runtime). Each index is processed by exactly one thread and every output slot is written by
+// the index that owns it, so results do not depend on the thread count.
+static int g_threads = 1;
+template <class F>
+void parallel_for(int64_t n, F f) {
+  int nt = g_threads;
+  if (nt <= 1 || n < 2) { for (int64_t i = 0; i < n; ++i) f(i); return; }
+  if (nt > n) nt = int(n);
+  std::atomic<int64_t> next(0);
+  const int64_t chunk = std::max<int64_t>(1, n / (int64_t(nt) * 16));
+  auto work = [&]() {
+    for (;;) {
+      const int64_t b = next.fetch_add(chunk);
+      if (b >= n) break;
+      const int64_t e = std::min(n, b + chunk);
+      for (int64_t i = b; i < e; ++i) f(i);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& x : th) x.join();
+}
+
+// ----------------------------------------------------------------------------------
+// Forward-mode dual numbers: the value and its gradient in D coordinates.
+template <class T, int D>
+struct Dual {
+  T v;
+  T g[D];
+};
+template <class T> inline T val(T x) { return x; }
+template <class T, int D> inline T val(const Dual<T, D>& x) { return x.v; }
+
+template <class T, int D> inline Dual<T, D> dconst(T c) {
+  Dual<T, D> r; r.v = c; for (int i = 0; i < D; ++i) r.g[i] = T(0); return r;
+}
+template <class T, int D> inline Dual<T, D> operator+(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v + b.v; for (int i = 0; i < D; ++i) r.g[i] = a.g[i] + b.g[i]; return r;
+}
+template <class T, int D> inline Dual<T, D> operator-(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v - b.v; for (int i = 0; i < D; ++i) r.g[i] = a.g[i] - b.g[i]; return r;
+}
+template <class T, int D> inline Dual<T, D> operator-(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = -a.v; for (int i = 0; i < D; ++i) r.g[i] = -a.g[i]; return r;
+}
+template <class T, int D> inline Dual<T, D> operator*(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v * b.v;
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+  return r;
+}
+template <class T, int D> inline Dual<T, D> operator/(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v / b.v;
+  const T bb = b.v * b.v;
+  for (int i = 0; i < D; ++i) r.g[i] = (a.g[i] * b.v - a.v * b.g[i]) / bb;
+  return r;
+}
+template <class T, int D> inline Dual<T, D> operator+(const Dual<T, D>& a, T c) { Dual<T, D> r = a; r.v = a.v + c; return r; }
+template <class T, int D> inline Dual<T, D> operator-(const Dual<T, D>& a, T c) { Dual<T, D> r = a; r.v = a.v - c; return r; }
+template <class T, int D> inline Dual<T, D> operator-(T c, const Dual<T, D>& a) { Dual<T, D> r = -a; r.v = c - a.v; return r; }
+template <class T, int D> inline Dual<T, D> operator*(T c, const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = c * a.v; for (int i = 0; i < D; ++i) r.g[i] = c * a.g[i]; return r;
+}
+template <class T, int D> inline Dual<T, D> operator*(const Dual<T, D>& a, T c) {
+  Dual<T, D> r; r.v = a.v * c; for (int i = 0; i < D; ++i) r.g[i] = a.g[i] * c; return r;
+}
+template <class T, int D> inline Dual<T, D> operator/(const Dual<T, D>& a, T c) {
+  Dual<T, D> r; r.v = a.v / c; for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / c; return r;
+}
+template <class T, int D> inline Dual<T, D> dsqrt(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = std::sqrt(a.v);
+  const T two_s = T(2) * r.v;
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / two_s;
+  return r;
+}
+template <class T, int D> inline Dual<T, D> dabs(const Dual<T, D>& a) {
+  // sign(0) == 0, so the gradient of |x| at x == 0 is zero.
+  const T sg = a.v > T(0) ? T(1) : (a.v < T(0) ? T(-1) : T(0));
+  Dual<T, D> r; r.v = std::fabs(a.v); for (int i = 0; i < D; ++i) r.g[i] = sg * a.g[i]; return r;
+}
+template <class T, int D> inline Dual<T, D> dsin(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = std::sin(a.v); const T c = std::cos(a.v);
+  for (int i = 0; i < D; ++i) r.g[i] = c * a.g[i];
+  return r;
+}
+template <class T, int D> inline Dual<T, D> dcos(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = std::cos(a.v); const T s = -std::sin(a.v);
+  for (int i = 0; i < D; ++i) r.g[i] = s * a.g[i];
+  return r;
+}
+template <class T, int D> inline Dual<T, D> datan2(const Dual<T, D>& y, const Dual<T, D>& x) {
+  Dual<T, D> r; r.v = std::atan2(y.v, x.v);
+  const T den = x.v * x.v + y.v * y.v;
+  for (int i = 0; i < D; ++i) r.g[i] = (x.v * y.g[i] - y.v * x.g[i]) / den;
+  return r;
+}
+// scalar overloads so one template serves T and Dual<T,D>
+template <class T> inline T dsqrt(T a) { return std::sqrt(a); }
+template <class T> inline T dabs(T a) { return std::fabs(a); }
+template <class T> inline T dsin(T a) { return std::sin(a); }
+template <class T> inline T dcos(T a) { return std::cos(a); }
+template <class T> inline T datan2(T y, T x) { return std::atan2(y, x); }
+
+template <class S> struct Lift;  // constant of the evaluation type
+template <> struct Lift<float> { static float c(float x) { return x; } };
+template <> struct Lift<double> { static double c(double x) { return x; } };
+template <class T, int D> struct Lift<Dual<T, D>> { static Dual<T, D> c(T x) { return dconst<T, D>(x); } };
+
+// ----------------------------------------------------------------------------------
+// The op-tape: SDF primitives and CSG combinators (include/cutcell_b200.h). Stands in for
+// SDFLibrary.jl's `sdf_value` (src/marching_squares/cache.jl:69) and `get_sdf`
+// (src/plic/plic.jl:74).
+template <class T>
+struct Tape {
+  std::vector<cc_op> ops;
+  std::vector<T> p;
+};
+
+template <class T, int D, class S>
+inline S prim(const cc_op& op, const T* p, const S* x) {
+  switch (op.opcode) {
+    case CC_OP_SPHERE: {
+      const T* c = p + op.poff;
+      S u = (x[0] - c[0]) * (x[0] - c[0]);
+      for (int a = 1; a < D; ++a) u = u + (x[a] - c[a]) * (x[a] - c[a]);
+      return dsqrt(u) - c[D];
+    }
+    case CC_OP_BOX: {
+      const T* c = p + op.poff;
+      const T* h = c + D;
+      S q[D];
+      for (int a = 0; a < D; ++a) q[a] = dabs(x[a] - c[a]) - h[a];
+      // outside part: |max(q, 0)|
+      S zero = Lift<S>::c(T(0));
+      S qp0 = val(q[0]) > T(0) ? q[0] : zero;
+      S u = qp0 * qp0;
+      for (int a = 1; a < D; ++a) { S qa = val(q[a]) > T(0) ? q[a] : zero; u = u + qa * qa; }
+      S outside = dsqrt(u);
+      // inside part: min(max_a q_a, 0)
+      S m = q[0];
+      for (int a = 1; a < D; ++a) m = val(q[a]) > val(m) ? q[a] : m;
+      S inside = val(m) < T(0) ? m : zero;
+      return outside + inside;
+    }
+    case CC_OP_TORUS: if constexpr (D == 3) {
+      const T* c = p + op.poff;
+      const T* R = c + 3;
+      S d0 = x[0] - c[0], d1 = x[1] - c[1], d2 = x[2] - c[2];
+      S l0 = R[0] * d0 + R[1] * d1 + R[2] * d2;
+      S l1 = R[3] * d0 + R[4] * d1 + R[5] * d2;
+      S l2 = R[6] * d0 + R[7] * d1 + R[8] * d2;
+      S qx = dsqrt(l0 * l0 + l1 * l1) - c[12];
+      return dsqrt(qx * qx + l2 * l2) - c[13];
+    } else { return Lift<S>::c(std::numeric_limits<T>::quiet_NaN()); }
+    case CC_OP_PLANE: {
+      const T* pt = p + op.poff;
+      const T* n = pt + D;
+      S s = n[0] * (x[0] - pt[0]);
+      for (int a = 1; a < D; ++a) s = s + n[a] * (x[a] - pt[a]);
+      return s;
+    }
+    case CC_OP_TRIG: {
+      const T* q = p + op.poff;
+      S s = q[0] * dsin(q[1] * x[0]);
+      for (int a = 1; a < D; ++a) s = s * dsin(q[1 + a] * x[a]);
+      return s + q[1 + D];
+    }
+    case CC_OP_CONST:
+      return Lift<S>::c(p[op.poff]);
+    case CC_OP_STAR: if constexpr (D == 2) {
+      const T* q = p + op.poff;
+      S dx = x[0] - q[0], dy = x[1] - q[1];
+      S rad = dsqrt(dx * dx + dy * dy);
+      S th = datan2(dy, dx);
+      S r = Lift<S>::c(q[2]);
+      for (int k = 2; k <= 6; ++k) r = r + q[3 + (k - 2)] * dcos(T(k) * th + q[8 + (k - 2)]);
+      return rad - r;
+    } else { return Lift<S>::c(std::numeric_limits<T>::quiet_NaN()); }
+    default:
+      return Lift<S>::c(std::numeric_limits<T>::quiet_NaN());
+  }
+}
+
+template <class T, class S>
+inline S combine(int mode, const S& top, const S& v, T k) {
+  switch (mode) {
+    case CC_COMB_MIN: return val(v) < val(top) ? v : top;
+    case CC_COMB_MAX: return val(v) > val(top) ? v : top;
+    case CC_COMB_SUB: { S w = -v; return val(w) > val(top) ? w : top; }
+    case CC_COMB_SMIN: {
+      // polynomial smooth minimum: min(a,b) - h^2 k / 4, h = max(k - |a-b|, 0) / k
+      S ad = dabs(top - v);
+      S hk = k - ad;
+      S zero = Lift<S>::c(T(0));
+      S h = (val(hk) > T(0) ? hk : zero) / k;
+      S m = val(v) < val(top) ? v : top;
+      return m - ((h * h) * k) * T(0.25);
+    }
+    default: return v;
+  }
+}
+
+template <class T, int D, class S>
+inline S eval_tape(const Tape<T>& t, const S* x) {
+  S st[CC_TAPE_MAX_STACK];
+  int sp = 0;
+  for (size_t i = 0; i < t.ops.size(); ++i) {
+    const cc_op& op = t.ops[i];
+    S v;
+    if (op.opcode == CC_OP_NONE) {
+      if (op.combine == CC_COMB_NEG) { st[sp - 1] = -st[sp - 1]; continue; }
+      v = st[--sp];
+    } else {
+      v = prim<T, D, S>(op, t.p.data(), x);
+    }
+    if (op.combine == CC_COMB_PUSH) st[sp++] = v;
+    else st[sp - 1] = combine<T, S>(op.combine, st[sp - 1], v, op.combine == CC_COMB_SMIN ? t.p[op.kparam] : T(0));
+  }
+  return st[0];
+}
+
+// ----------------------------------------------------------------------------------
+// CartesianMeshes stand-ins.
+template <class T> inline T node_coord(T x0, T d, int64_t i) { return x0 + T(i) * d; }
+template <class T> inline T centroid_coord(T x0, T d, int64_t i) { return x0 + T(double(i) + 0.5) * d; }
+
+// Solid fraction of the unit square {n . xi <= a}, Scardovelli & Zaleski (2000), 2D form.
+template <class T>
+inline T gvf2(T n1, T n2, T a) {
+  T m1 = std::fabs(n1), m2 = std::fabs(n2);
+  T alpha = a;
+  if (n1 < T(0)) alpha = alpha + m1;
+  if (n2 < T(0)) alpha = alpha + m2;
+  const T s = m1 + m2;
+  if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  m1 = m1 / s; m2 = m2 / s; alpha = alpha / s;
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= T(1)) return T(1);
+  const bool flip = alpha > T(0.5);
+  if (flip) alpha = T(1) - alpha;
+  if (m1 > m2) std::swap(m1, m2);
+  T v;
+  if (alpha < m1) v = (alpha * alpha) / (T(2) * m1 * m2);
+  else v = (alpha - T(0.5) * m1) / m2;
+  return flip ? T(1) - v : v;
+}
+
+// Solid fraction of the unit cube {n . xi <= a}, Scardovelli & Zaleski (2000).
+template <class T>
+inline T gvf3(T n1, T n2, T n3, T a) {
+  T m[3] = {std::fabs(n1), std::fabs(n2), std::fabs(n3)};
+  T alpha = a;
+  if (n1 < T(0)) alpha = alpha + m[0];
+  if (n2 < T(0)) alpha = alpha + m[1];
+  if (n3 < T(0)) alpha = alpha + m[2];
+  const T s = (m[0] + m[1]) + m[2];
+  if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  m[0] = m[0] / s; m[1] = m[1] / s; m[2] = m[2] / s; alpha = alpha / s;
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= T(1)) return T(1);
+  const bool flip = alpha > T(0.5);
+  if (flip) alpha = T(1) - alpha;
+  if (m[0] > m[1]) std::swap(m[0], m[1]);
+  if (m[1] > m[2]) std::swap(m[1], m[2]);
+  if (m[0] > m[1]) std::swap(m[0], m[1]);
+  const T m1 = m[0], m2 = m[1], m3 = m[2];
+  const T m12 = m1 + m2;
+  T v;
+  // alpha^3 - (alpha - m1)^3 is expanded as m1 * (3 alpha^2 - 3 alpha m1 + m1^2) so that no branch
+  // divides a cancelling difference by a small m1; the remaining cubes (alpha - m2)^3 and
+  // (alpha - m3)^3 are below m1^3 wherever they appear.
+  if (alpha < m1) {
+    v = (alpha * alpha * alpha) / (T(6) * m1 * m2 * m3);
+  } else {
+    const T core = (T(3) * alpha * alpha - T(3) * alpha * m1 + m1 * m1) / (T(6) * m2 * m3);
+    if (alpha < m2) {
+      v = core;
+    } else if (alpha < std::min(m12, m3)) {
+      const T u = alpha - m2;
+      v = core - (u * u * u) / (T(6) * m1 * m2 * m3);
+    } else if (m3 < m12) {
+      const T u = alpha - m2, w = alpha - m3;
+      v = core - (u * u * u + w * w * w) / (T(6) * m1 * m2 * m3);
+    } else {
+      v = (T(2) * alpha - m12) / (T(2) * m3);
+    }
+  }
+  return flip ? T(1) - v : v;
+}
+
+// ----------------------------------------------------------------------------------
+// Marching squares (src/marching_squares/marching_squares.jl, src/marching_squares/moments.jl).
+// Edges 0..3 of the counter-clockwise walk; 0-based forms of MS_EDGE_DIRECTION /
+// MS_DIRECTION_EDGE (marching_squares.jl:81-82).
+static const int MS_DIRECTION_EDGE0[4] = {3, 1, 0, 2};
+inline int ms_next(int k) { return (k + 1) & 3; }
+inline int ms_prev(int k) { return (k + 3) & 3; }
+
+// _open_fraction, marching_squares.jl:192-198
+template <class T>
+inline T open_fraction(T pa, T pb) {
+  const bool fa = pa >= T(0), fb = pb >= T(0);
+  if (fa && fb) return T(1);
+  if (!fa && !fb) return T(0);
+  return fa ? pa / (pa - pb) : pb / (pb - pa);
+}
+
+// _open_segment, marching_squares.jl:208-217
+template <class T>
+inline void open_segment(const T* pa, const T* pb, T fa, T fb, T frac, T* a, T* b) {
+  if (fa >= T(0) && fb >= T(0)) {
+    a[0] = pa[0]; a[1] = pa[1]; b[0] = pb[0]; b[1] = pb[1];
+  } else if (fa >= T(0)) {
+    a[0] = pa[0]; a[1] = pa[1];
+    b[0] = pa[0] + frac * (pb[0] - pa[0]);
+    b[1] = pa[1] + frac * (pb[1] - pa[1]);
+  } else {
+    a[0] = pb[0] + frac * (pa[0] - pb[0]);
+    a[1] = pb[1] + frac * (pa[1] - pb[1]);
+    b[0] = pb[0]; b[1] = pb[1];
+  }
+}
+
+// cell_boundary_walk, marching_squares.jl:240-251
+template <class T>
+struct Walk {
+  T fracs[4];
+  bool present[4];
+  T sa[4][2];
+  T sb[4][2];
+};
+template <class T>
+inline void boundary_walk(const T nodes[4][2], const T phi[4], Walk<T>& w) {
+  for (int k = 0; k < 4; ++k) w.fracs[k] = open_fraction(phi[k], phi[ms_next(k)]);
+  for (int k = 0; k < 4; ++k) w.present[k] = phi[k] >= T(0) || phi[ms_next(k)] >= T(0);
+  for (int k = 0; k < 4; ++k)
+    open_segment(nodes[k], nodes[ms_next(k)], phi[k], phi[ms_next(k)], w.fracs[k], w.sa[k], w.sb[k]);
+}
+
+// _next_present, marching_squares.jl:255-264
+inline int next_present(const bool present[4], int k) {
+  int j = ms_next(k);
+  if (present[j]) return j;
+  j = ms_next(j);
+  if (present[j]) return j;
+  j = ms_next(j);
+  if (present[j]) return j;
+  return k;
+}
+
+// cell_gap_segments, marching_squares.jl:291-317
+template <class T>
+inline int gap_segments(const Walk<T>& w, T ia[2][2], T ib[2][2]) {
+  int n = 0;
+  ia[0][0] = ia[0][1] = ia[1][0] = ia[1][1] = T(0);
+  ib[0][0] = ib[0][1] = ib[1][0] = ib[1][1] = T(0);
+  for (int k = 0; k < 4; ++k) {
+    if (!w.present[k]) continue;
+    const int j = next_present(w.present, k);
+    const T* a = w.sb[k];
+    const T* b = w.sa[j];
+    if (a[0] != b[0] || a[1] != b[1]) {
+      ++n;
+      if (n == 1) { ia[0][0] = a[0]; ia[0][1] = a[1]; ib[0][0] = b[0]; ib[0][1] = b[1]; }
+      else if (n == 2) { ia[1][0] = a[0]; ia[1][1] = a[1]; ib[1][0] = b[0]; ib[1][1] = b[1]; }
+    }
+  }
+  return std::min(n, 2);
+}
+
+template <class T, int D>
+struct CellOut {
+  int8_t kind;
+  uint8_t amb;
+  T vf;
+  T c[D];
+  T ff[2 * D];
+  T fcl[2 * D * (D - 1)];
+  T ic[D];
+};
+
+// cut_cell_moments (2D), src/marching_squares/moments.jl:66-164
+template <class T>
+inline void ms_moments(const T nodes[4][2], const T phi[4], const T cs[2], CellOut<T, 2>& o) {
+  const T* origin = nodes[0];
+  const T centre[2] = {origin[0] + T(0.5) * cs[0], origin[1] + T(0.5) * cs[1]};
+  const T vol_cell = cs[0] * cs[1];
+  int noutside = 0;
+  for (int k = 0; k < 4; ++k) noutside += phi[k] >= T(0) ? 1 : 0;
+
+  auto full_face_centre = [&](int dir, T* x) {  // moments.jl:39-42
+    const int k = MS_DIRECTION_EDGE0[dir];
+    x[0] = T(0.5) * (nodes[k][0] + nodes[ms_next(k)][0]);
+    x[1] = T(0.5) * (nodes[k][1] + nodes[ms_next(k)][1]);
+  };
+  auto face_offset = [&](const T* x, int dir) -> T {  // moments.jl:48-51
+    const int p = dir < 2 ? 1 : 0;  // 3 - direction_axis(dir), 0-based
+    return x[p] - origin[p];
+  };
+
+  if (noutside == 4 || noutside == 0) {  // moments.jl:84-93
+    const bool outside = noutside == 4;
+    o.kind = outside ? 1 : 0;
+    o.amb = 0;
+    o.vf = outside ? T(1) : T(0);
+    o.c[0] = centre[0]; o.c[1] = centre[1];
+    for (int dir = 0; dir < 4; ++dir) {
+      o.ff[dir] = outside ? T(1) : T(0);
+      T x[2]; full_face_centre(dir, x);
+      o.fcl[dir] = face_offset(x, dir);
+    }
+    o.ic[0] = centre[0]; o.ic[1] = centre[1];
+    return;
+  }
+  Walk<T> w;
+  boundary_walk(nodes, phi, w);
+  for (int dir = 0; dir < 4; ++dir) {
+    const int k = MS_DIRECTION_EDGE0[dir];
+    o.ff[dir] = w.fracs[k];
+    T x[2];
+    if (w.present[k]) { x[0] = T(0.5) * (w.sa[k][0] + w.sb[k][0]); x[1] = T(0.5) * (w.sa[k][1] + w.sb[k][1]); }
+    else full_face_centre(dir, x);
+    o.fcl[dir] = face_offset(x, dir);
+  }
+  T area2 = T(0), cm0 = T(0), cm1 = T(0);
+  for (int k = 0; k < 4; ++k) {
+    if (!w.present[k]) continue;
+    const T la0 = w.sa[k][0] - origin[0], la1 = w.sa[k][1] - origin[1];
+    const T lb0 = w.sb[k][0] - origin[0], lb1 = w.sb[k][1] - origin[1];
+    const T cr = la0 * lb1 - la1 * lb0;
+    area2 = area2 + cr;
+    cm0 = cm0 + (la0 + lb0) * cr;
+    cm1 = cm1 + (la1 + lb1) * cr;
+  }
+  T ia[2][2], ib[2][2];
+  const int nint = gap_segments(w, ia, ib);
+  T ilen = T(0), icm0 = T(0), icm1 = T(0);
+  for (int s = 0; s < nint; ++s) {
+    const T* a = ia[s];
+    const T* b = ib[s];
+    const T la0 = a[0] - origin[0], la1 = a[1] - origin[1];
+    const T lb0 = b[0] - origin[0], lb1 = b[1] - origin[1];
+    const T cr = la0 * lb1 - la1 * lb0;
+    area2 = area2 + cr;
+    cm0 = cm0 + (la0 + lb0) * cr;
+    cm1 = cm1 + (la1 + lb1) * cr;
+    const T v0 = b[0] - a[0], v1 = b[1] - a[1];
+    const T len = std::sqrt(v0 * v0 + v1 * v1);
+    ilen = ilen + len;
+    const T hl = T(0.5) * len;
+    icm0 = icm0 + hl * (a[0] + b[0]);
+    icm1 = icm1 + hl * (a[1] + b[1]);
+  }
+  const T area = T(0.5) * area2;
+  o.kind = 2;
+  o.amb = nint > 1 ? 1 : 0;
+  o.vf = area / vol_cell;
+  if (area2 != T(0)) {
+    const T den = T(3) * area2;
+    o.c[0] = origin[0] + cm0 / den;
+    o.c[1] = origin[1] + cm1 / den;
+  } else { o.c[0] = centre[0]; o.c[1] = centre[1]; }
+  if (ilen > T(0)) { o.ic[0] = icm0 / ilen; o.ic[1] = icm1 / ilen; }
+  else { o.ic[0] = centre[0]; o.ic[1] = centre[1]; }
+}
+
+// ----------------------------------------------------------------------------------
+// Marching cubes (src/marching_cubes/marching_cubes.jl, src/marching_cubes/moments.jl).
+// MC_NODE_BITS :106-107, MC_EDGE_NODES :135-137 (1-based node pairs),
+// MC_TEST_FACE_QUADS :372-373.
+static const int MC_BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                  {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+static const int MC_EDGE_NODES1[12][2] = {{1, 2}, {2, 3}, {4, 3}, {1, 4}, {5, 6}, {6, 7},
+                                          {8, 7}, {5, 8}, {1, 5}, {2, 6}, {3, 7}, {4, 8}};
+static const int MC_TEST_FACE_QUADS1[6][4] = {{1, 5, 6, 2}, {2, 6, 7, 3}, {3, 7, 8, 4},
+                                              {4, 8, 5, 1}, {1, 4, 3, 2}, {5, 8, 7, 6}};
+// Derived once, as the reference derives them (:146-180, :385-388).
+struct McConst {
+  int face_axes[6][2];  // 0-based in-plane axes (p, q)
+  int face_nodes[6][4]; // 0-based corner indices
+  int face_test_code[6];
+  McConst() {
+    for (int dir = 0; dir < 6; ++dir) {
+      const int ax = dir >> 1;
+      int pq[2], np = 0;
+      for (int a = 0; a < 3; ++a) if (a != ax) pq[np++] = a;
+      face_axes[dir][0] = pq[0]; face_axes[dir][1] = pq[1];
+      const int bax = (dir & 1) ? 1 : 0;
+      static const int MSB[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+      for (int k = 0; k < 4; ++k) {
+        int bits[3];
+        for (int a = 0; a < 3; ++a) bits[a] = a == ax ? bax : (a == pq[0] ? MSB[k][0] : MSB[k][1]);
+        for (int c = 0; c < 8; ++c)
+          if (MC_BITS[c][0] == bits[0] && MC_BITS[c][1] == bits[1] && MC_BITS[c][2] == bits[2]) face_nodes[dir][k] = c;
+      }
+      for (int f = 0; f < 6; ++f) {
+        int hit = 0;
+        for (int k = 0; k < 4; ++k)
+          for (int l = 0; l < 4; ++l) hit += (MC_TEST_FACE_QUADS1[f][l] - 1) == face_nodes[dir][k];
+        if (hit == 4) face_test_code[dir] = f + 1;
+      }
+    }
+  }
+};
+static const McConst MCC;
+
+// nudge_zeros, marching_cubes.jl:240-243
+template <class T> inline T nudge(T v) {
+  const T e = std::numeric_limits<T>::epsilon();
+  return std::fabs(v) < e ? e : v;
+}
+
+// _test_face, marching_cubes.jl:401-406
+template <class T>
+inline bool test_face(const T* cb, int face) {
+  const int* q = MC_TEST_FACE_QUADS1[std::abs(face) - 1];
+  const T A = cb[q[0] - 1], B = cb[q[1] - 1], C = cb[q[2] - 1], D = cb[q[3] - 1];
+  const T det = A * C - B * D;
+  if (std::fabs(det) < std::numeric_limits<T>::epsilon()) return face >= 0;
+  return (T(face) * A) * det >= T(0);
+}
+
+// _test_interior, marching_cubes.jl:427-504. Reference edges 0..11 as
+// (t numerator corner, t other corner, B pair, C pair, D pair), 1-based corners, restating the
+// twelve branches of :450-486.
+static const int MC_INTERIOR_EDGE1[12][8] = {
+    {1, 2, 4, 3, 8, 7, 5, 6}, {2, 3, 1, 4, 5, 8, 6, 7}, {3, 4, 2, 1, 6, 5, 7, 8},
+    {4, 1, 3, 2, 7, 6, 8, 5}, {5, 6, 8, 7, 4, 3, 1, 2}, {6, 7, 5, 8, 1, 4, 2, 3},
+    {7, 8, 6, 5, 2, 1, 3, 4}, {8, 5, 7, 6, 3, 2, 4, 1}, {1, 5, 4, 8, 3, 7, 2, 6},
+    {2, 6, 1, 5, 4, 8, 3, 7}, {3, 7, 2, 6, 1, 5, 4, 8}, {4, 8, 3, 7, 2, 6, 1, 5}};
+template <class T>
+inline bool test_interior(int itype, int edge, const T* cb, int s) {
+  T At = T(0), Bt = T(0), Ct = T(0), Dt = T(0);
+  auto c = [&](int i) { return cb[i - 1]; };
+  if (itype == CC_MC_INTERIOR_CASE4_10) {
+    const T a = (c(5) - c(1)) * (c(7) - c(3)) - (c(8) - c(4)) * (c(6) - c(2));
+    const T b = ((c(3) * (c(5) - c(1)) + c(1) * (c(7) - c(3))) - c(2) * (c(8) - c(4))) - c(4) * (c(6) - c(2));
+    const T t = -b / (T(2) * a);
+    if (t < T(0) || t > T(1)) return s > 0;
+    At = c(1) + (c(5) - c(1)) * t;
+    Bt = c(4) + (c(8) - c(4)) * t;
+    Ct = c(3) + (c(7) - c(3)) * t;
+    Dt = c(2) + (c(6) - c(2)) * t;
+  } else {
+    const int* e = MC_INTERIOR_EDGE1[edge];
+    const T t = c(e[0]) / (c(e[0]) - c(e[1]));
+    Bt = c(e[2]) + (c(e[3]) - c(e[2])) * t;
+    Ct = c(e[4]) + (c(e[5]) - c(e[4])) * t;
+    Dt = c(e[6]) + (c(e[7]) - c(e[6])) * t;
+  }
+  int test = 0;
+  if (At >= T(0)) test += 1;
+  if (Bt >= T(0)) test += 2;
+  if (Ct >= T(0)) test += 4;
+  if (Dt >= T(0)) test += 8;
+  const T eps = std::numeric_limits<T>::epsilon();
+  if (test == 6 || test == 8 || test == 9 || test == 12 || (test >= 0 && test <= 4)) return s > 0;
+  if (test == 5) return (At * Ct - Bt * Dt < eps) ? s > 0 : s < 0;
+  if (test == 10) return (At * Ct - Bt * Dt >= eps) ? s > 0 : s < 0;
+  return s < 0;
+}
+
+struct McTable {
+  const cc_mc_table_header* h = nullptr;
+  const cc_mc_lut* luts = nullptr;
+  const cc_mc_outcome* outs = nullptr;
+  const cc_mc_tile* tiles = nullptr;
+  const uint8_t* codes = nullptr;
+  bool parse(const uint8_t* blob) {
+    h = reinterpret_cast<const cc_mc_table_header*>(blob);
+    if (h->magic != CC_MC_TABLE_MAGIC) return false;
+    luts = reinterpret_cast<const cc_mc_lut*>(blob + sizeof(cc_mc_table_header));
+    outs = reinterpret_cast<const cc_mc_outcome*>(luts + 256);
+    tiles = reinterpret_cast<const cc_mc_tile*>(outs + h->n_outcomes);
+    codes = reinterpret_cast<const uint8_t*>(tiles + h->n_tiles);
+    return true;
+  }
+};
+
+// cell_case, marching_cubes.jl:343-349 (returned 0-based: lut - 1)
+template <class T> inline int cell_case0(const T* phi) {
+  int lut = 0;
+  for (int p = 0; p < 8; ++p) if (phi[p] >= T(0)) lut |= 1 << p;
+  return lut;
+}
+
+// cell_triangles, marching_cubes.jl:538-651, over the table blob: the face tests, then the
+// optional interior test, pick one tiling. Returns the triangle count and the tile's codes.
+template <class T>
+inline int cell_triangles(const McTable& tb, const T* phi, const uint8_t** codes, int* lcase) {
+  const int lut = cell_case0(phi);
+  const cc_mc_lut& e = tb.luts[lut];
+  *lcase = e.lcase;
+  int o = 0;
+  for (int i = 0; i < e.ntests; ++i) if (test_face(phi, e.face[i])) o |= 1 << i;
+  const cc_mc_outcome& oc = tb.outs[e.outcome_base + o];
+  int tile = oc.tile_true;
+  if (oc.itype != CC_MC_INTERIOR_NONE && !test_interior(oc.itype, oc.edge, phi, oc.s)) tile = oc.tile_false;
+  *codes = tb.codes + tb.tiles[tile].code_off;
+  return tb.tiles[tile].ntris;
+}
+
+// _chord_target, moments.jl:91-98 (returns -1 for none)
+template <class T>
+inline int chord_target(const T* fphi, int k, bool forward) {
+  int j = k;
+  for (int it = 0; it < 4; ++it) {
+    j = forward ? ms_next(j) : ms_prev(j);
+    if (fphi[j] < T(0) && fphi[ms_next(j)] >= T(0)) return j;
+  }
+  return -1;
+}
+
+// _face_polygon, moments.jl:111-139
+template <class T>
+inline void face_polygon(const T fn[4][2], const T* fphi, bool connect, T& area2, T& c0, T& c1) {
+  Walk<T> w;
+  boundary_walk(fn, fphi, w);
+  area2 = T(0); c0 = T(0); c1 = T(0);
+  for (int k = 0; k < 4; ++k) {
+    if (!w.present[k]) continue;
+    const T* la = w.sa[k]; const T* lb = w.sb[k];
+    const T cr = la[0] * lb[1] - la[1] * lb[0];
+    area2 = area2 + cr;
+    c0 = c0 + (la[0] + lb[0]) * cr;
+    c1 = c1 + (la[1] + lb[1]) * cr;
+  }
+  for (int k = 0; k < 4; ++k) {
+    if (!(fphi[k] >= T(0) && fphi[ms_next(k)] < T(0))) continue;
+    const int j = chord_target(fphi, k, connect);
+    if (j < 0) continue;
+    const T* la = w.sb[k]; const T* lb = w.sa[j];
+    const T cr = la[0] * lb[1] - la[1] * lb[0];
+    area2 = area2 + cr;
+    c0 = c0 + (la[0] + lb[0]) * cr;
+    c1 = c1 + (la[1] + lb[1]) * cr;
+  }
+}
+
+// full_face_area (3D), src/cut_cell.jl:190-197
+template <class T> inline T full_face_area3(const T* cs, int dir) {
+  const int ax = dir >> 1;
+  T p = T(1);
+  for (int a = 0; a < 3; ++a) if (a != ax) p = p * cs[a];
+  return p;
+}
+
+// _edge_crossing, marching_cubes.jl:284-287
+template <class T>
+inline void edge_crossing(const T* pa, const T* pb, T fa, T fb, T* out) {
+  const T s = open_fraction(fa, fb);
+  if (fa >= T(0)) for (int i = 0; i < 3; ++i) out[i] = pa[i] + s * (pb[i] - pa[i]);
+  else for (int i = 0; i < 3; ++i) out[i] = pb[i] + s * (pa[i] - pb[i]);
+}
+
+// cut_cell_moments (3D), moments.jl:275-346, with cut_cell_faces (:224-257) and
+// _cut_cell_face (:150-196) inlined.
+template <class T>
+inline void mc_moments(const McTable& tb, const T nodes[8][3], const T phi_raw[8], const T cs[3],
+                       CellOut<T, 3>& o) {
+  T phi[8];
+  for (int k = 0; k < 8; ++k) phi[k] = nudge(phi_raw[k]);
+  const T* origin = nodes[0];
+  T centre[3];
+  for (int a = 0; a < 3; ++a) centre[a] = origin[a] + T(0.5) * cs[a];
+  const T vol_cell = (cs[0] * cs[1]) * cs[2];
+  const uint8_t* codes = nullptr;
+  int lcase = 1;
+  const int ntri = cell_triangles(tb, phi, &codes, &lcase);
+
+  T ln[8][3];
+  for (int k = 0; k < 8; ++k) for (int a = 0; a < 3; ++a) ln[k][a] = nodes[k][a] - origin[a];
+  int noutside = 0;
+  for (int k = 0; k < 8; ++k) noutside += phi[k] >= T(0) ? 1 : 0;
+  const int kind = noutside == 8 ? 1 : (noutside == 0 ? 0 : 2);
+  bool amb_face = false;
+  for (int dir = 0; dir < 6; ++dir) {
+    const int p = MCC.face_axes[dir][0], q = MCC.face_axes[dir][1];
+    const int* idx = MCC.face_nodes[dir];
+    T fn[4][2], fphi[4];
+    for (int k = 0; k < 4; ++k) { fn[k][0] = ln[idx[k]][p]; fn[k][1] = ln[idx[k]][q]; fphi[k] = phi[idx[k]]; }
+    int nout = 0;
+    for (int k = 0; k < 4; ++k) nout += fphi[k] >= T(0) ? 1 : 0;
+    const bool amb_dir = (nout == 2) && ((fphi[0] >= T(0)) == (fphi[2] >= T(0)));
+    T frac, c0, c1;
+    const T avg0 = T(0.25) * (((fn[0][0] + fn[1][0]) + fn[2][0]) + fn[3][0]);
+    const T avg1 = T(0.25) * (((fn[0][1] + fn[1][1]) + fn[2][1]) + fn[3][1]);
+    if (nout == 4 || nout == 0) {
+      frac = nout == 4 ? T(1) : T(0);
+      c0 = avg0; c1 = avg1;
+    } else {
+      T area2, m0, m1;
+      face_polygon(fn, fphi, test_face(phi, MCC.face_test_code[dir]), area2, m0, m1);
+      frac = (T(0.5) * area2) / full_face_area3(cs, dir);
+      if (area2 != T(0)) { const T den = T(3) * area2; c0 = m0 / den; c1 = m1 / den; }
+      else { c0 = avg0; c1 = avg1; }
+    }
+    o.ff[dir] = frac;
+    o.fcl[2 * dir] = c0;
+    o.fcl[2 * dir + 1] = c1;
+    amb_face = amb_face || amb_dir;
+  }
+  o.kind = int8_t(kind);
+  if (kind != 2) {
+    o.amb = 0;
+    o.vf = kind == 1 ? T(1) : T(0);
+    for (int a = 0; a < 3; ++a) { o.c[a] = centre[a]; o.ic[a] = centre[a]; }
+    return;
+  }
+  // edge_crossings, marching_cubes.jl:306-330
+  T pts[13][3];
+  T acc[3] = {T(0), T(0), T(0)};
+  int ncr = 0;
+  for (int e = 0; e < 12; ++e) {
+    const int a = MC_EDGE_NODES1[e][0] - 1, b = MC_EDGE_NODES1[e][1] - 1;
+    const bool crossed = (phi[a] >= T(0)) != (phi[b] >= T(0));
+    if (crossed) {
+      edge_crossing(ln[a], ln[b], phi[a], phi[b], pts[e]);
+      for (int i = 0; i < 3; ++i) acc[i] = acc[i] + pts[e][i];
+      ++ncr;
+    } else {
+      pts[e][0] = pts[e][1] = pts[e][2] = T(0);
+    }
+  }
+  for (int i = 0; i < 3; ++i) pts[12][i] = ncr > 0 ? acc[i] / T(ncr) : T(0);
+
+  T vol3 = T(0);
+  T cm2[3] = {T(0), T(0), T(0)};
+  for (int dir = 0; dir < 6; ++dir) {
+    const int ax = dir >> 1;
+    const T s = (dir & 1) ? T(1) : T(-1);
+    const T x_ax = ln[MCC.face_nodes[dir][0]][ax];
+    const T a_open = o.ff[dir] * full_face_area3(cs, dir);
+    vol3 = vol3 + (s * x_ax) * a_open;
+    for (int a = 0; a < 3; ++a) cm2[a] = cm2[a] + (a == ax ? ((s * x_ax) * x_ax) * a_open : T(0));
+  }
+  T iarea = T(0);
+  T icm[3] = {T(0), T(0), T(0)};
+  for (int t = 0; t < ntri; ++t) {
+    const T* A = pts[codes[3 * t] - 1];
+    const T* B = pts[codes[3 * t + 1] - 1];
+    const T* Dd = pts[codes[3 * t + 2] - 1];
+    T u[3], v[3];
+    for (int i = 0; i < 3; ++i) { u[i] = B[i] - A[i]; v[i] = Dd[i] - A[i]; }
+    T w[3] = {T(0.5) * (u[1] * v[2] - u[2] * v[1]), T(0.5) * (u[2] * v[0] - u[0] * v[2]),
+              T(0.5) * (u[0] * v[1] - u[1] * v[0])};
+    T xc[3];
+    for (int i = 0; i < 3; ++i) xc[i] = ((A[i] + B[i]) + Dd[i]) / T(3);
+    vol3 = vol3 - ((w[0] * xc[0] + w[1] * xc[1]) + w[2] * xc[2]);
+    for (int i = 0; i < 3; ++i) {
+      const T m2 = (((((A[i] * A[i] + B[i] * B[i]) + Dd[i] * Dd[i]) + A[i] * B[i]) + B[i] * Dd[i]) + Dd[i] * A[i]) / T(6);
+      cm2[i] = cm2[i] - w[i] * m2;
+    }
+    const T len = std::sqrt((w[0] * w[0] + w[1] * w[1]) + w[2] * w[2]);
+    iarea = iarea + len;
+    for (int i = 0; i < 3; ++i) icm[i] = icm[i] + len * xc[i];
+  }
+  const T volume = vol3 / T(3);
+  if (volume > T(0)) { const T den = T(2) * volume; for (int a = 0; a < 3; ++a) o.c[a] = origin[a] + cm2[a] / den; }
+  else for (int a = 0; a < 3; ++a) o.c[a] = centre[a];
+  if (iarea > T(0)) for (int a = 0; a < 3; ++a) o.ic[a] = origin[a] + icm[a] / iarea;
+  else for (int a = 0; a < 3; ++a) o.ic[a] = centre[a];
+  const bool amb_case = lcase == 5 || lcase == 7 || lcase == 8 || lcase == 11 || lcase == 13 || lcase == 14;
+  o.amb = (amb_face || amb_case) ? 1 : 0;
+  o.vf = volume / vol_cell;
+}
+
+// ----------------------------------------------------------------------------------
+// Column writers (the StructArray layout of include/cutcell_b200.h).
+template <class T, int D>
+inline void store(const cc_cells& c, int64_t ci, const CellOut<T, D>& o) {
+  c.kind[ci] = o.kind;
+  c.ambiguous[ci] = o.amb;
+  static_cast<T*>(c.volume_fraction)[ci] = o.vf;
+  for (int a = 0; a < D; ++a) static_cast<T*>(c.centroid)[D * ci + a] = o.c[a];
+  for (int a = 0; a < 2 * D; ++a) static_cast<T*>(c.face_fraction)[2 * D * ci + a] = o.ff[a];
+  for (int a = 0; a < 2 * D * (D - 1); ++a) static_cast<T*>(c.face_centroid_local)[2 * D * (D - 1) * ci + a] = o.fcl[a];
+  for (int a = 0; a < D; ++a) static_cast<T*>(c.interface_centroid)[D * ci + a] = o.ic[a];
+}
+
+template <class T>
+Tape<T> make_tape(const cc_optape* t) {
+  Tape<T> r;
+  r.ops.assign(t->ops, t->ops + t->n_ops);
+  r.p.resize(t->n_params);
+  for (int i = 0; i < t->n_params; ++i) r.p[i] = T(t->params[i]);
+  return r;
+}
+
+// _sample_nodes_kernel!, src/marching_squares/cache.jl:67-70
+template <class T, int D>
+void sample_nodes(const cc_grid& g, const Tape<T>& tp, T* phi) {
+  const int64_t nx = g.n[0] + 1, ny = g.n[1] + 1, nz = D == 3 ? g.n[2] + 1 : 1;
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
+  const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  parallel_for(ny * nz, [&](int64_t row) {
+    const int64_t j = row % ny, k = row / ny;
+    for (int64_t i = 0; i < nx; ++i) {
+      T x[3];
+      x[0] = node_coord(x0[0], d[0], i);
+      x[1] = node_coord(x0[1], d[1], j);
+      x[2] = node_coord(x0[2], d[2], k);
+      phi[i + nx * (j + ny * k)] = eval_tape<T, D, T>(tp, x);
+    }
+  });
+}
+
+// _nodal_cells_kernel!, src/marching_squares/cache.jl:75-78, 3D
+template <class T>
+void mc_cells(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells& c) {
+  const int64_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int64_t nx = n0 + 1, ny = n1 + 1;
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
+  const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  parallel_for(n1 * n2, [&](int64_t row) {
+    const int64_t j = row % n1, k = row / n1;
+    for (int64_t i = 0; i < n0; ++i) {
+        T nodes[8][3], ph[8];
+        for (int q = 0; q < 8; ++q) {
+          const int64_t ii = i + MC_BITS[q][0], jj = j + MC_BITS[q][1], kk = k + MC_BITS[q][2];
+          nodes[q][0] = node_coord(x0[0], d[0], ii);
+          nodes[q][1] = node_coord(x0[1], d[1], jj);
+          nodes[q][2] = node_coord(x0[2], d[2], kk);
+          ph[q] = phi[ii + nx * (jj + ny * kk)];
+        }
+        CellOut<T, 3> o;
+        mc_moments(tb, nodes, ph, d, o);
+        store<T, 3>(c, i + n0 * (j + n1 * k), o);
+    }
+  });
+}
+
+static const int MS_BITS[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+
+template <class T>
+void ms_cells(const cc_grid& g, const T* phi, const cc_cells& c) {
+  const int64_t n0 = g.n[0], n1 = g.n[1], nx = n0 + 1;
+  const T x0[2] = {T(g.x0[0]), T(g.x0[1])};
+  const T d[2] = {T(g.d[0]), T(g.d[1])};
+  parallel_for(n1, [&](int64_t j) {
+    for (int64_t i = 0; i < n0; ++i) {
+      T nodes[4][2], ph[4];
+      for (int q = 0; q < 4; ++q) {
+        const int64_t ii = i + MS_BITS[q][0], jj = j + MS_BITS[q][1];
+        nodes[q][0] = node_coord(x0[0], d[0], ii);
+        nodes[q][1] = node_coord(x0[1], d[1], jj);
+        ph[q] = phi[ii + nx * jj];
+      }
+      CellOut<T, 2> o;
+      ms_moments(nodes, ph, d, o);
+      store<T, 2>(c, i + n0 * j, o);
+    }
+  });
+}
+
+// _leaf_cells_kernel!, src/marching_squares/cache.jl:129-137
+template <class T>
+void ms_tree(const double* x0d, const double* based, int64_t nl, const int32_t* level,
+             const int32_t* coord, const Tape<T>& tp, T* phi4, const cc_cells& c) {
+  const T x0[2] = {T(x0d[0]), T(x0d[1])};
+  parallel_for(nl, [&](int64_t i) {
+    const T scale = T(std::ldexp(1.0, -level[i]));
+    const T h[2] = {T(based[0]) * scale, T(based[1]) * scale};
+    T nodes[4][2], ph[4];
+    for (int q = 0; q < 4; ++q) {
+      nodes[q][0] = x0[0] + T(int64_t(coord[2 * i]) + MS_BITS[q][0]) * h[0];
+      nodes[q][1] = x0[1] + T(int64_t(coord[2 * i + 1]) + MS_BITS[q][1]) * h[1];
+      ph[q] = eval_tape<T, 2, T>(tp, nodes[q]);
+      phi4[4 * i + q] = ph[q];
+    }
+    CellOut<T, 2> o;
+    ms_moments(nodes, ph, h, o);
+    store<T, 2>(c, i, o);
+  });
+}
+
+// ----------------------------------------------------------------------------------
+// PLIC (src/plic/plic.jl:72-88, src/plic/apertures.jl:73-125, src/plic/cache.jl:96-162)
+template <class T, int D>
+struct Plane {
+  T n[D];
+  T a;
+  T fraction;  // solid
+  bool valid;
+};
+
+template <class T, int D>
+inline Plane<T, D> cell_plane(const Tape<T>& tp, const T* x0, const T* d, const int64_t* idx) {
+  Dual<T, D> x[D];
+  for (int a = 0; a < D; ++a) {
+    x[a] = dconst<T, D>(centroid_coord(x0[a], d[a], idx[a]));
+    x[a].g[a] = T(1);
+  }
+  const Dual<T, D> r = eval_tape<T, D, Dual<T, D>>(tp, x);
+  const T dist = r.v;
+  T s = r.g[0];
+  for (int a = 1; a < D; ++a) s = s + r.g[a];
+  const T a = T(0.5) * s - dist / d[0];
+  bool allzero = true;
+  for (int q = 0; q < D; ++q) allzero = allzero && (r.g[q] == T(0));
+  Plane<T, D> pl;
+  if (std::isnan(a) || allzero) {
+    for (int q = 0; q < D; ++q) pl.n[q] = T(0);
+    pl.a = T(0);
+    pl.fraction = dist <= T(0) ? T(1) : T(0);
+    pl.valid = false;
+    return pl;
+  }
+  for (int q = 0; q < D; ++q) pl.n[q] = r.g[q];
+  pl.a = a;
+  pl.fraction = D == 2 ? gvf2(r.g[0], r.g[1], a) : gvf3(r.g[0], r.g[1], r.g[D - 1], a);
+  pl.valid = true;
+  return pl;
+}
+
+// _cell_wet + _face_area (2D and 3D), apertures.jl:73-125
+template <class T, int D>
+inline T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k /*0-based*/) {
+  const T s = (k & 1) ? T(1) : T(0);
+  if (D == 2) {
+    const int c = k < 2 ? 0 : 1, p = k < 2 ? 1 : 0;
+    const T len = cs[p];
+    if (!valid) return frac < T(0.5) ? T(0) : len;
+    const T base = n[c] * s - a;
+    return open_fraction(base, base + n[p]) * len;
+  } else {
+    int c, p, q;
+    if (k < 2) { c = 0; p = 1; q = 2; }
+    else if (k < 4) { c = 1; p = 0; q = 2; }
+    else { c = 2; p = 0; q = 1; }
+    const T U = cs[p], V = cs[q];
+    if (!valid) return frac < T(0.5) ? T(0) : U * V;
+    const T base = n[c] * s - a;
+    if (n[p] == T(0) && n[q] == T(0)) return base >= T(0) ? U * V : T(0);
+    const T solid = gvf2(n[p], n[q], -base);
+    return (U * V) * (T(1) - solid);
+  }
+}
+
+template <class T, int D>
+void plic_update(const cc_grid& g, const Tape<T>& tp, const cc_cells& c, T* normals, T* intercepts,
+                 uint8_t* is_valid) {
+  const int64_t n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
+  const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  const int64_t ncell = n[0] * n[1] * n[2];
+  T* vf = static_cast<T*>(c.volume_fraction);
+  parallel_for(ncell, [&](int64_t ci) {
+    const int64_t idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+    Plane<T, D> pl = cell_plane<T, D>(tp, x0, d, idx);
+    const T frac = T(1) - pl.fraction;
+    for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
+    intercepts[ci] = pl.a;
+    is_valid[ci] = pl.valid ? 1 : 0;
+    vf[ci] = frac;
+    c.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+  });
+  T* ff = static_cast<T*>(c.face_fraction);
+  parallel_for(ncell, [&](int64_t ci) {
+    const int64_t idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+    for (int k = 0; k < 2 * D; ++k) {
+      const int cax = k >> 1;
+      int64_t stride = 1;
+      for (int a = 0; a < cax; ++a) stride *= n[a];
+      T full;
+      if (D == 2) full = d[1 - cax];
+      else full = full_face_area3(d, k);
+      auto area_of = [&](int64_t cj, int kk) {
+        return face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], is_valid[cj] != 0, d, kk);
+      };
+      const T own = area_of(ci, k);
+      T r;
+      if ((k & 1) == 0) {
+        const bool has = idx[cax] >= 1;
+        const T below = area_of(has ? ci - stride : ci, k + 1);
+        r = has ? (below / full + own / full) / T(2) : own / full;
+      } else {
+        const bool has = idx[cax] <= n[cax] - 2;
+        const T above = area_of(has ? ci + stride : ci, k - 1);
+        r = has ? (own / full + above / full) / T(2) : own / full;
+      }
+      ff[2 * D * ci + k] = r;
+    }
+  });
+}
+
+template <class T, int D>
+T calc_volume(const cc_grid& g, const Tape<T>& tp) {
+  const int64_t n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
+  const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  T vol = T(0);
+  for (int64_t k = 0; k < n[2]; ++k)
+    for (int64_t j = 0; j < n[1]; ++j)
+      for (int64_t i = 0; i < n[0]; ++i) {
+        const int64_t idx[3] = {i, j, k};
+        vol = vol + cell_plane<T, D>(tp, x0, d, idx).fraction;
+      }
+  T pd = d[0];
+  for (int a = 1; a < D; ++a) pd = pd * d[a];
+  return vol * pd;
+}
+
+}  // namespace oc
+
+// ======================================================================================
+// C entry points for the test harness (ctypes). prec: 0 = Float32, 1 = Float64.
+extern "C" {
+
+int oc_set_threads(int n) {
+  if (n > 0) oc::g_threads = n;
+  return oc::g_threads;
+}
+
+int oc_sample_nodes(int prec, const cc_grid* g, const cc_optape* t, void* phi) {
+  if (g->dim == 3) {
+    if (prec == 1) oc::sample_nodes<double, 3>(*g, oc::make_tape<double>(t), (double*)phi);
+    else oc::sample_nodes<float, 3>(*g, oc::make_tape<float>(t), (float*)phi);
+  } else {
+    if (prec == 1) oc::sample_nodes<double, 2>(*g, oc::make_tape<double>(t), (double*)phi);
+    else oc::sample_nodes<float, 2>(*g, oc::make_tape<float>(t), (float*)phi);
+  }
+  return 0;
+}
+
+int oc_mc_cells_from_phi(int prec, const cc_grid* g, const uint8_t* table, const void* phi,
+                         const cc_cells* c) {
+  oc::McTable tb;
+  if (!tb.parse(table)) return CC_BAD_TABLE;
+  if (prec == 1) oc::mc_cells<double>(*g, tb, (const double*)phi, *c);
+  else oc::mc_cells<float>(*g, tb, (const float*)phi, *c);
+  return 0;
+}
+
+int oc_mc_update(int prec, const cc_grid* g, const cc_optape* t, const uint8_t* table, void* phi,
+                 const cc_cells* c) {
+  oc_sample_nodes(prec, g, t, phi);
+  return oc_mc_cells_from_phi(prec, g, table, phi, c);
+}
+
+int oc_ms_cells_from_phi(int prec, const cc_grid* g, const void* phi, const cc_cells* c) {
+  if (prec == 1) oc::ms_cells<double>(*g, (const double*)phi, *c);
+  else oc::ms_cells<float>(*g, (const float*)phi, *c);
+  return 0;
+}
+
+int oc_ms_update(int prec, const cc_grid* g, const cc_optape* t, void* phi, const cc_cells* c) {
+  oc_sample_nodes(prec, g, t, phi);
+  return oc_ms_cells_from_phi(prec, g, phi, c);
+}
+
+int oc_ms_tree_update(int prec, const double* x0, const double* base_d, int64_t nleaves,
+                      const int32_t* level, const int32_t* coord, const cc_optape* t, void* phi4,
+                      const cc_cells* c) {
+  if (prec == 1) oc::ms_tree<double>(x0, base_d, nleaves, level, coord, oc::make_tape<double>(t), (double*)phi4, *c);
+  else oc::ms_tree<float>(x0, base_d, nleaves, level, coord, oc::make_tape<float>(t), (float*)phi4, *c);
+  return 0;
+}
+
+int oc_plic_update(int prec, const cc_grid* g, const cc_optape* t, const cc_cells* c, void* normals,
+                   void* intercepts, uint8_t* is_valid) {
+  if (g->dim == 3) {
+    if (prec == 1) oc::plic_update<double, 3>(*g, oc::make_tape<double>(t), *c, (double*)normals, (double*)intercepts, is_valid);
+    else oc::plic_update<float, 3>(*g, oc::make_tape<float>(t), *c, (float*)normals, (float*)intercepts, is_valid);
+  } else {
+    if (prec == 1) oc::plic_update<double, 2>(*g, oc::make_tape<double>(t), *c, (double*)normals, (double*)intercepts, is_valid);
+    else oc::plic_update<float, 2>(*g, oc::make_tape<float>(t), *c, (float*)normals, (float*)intercepts, is_valid);
+  }
+  return 0;
+}
+
+double oc_calc_volume(int prec, const cc_grid* g, const cc_optape* t) {
+  if (g->dim == 3) {
+    if (prec == 1) return oc::calc_volume<double, 3>(*g, oc::make_tape<double>(t));
+    return double(oc::calc_volume<float, 3>(*g, oc::make_tape<float>(t)));
+  }
+  if (prec == 1) return oc::calc_volume<double, 2>(*g, oc::make_tape<double>(t));
+  return double(oc::calc_volume<float, 2>(*g, oc::make_tape<float>(t)));
+}
+
+double oc_gvf3(double n1, double n2, double n3, double a) { return oc::gvf3(n1, n2, n3, a); }
+double oc_gvf2(double n1, double n2, double a) { return oc::gvf2(n1, n2, a); }
+float oc_gvf3f(float n1, float n2, float n3, float a) { return oc::gvf3(n1, n2, n3, a); }
+
+// Per-cube dispatch pieces, exposed for the table tests.
+int oc_mc_triangles(const uint8_t* table, const double* phi8, uint8_t* codes_out, int* lcase) {
+  oc::McTable tb;
+  if (!tb.parse(table)) return -1;
+  double ph[8];
+  for (int k = 0; k < 8; ++k) ph[k] = oc::nudge(phi8[k]);
+  const uint8_t* codes = nullptr;
+  const int n = oc::cell_triangles(tb, ph, &codes, lcase);
+  std::memcpy(codes_out, codes, 3 * n);
+  return n;
+}
+int oc_test_face(const double* phi8, int face) { return oc::test_face(phi8, face) ? 1 : 0; }
+int oc_test_interior(int itype, int edge, const double* phi8, int s) {
+  return oc::test_interior(itype, edge, phi8, s) ? 1 : 0;
+}
+int oc_face_test_code(int dir) { return oc::MCC.face_test_code[dir]; }
+int oc_face_node(int dir, int k) { return oc::MCC.face_nodes[dir][k]; }
+
+double oc_eval_tape(int dim, int prec, const cc_optape* t, const double* x, double* grad) {
+  if (dim == 3) {
+    if (prec == 1) {
+      oc::Tape<double> tp = oc::make_tape<double>(t);
+      oc::Dual<double, 3> xs[3];
+      for (int a = 0; a < 3; ++a) { xs[a] = oc::dconst<double, 3>(x[a]); xs[a].g[a] = 1.0; }
+      auto r = oc::eval_tape<double, 3, oc::Dual<double, 3>>(tp, xs);
+      if (grad) for (int a = 0; a < 3; ++a) grad[a] = r.g[a];
+      return r.v;
+    }
+    oc::Tape<float> tp = oc::make_tape<float>(t);
+    float xs[3] = {float(x[0]), float(x[1]), float(x[2])};
+    return oc::eval_tape<float, 3, float>(tp, xs);
+  }
+  if (prec == 1) {
+    oc::Tape<double> tp = oc::make_tape<double>(t);
+    oc::Dual<double, 2> xs[2];
+    for (int a = 0; a < 2; ++a) { xs[a] = oc::dconst<double, 2>(x[a]); xs[a].g[a] = 1.0; }
+    auto r = oc::eval_tape<double, 2, oc::Dual<double, 2>>(tp, xs);
+    if (grad) for (int a = 0; a < 2; ++a) grad[a] = r.g[a];
+    return r.v;
+  }
+  oc::Tape<float> tp = oc::make_tape<float>(t);
+  float xs[2] = {float(x[0]), float(x[1])};
+  return oc::eval_tape<float, 2, float>(tp, xs);
+}
+
+}  // extern "C"
