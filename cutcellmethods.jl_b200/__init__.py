@@ -10,7 +10,7 @@ from .grid import CartesianGrid, CartesianIsoGrid, QuadTree, grid3, star_curve_t
 from .geometry import (Sphere, Circle, Box, Torus, Plane, Trig, Const, EmptyGeo, Star,  # noqa: F401
                        Union, SmoothUnion, Intersection, Subtraction, Negate, flatten, Tape,
                        quat_to_matrix)
-from . import mc_tables, readers  # noqa: F401
+from . import mc_tables, readers, workloads  # noqa: F401
 from .readers import CELL_INSIDE, CELL_OUTSIDE, CELL_CUT  # noqa: F401
 
 
@@ -31,7 +31,7 @@ def __getattr__(name):
     if name in ("allocate_cache", "update_cache", "MarchingCubesCutCellCache",
                 "MarchingSquaresCutCellCache", "PLICCutCellCache", "calc_volume",
                 "cut_cell_report", "face_fractions", "volume_fractions", "kinds", "CCError",
-                "DimensionMismatch", "ArgumentError_"):
+                "DimensionMismatch", "ArgumentError", "NodalField", "CellColumns"):
         from . import cache
         return getattr(cache, name)
     raise AttributeError(name)

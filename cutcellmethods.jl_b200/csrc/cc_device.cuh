@@ -1,0 +1,369 @@
+// cc_device.cuh -- device building blocks shared by the sm_100a kernels.
+//
+// Everything here is compiled with --fmad=false and IEEE division / square root, so each
+// expression rounds exactly as the reference's Julia code does on the CPU (Julia contracts no
+// a*b+c unless asked). Expression order follows the reference line by line (StaticArrays left
+// folds, elementwise division); the citations are to the reference files.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/cutcell_b200.h"
+
+namespace ccd {
+
+template <class T> struct Eps;
+template <> struct Eps<float> { static __device__ __forceinline__ float v() { return 1.1920928955078125e-07f; } };
+template <> struct Eps<double> { static __device__ __forceinline__ double v() { return 2.220446049250313e-16; } };
+
+template <class T> __device__ __forceinline__ T qnan();
+template <> __device__ __forceinline__ float qnan<float>() { return __int_as_float(0x7fc00000); }
+template <> __device__ __forceinline__ double qnan<double>() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+// ---------------------------------------------------------------------------------------------
+// Op-tape (include/cutcell_b200.h). The tape is copied into shared memory once per CTA; every
+// lane reads the same op at the same time, so the reads are broadcasts.
+template <class T>
+struct STape {
+  const cc_op* ops;
+  const T* p;
+  int n_ops;
+};
+
+// Forward-mode dual: the value and its gradient in D coordinates (the PLIC normal).
+template <class T, int D>
+struct Dual {
+  T v;
+  T g[D];
+};
+template <class T> __device__ __forceinline__ T val(T x) { return x; }
+template <class T, int D> __device__ __forceinline__ T val(const Dual<T, D>& x) { return x.v; }
+
+template <class S, class T> struct Lift { static __device__ __forceinline__ S c(T x) { return x; } };
+template <class T, int D> struct Lift<Dual<T, D>, T> {
+  static __device__ __forceinline__ Dual<T, D> c(T x) {
+    Dual<T, D> r; r.v = x;
+#pragma unroll
+    for (int i = 0; i < D; ++i) r.g[i] = T(0);
+    return r;
+  }
+};
+
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator+(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v + b.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] + b.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator-(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v - b.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] - b.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator-(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = -a.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = -a.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator*(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v * b.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator/(const Dual<T, D>& a, const Dual<T, D>& b) {
+  Dual<T, D> r; r.v = a.v / b.v;
+  const T bb = b.v * b.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = (a.g[i] * b.v - a.v * b.g[i]) / bb;
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator+(const Dual<T, D>& a, T c) { Dual<T, D> r = a; r.v = a.v + c; return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator-(const Dual<T, D>& a, T c) { Dual<T, D> r = a; r.v = a.v - c; return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator-(T c, const Dual<T, D>& a) { Dual<T, D> r = -a; r.v = c - a.v; return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator*(T c, const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = c * a.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = c * a.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator*(const Dual<T, D>& a, T c) {
+  Dual<T, D> r; r.v = a.v * c;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] * c;
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> operator/(const Dual<T, D>& a, T c) {
+  Dual<T, D> r; r.v = a.v / c;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / c;
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> dsqrt(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = sqrt(a.v);
+  const T two_s = T(2) * r.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / two_s;
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> dabs(const Dual<T, D>& a) {
+  const T sg = a.v > T(0) ? T(1) : (a.v < T(0) ? T(-1) : T(0));
+  Dual<T, D> r; r.v = fabs(a.v);
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = sg * a.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> dsin(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = sin(a.v); const T c = cos(a.v);
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = c * a.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> dcos(const Dual<T, D>& a) {
+  Dual<T, D> r; r.v = cos(a.v); const T s = -sin(a.v);
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = s * a.g[i];
+  return r; }
+template <class T, int D>
+__device__ __forceinline__ Dual<T, D> datan2(const Dual<T, D>& y, const Dual<T, D>& x) {
+  Dual<T, D> r; r.v = atan2(y.v, x.v);
+  const T den = x.v * x.v + y.v * y.v;
+#pragma unroll
+  for (int i = 0; i < D; ++i) r.g[i] = (x.v * y.g[i] - y.v * x.g[i]) / den;
+  return r; }
+
+__device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float dabs(float a) { return fabsf(a); }
+__device__ __forceinline__ double dabs(double a) { return fabs(a); }
+__device__ __forceinline__ float dsin(float a) { return sinf(a); }
+__device__ __forceinline__ double dsin(double a) { return sin(a); }
+__device__ __forceinline__ float dcos(float a) { return cosf(a); }
+__device__ __forceinline__ double dcos(double a) { return cos(a); }
+__device__ __forceinline__ float datan2(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double datan2(double y, double x) { return atan2(y, x); }
+
+// One primitive at the point x (SDFLibrary's sdf_value / get_sdf stand-ins).
+template <class T, int D, class S>
+__device__ __forceinline__ S tape_prim(const cc_op op, const T* __restrict__ p, const S* x) {
+  switch (op.opcode) {
+    case CC_OP_SPHERE: {
+      const T* c = p + op.poff;
+      S u = (x[0] - c[0]) * (x[0] - c[0]);
+#pragma unroll
+      for (int a = 1; a < D; ++a) u = u + (x[a] - c[a]) * (x[a] - c[a]);
+      return dsqrt(u) - c[D];
+    }
+    case CC_OP_BOX: {
+      const T* c = p + op.poff;
+      const T* h = c + D;
+      S q[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) q[a] = dabs(x[a] - c[a]) - h[a];
+      const S zero = Lift<S, T>::c(T(0));
+      S qa = val(q[0]) > T(0) ? q[0] : zero;
+      S u = qa * qa;
+#pragma unroll
+      for (int a = 1; a < D; ++a) { qa = val(q[a]) > T(0) ? q[a] : zero; u = u + qa * qa; }
+      const S outside = dsqrt(u);
+      S m = q[0];
+#pragma unroll
+      for (int a = 1; a < D; ++a) m = val(q[a]) > val(m) ? q[a] : m;
+      const S inside = val(m) < T(0) ? m : zero;
+      return outside + inside;
+    }
+    case CC_OP_TORUS:
+      if constexpr (D == 3) {
+        const T* c = p + op.poff;
+        const T* R = c + 3;
+        const S d0 = x[0] - c[0], d1 = x[1] - c[1], d2 = x[2] - c[2];
+        const S l0 = R[0] * d0 + R[1] * d1 + R[2] * d2;
+        const S l1 = R[3] * d0 + R[4] * d1 + R[5] * d2;
+        const S l2 = R[6] * d0 + R[7] * d1 + R[8] * d2;
+        const S qx = dsqrt(l0 * l0 + l1 * l1) - c[12];
+        return dsqrt(qx * qx + l2 * l2) - c[13];
+      } else {
+        return Lift<S, T>::c(qnan<T>());
+      }
+    case CC_OP_PLANE: {
+      const T* pt = p + op.poff;
+      const T* n = pt + D;
+      S s = n[0] * (x[0] - pt[0]);
+#pragma unroll
+      for (int a = 1; a < D; ++a) s = s + n[a] * (x[a] - pt[a]);
+      return s;
+    }
+    case CC_OP_TRIG: {
+      const T* q = p + op.poff;
+      S s = q[0] * dsin(q[1] * x[0]);
+#pragma unroll
+      for (int a = 1; a < D; ++a) s = s * dsin(q[1 + a] * x[a]);
+      return s + q[1 + D];
+    }
+    case CC_OP_CONST:
+      return Lift<S, T>::c(p[op.poff]);
+    case CC_OP_STAR:
+      if constexpr (D == 2) {
+        const T* q = p + op.poff;
+        const S dx = x[0] - q[0], dy = x[1] - q[1];
+        const S rad = dsqrt(dx * dx + dy * dy);
+        const S th = datan2(dy, dx);
+        S r = Lift<S, T>::c(q[2]);
+        for (int k = 2; k <= 6; ++k) r = r + q[3 + (k - 2)] * dcos(T(k) * th + q[8 + (k - 2)]);
+        return rad - r;
+      } else {
+        return Lift<S, T>::c(qnan<T>());
+      }
+    default:
+      return Lift<S, T>::c(qnan<T>());
+  }
+}
+
+template <class T, class S>
+__device__ __forceinline__ S tape_combine(int mode, const S& top, const S& v, T k) {
+  switch (mode) {
+    case CC_COMB_MIN: return val(v) < val(top) ? v : top;
+    case CC_COMB_MAX: return val(v) > val(top) ? v : top;
+    case CC_COMB_SUB: { const S w = -v; return val(w) > val(top) ? w : top; }
+    case CC_COMB_SMIN: {
+      const S ad = dabs(top - v);
+      const S hk = k - ad;
+      const S zero = Lift<S, T>::c(T(0));
+      const S h = (val(hk) > T(0) ? hk : zero) / k;
+      const S m = val(v) < val(top) ? v : top;
+      return m - ((h * h) * k) * T(0.25);
+    }
+    default: return v;
+  }
+}
+
+// Postfix evaluation. The top of the stack lives in a register; only nested CSG (a combinator
+// whose operand is itself a combinator) touches the local-memory stack below it.
+template <class T, int D, class S>
+__device__ __forceinline__ S tape_eval(const STape<T>& t, const S* x) {
+  S acc = Lift<S, T>::c(T(0));
+  S st[CC_TAPE_MAX_STACK];
+  int sp = 0;  // entries below acc
+  bool have = false;
+  for (int i = 0; i < t.n_ops; ++i) {
+    const cc_op op = t.ops[i];
+    S v;
+    if (op.opcode == CC_OP_NONE) {
+      if (op.combine == CC_COMB_NEG) { acc = -acc; continue; }
+      v = acc;
+      acc = st[--sp];
+    } else {
+      v = tape_prim<T, D, S>(op, t.p, x);
+    }
+    if (op.combine == CC_COMB_PUSH) {
+      if (have) st[sp++] = acc;
+      acc = v;
+      have = true;
+    } else {
+      acc = tape_combine<T, S>(op.combine, acc, v, op.combine == CC_COMB_SMIN ? t.p[op.kparam] : T(0));
+    }
+  }
+  return acc;
+}
+
+// Copy a tape (ops then params, already narrowed to T) from global into shared memory.
+template <class T>
+__device__ __forceinline__ STape<T> load_tape(const unsigned char* __restrict__ gtape, int n_ops, int n_params,
+                                              unsigned char* smem) {
+  const int bytes = n_ops * int(sizeof(cc_op)) + n_params * int(sizeof(T));
+  const int words = (bytes + 7) / 8;
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(gtape);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(smem);
+  for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = __ldg(src + w);
+  STape<T> t;
+  t.ops = reinterpret_cast<const cc_op*>(smem);
+  t.p = reinterpret_cast<const T*>(smem + ((n_ops * sizeof(cc_op) + 7) / 8) * 8);
+  t.n_ops = n_ops;
+  return t;
+}
+
+// ---------------------------------------------------------------------------------------------
+// CartesianMeshes stand-ins: node and centroid coordinates, the plane-cube clip.
+template <class T> __device__ __forceinline__ T node_coord(T x0, T d, long long i) { return x0 + T(i) * d; }
+template <class T> __device__ __forceinline__ T centroid_coord(T x0, T d, long long i) {
+  return x0 + T(double(i) + 0.5) * d;
+}
+
+// _open_fraction, src/marching_squares/marching_squares.jl:192-198
+template <class T>
+__device__ __forceinline__ T open_fraction(T pa, T pb) {
+  const bool fa = pa >= T(0), fb = pb >= T(0);
+  if (fa && fb) return T(1);
+  if (!fa && !fb) return T(0);
+  return fa ? pa / (pa - pb) : pb / (pb - pa);
+}
+
+// Solid fraction of the unit square {n . xi <= a} (Scardovelli & Zaleski 2000).
+template <class T>
+__device__ __forceinline__ T gvf2(T n1, T n2, T a) {
+  T m1 = fabs(n1), m2 = fabs(n2);
+  T alpha = a;
+  if (n1 < T(0)) alpha = alpha + m1;
+  if (n2 < T(0)) alpha = alpha + m2;
+  const T s = m1 + m2;
+  if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  m1 = m1 / s; m2 = m2 / s; alpha = alpha / s;
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= T(1)) return T(1);
+  const bool flip = alpha > T(0.5);
+  if (flip) alpha = T(1) - alpha;
+  if (m1 > m2) { const T t = m1; m1 = m2; m2 = t; }
+  T v;
+  if (alpha < m1) v = (alpha * alpha) / (T(2) * m1 * m2);
+  else v = (alpha - T(0.5) * m1) / m2;
+  return flip ? T(1) - v : v;
+}
+
+// Solid fraction of the unit cube {n . xi <= a} (Scardovelli & Zaleski 2000, with the
+// alpha^3 - (alpha - m1)^3 difference expanded so no branch divides a cancellation by a small m1).
+template <class T>
+__device__ __forceinline__ T gvf3(T n1, T n2, T n3, T a) {
+  T m0 = fabs(n1), m1_ = fabs(n2), m2_ = fabs(n3);
+  T alpha = a;
+  if (n1 < T(0)) alpha = alpha + m0;
+  if (n2 < T(0)) alpha = alpha + m1_;
+  if (n3 < T(0)) alpha = alpha + m2_;
+  const T s = (m0 + m1_) + m2_;
+  if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  m0 = m0 / s; m1_ = m1_ / s; m2_ = m2_ / s; alpha = alpha / s;
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= T(1)) return T(1);
+  const bool flip = alpha > T(0.5);
+  if (flip) alpha = T(1) - alpha;
+  T t;
+  if (m0 > m1_) { t = m0; m0 = m1_; m1_ = t; }
+  if (m1_ > m2_) { t = m1_; m1_ = m2_; m2_ = t; }
+  if (m0 > m1_) { t = m0; m0 = m1_; m1_ = t; }
+  const T m1 = m0, m2 = m1_, m3 = m2_;
+  const T m12 = m1 + m2;
+  T v;
+  if (alpha < m1) {
+    v = (alpha * alpha * alpha) / (T(6) * m1 * m2 * m3);
+  } else {
+    const T core = (T(3) * alpha * alpha - T(3) * alpha * m1 + m1 * m1) / (T(6) * m2 * m3);
+    if (alpha < m2) {
+      v = core;
+    } else if (alpha < (m12 < m3 ? m12 : m3)) {
+      const T u = alpha - m2;
+      v = core - (u * u * u) / (T(6) * m1 * m2 * m3);
+    } else if (m3 < m12) {
+      const T u = alpha - m2, w = alpha - m3;
+      v = core - (u * u * u + w * w * w) / (T(6) * m1 * m2 * m3);
+    } else {
+      v = (T(2) * alpha - m12) / (T(2) * m3);
+    }
+  }
+  return flip ? T(1) - v : v;
+}
+
+}  // namespace ccd

@@ -1,0 +1,279 @@
+// plic.cu -- PLICCutCell update_cache!, calc_volume and cut_cell_report on sm_100a.
+//
+// Fit pass (_plic_fit_kernel!, src/plic/cache.jl:96-113): per cell one forward-mode evaluation of
+// the op-tape at the centroid gives (dist, normal) -- get_sdf -- and cell_plane
+// (src/plic/plic.jl:72-88) turns it into the stored plane. Face pass
+// (_plic_face_fraction_kernel!, src/plic/cache.jl:118-162): per cell, per face, the mean of the
+// two one-sided candidates evaluated from the two cells' stored planes by the same _face_area
+// (src/plic/apertures.jl:112-125), so both cells of a face compute identical bits.
+#include <cstdint>
+#include "cc_device.cuh"
+#include "cc_internal.h"
+
+namespace {
+
+using namespace ccd;
+using cci::Cols;
+using cci::DevGrid;
+using cci::DevTape;
+
+constexpr int NT = 256;
+constexpr int VOL_BLOCKS = 148 * 8;
+
+template <class T, int D>
+struct PlaneFit {
+  T n[D];
+  T a;
+  T fraction;
+  bool valid;
+};
+
+// cell_plane, src/plic/plic.jl:72-88
+template <class T, int D>
+__device__ __forceinline__ PlaneFit<T, D> cell_plane(const STape<T>& t, const DevGrid<T>& g, const long long idx[3]) {
+  Dual<T, D> x[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    x[a].v = centroid_coord(g.x0[a], g.d[a], idx[a]);
+#pragma unroll
+    for (int b = 0; b < D; ++b) x[a].g[b] = a == b ? T(1) : T(0);
+  }
+  const Dual<T, D> r = tape_eval<T, D, Dual<T, D>>(t, x);
+  T s = r.g[0];
+#pragma unroll
+  for (int a = 1; a < D; ++a) s = s + r.g[a];
+  const T a = T(0.5) * s - r.v / g.d[0];
+  bool allzero = true;
+#pragma unroll
+  for (int q = 0; q < D; ++q) allzero = allzero && (r.g[q] == T(0));
+  PlaneFit<T, D> pl;
+  if (isnan(a) || allzero) {
+#pragma unroll
+    for (int q = 0; q < D; ++q) pl.n[q] = T(0);
+    pl.a = T(0);
+    pl.fraction = r.v <= T(0) ? T(1) : T(0);
+    pl.valid = false;
+    return pl;
+  }
+#pragma unroll
+  for (int q = 0; q < D; ++q) pl.n[q] = r.g[q];
+  pl.a = a;
+  if constexpr (D == 2) pl.fraction = gvf2(r.g[0], r.g[1], a);
+  else pl.fraction = gvf3(r.g[0], r.g[1], r.g[D - 1], a);
+  pl.valid = true;
+  return pl;
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const DevTape tape, const Cols cols,
+                                                      T* normals, T* intercepts, uint8_t* valid) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
+  __syncthreads();
+  const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
+  const long long total = n0 * n1 * n2;
+  T* vf = static_cast<T*>(cols.vf);
+  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
+    const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
+    const PlaneFit<T, D> pl = cell_plane<T, D>(t, g, idx);
+    const T frac = T(1) - pl.fraction;
+#pragma unroll
+    for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
+    intercepts[ci] = pl.a;
+    valid[ci] = pl.valid ? 1 : 0;
+    vf[ci] = frac;
+    cols.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+  }
+}
+
+// _cell_wet + _face_area, src/plic/apertures.jl:73-125 (k is the 0-based direction)
+template <class T, int D>
+__device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k) {
+  const T s = (k & 1) ? T(1) : T(0);
+  if constexpr (D == 2) {
+    const int c = k < 2 ? 0 : 1, p = k < 2 ? 1 : 0;
+    const T len = cs[p];
+    if (!valid) return frac < T(0.5) ? T(0) : len;
+    const T base = n[c] * s - a;
+    return open_fraction(base, base + n[p]) * len;
+  } else {
+    const int c = k >> 1;
+    const int p = c == 0 ? 1 : 0;
+    const int q = c == 2 ? 1 : 2;
+    const T U = cs[p], V = cs[q];
+    if (!valid) return frac < T(0.5) ? T(0) : U * V;
+    const T base = n[c] * s - a;
+    if (n[p] == T(0) && n[q] == T(0)) return base >= T(0) ? U * V : T(0);
+    const T solid = gvf2(n[p], n[q], -base);
+    return (U * V) * (T(1) - solid);
+  }
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const Cols cols, const T* __restrict__ normals,
+                                                       const T* __restrict__ intercepts, const uint8_t* __restrict__ valid) {
+  const long long n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
+  const long long total = n[0] * n[1] * n[2];
+  const T* vf = static_cast<const T*>(cols.vf);
+  T* ff = static_cast<T*>(cols.ff);
+  const T cs[3] = {g.d[0], g.d[1], D == 3 ? g.d[2] : T(1)};
+  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
+    const long long idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+#pragma unroll
+    for (int k = 0; k < 2 * D; ++k) {
+      const int c = k >> 1;
+      const long long stride = c == 0 ? 1 : (c == 1 ? n[0] : n[0] * n[1]);
+      T full;
+      if constexpr (D == 2) full = cs[1 - c];
+      else full = (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
+      const T own = face_area<T, D>(normals + D * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, k);
+      T r;
+      if ((k & 1) == 0) {
+        const bool has = idx[c] >= 1;
+        const long long cj = has ? ci - stride : ci;
+        const T below = face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k + 1);
+        r = has ? (below / full + own / full) / T(2) : own / full;
+      } else {
+        const bool has = idx[c] <= n[c] - 2;
+        const long long cj = has ? ci + stride : ci;
+        const T above = face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k - 1);
+        r = has ? (own / full + above / full) / T(2) : own / full;
+      }
+      ff[2 * D * ci + k] = r;
+    }
+  }
+}
+
+// Neumaier-compensated accumulation in Float64.
+struct KSum {
+  double s, c;
+  __device__ __forceinline__ void add(double x) {
+    const double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+  }
+};
+
+// calc_volume, src/volume.jl:29-40: every cell's cell_plane solid fraction, summed.
+template <class T, int D>
+__global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, const DevTape tape, double* partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
+  __syncthreads();
+  const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
+  const long long total = n0 * n1 * n2;
+  KSum acc{0.0, 0.0};
+  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
+    const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
+    acc.add(double(cell_plane<T, D>(t, g, idx).fraction));
+  }
+  __shared__ double ss[NT], sc[NT];
+  ss[threadIdx.x] = acc.s;
+  sc[threadIdx.x] = acc.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    KSum b{0.0, 0.0};
+    double cc = 0.0;
+    for (int i = 0; i < NT; ++i) { b.add(ss[i]); cc += sc[i]; }
+    partial[2 * blockIdx.x] = b.s;
+    partial[2 * blockIdx.x + 1] = b.c + cc;
+  }
+}
+
+__global__ void calc_volume_final(const double* partial, int nb, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  KSum b{0.0, 0.0};
+  double cc = 0.0;
+  for (int i = 0; i < nb; ++i) { b.add(partial[2 * i]); cc += partial[2 * i + 1]; }
+  out[0] = b.s + (b.c + cc);
+}
+
+// cut_cell_report, src/cut_cell.jl:302-319: counts by kind, ambiguous, smallest cut fraction.
+template <class T>
+__global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_t* __restrict__ kind,
+                                                    const uint8_t* __restrict__ amb, const T* __restrict__ vf,
+                                                    unsigned long long* counts, unsigned long long* vmin_bits) {
+  unsigned long long cut = 0, ins = 0, out = 0, am = 0;
+  T vmin = T(1);
+  for (long long i = blockIdx.x * (long long)NT + threadIdx.x; i < ncell; i += (long long)gridDim.x * NT) {
+    const int k = kind[i];
+    cut += k == 2;
+    ins += k == 0;
+    out += k == 1;
+    am += amb[i] != 0;
+    if (k == 2) { const T v = vf[i]; if (v > T(0) && v < vmin) vmin = v; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cut += __shfl_down_sync(0xffffffffu, cut, o);
+    ins += __shfl_down_sync(0xffffffffu, ins, o);
+    out += __shfl_down_sync(0xffffffffu, out, o);
+    am += __shfl_down_sync(0xffffffffu, am, o);
+    const T w = __shfl_down_sync(0xffffffffu, vmin, o);
+    vmin = w < vmin ? w : vmin;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(counts + 0, cut);
+    atomicAdd(counts + 1, ins);
+    atomicAdd(counts + 2, out);
+    atomicAdd(counts + 3, am);
+    // non-negative floats order as their bit patterns
+    const double dv = double(vmin);
+    atomicMin(vmin_bits, (unsigned long long)__double_as_longlong(dv));
+  }
+}
+
+int blocks_for(long long work, int per_sm) {
+  long long b = (work + NT - 1) / NT;
+  const long long cap = 148LL * per_sm;
+  return int(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+namespace cci {
+
+template <class T, int D>
+cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals, T* intercepts,
+                        uint8_t* valid, cudaStream_t s) {
+  const long long total = g.n[0] * g.n[1] * (D == 3 ? g.n[2] : 1);
+  const int sm = ((tape.bytes_len + 15) / 16) * 16;
+  plic_fit_kernel<T, D><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
+  plic_face_kernel<T, D><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+  return cudaGetLastError();
+}
+
+int calc_volume_blocks() { return VOL_BLOCKS; }
+
+template <class T, int D>
+cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial, double* out,
+                               cudaStream_t s) {
+  const int sm = ((tape.bytes_len + 15) / 16) * 16;
+  calc_volume_kernel<T, D><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+  calc_volume_final<<<1, 32, 0, s>>>(partial, VOL_BLOCKS, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* amb, const void* vf, int is_f64,
+                          unsigned long long* counts, double* vmin, cudaStream_t s) {
+  const int nb = blocks_for(ncell, 8);
+  unsigned long long* vb = reinterpret_cast<unsigned long long*>(vmin);
+  if (is_f64)
+    report_kernel<double><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const double*>(vf), counts, vb);
+  else
+    report_kernel<float><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const float*>(vf), counts, vb);
+  return cudaGetLastError();
+}
+
+#define INST(T, D)                                                                                      \
+  template cudaError_t launch_plic<T, D>(const DevGrid<T>&, const DevTape&, const Cols&, T*, T*, uint8_t*, \
+                                         cudaStream_t);                                                 \
+  template cudaError_t launch_calc_volume<T, D>(const DevGrid<T>&, const DevTape&, double*, double*, cudaStream_t);
+INST(float, 2)
+INST(float, 3)
+INST(double, 2)
+INST(double, 3)
+#undef INST
+
+}  // namespace cci

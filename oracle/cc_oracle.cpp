@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <thread>
 #include <atomic>
+#include <type_traits>
 #include "../include/cutcell_b200.h"
 
 namespace oc {
@@ -1116,6 +1117,26 @@ double oc_calc_volume(int prec, const cc_grid* g, const cc_optape* t) {
   }
   if (prec == 1) return oc::calc_volume<double, 2>(*g, oc::make_tape<double>(t));
   return double(oc::calc_volume<float, 2>(*g, oc::make_tape<float>(t)));
+}
+
+// Every cell's cell_plane solid fraction, widened to double (the calc_volume integrand).
+int oc_plic_fractions(int prec, const cc_grid* g, const cc_optape* t, double* out) {
+  const int64_t n[3] = {g->n[0], g->n[1], g->dim == 3 ? g->n[2] : 1};
+  const int64_t ncell = n[0] * n[1] * n[2];
+  auto run = [&](auto zero, auto dimc) {
+    using T = decltype(zero);
+    constexpr int D = decltype(dimc)::value;
+    const oc::Tape<T> tp = oc::make_tape<T>(t);
+    const T x0[3] = {T(g->x0[0]), T(g->x0[1]), T(g->x0[2])};
+    const T d[3] = {T(g->d[0]), T(g->d[1]), T(g->d[2])};
+    oc::parallel_for(ncell, [&](int64_t ci) {
+      const int64_t idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+      out[ci] = double(oc::cell_plane<T, D>(tp, x0, d, idx).fraction);
+    });
+  };
+  if (g->dim == 3) { if (prec == 1) run(0.0, std::integral_constant<int, 3>()); else run(0.0f, std::integral_constant<int, 3>()); }
+  else { if (prec == 1) run(0.0, std::integral_constant<int, 2>()); else run(0.0f, std::integral_constant<int, 2>()); }
+  return 0;
 }
 
 double oc_gvf3(double n1, double n2, double n3, double a) { return oc::gvf3(n1, n2, n3, a); }

@@ -215,3 +215,11 @@ def test_face(phi8, face):
 def test_interior(itype, edge, phi8, s):
     ph = np.ascontiguousarray(phi8, np.float64)
     return bool(lib().oc_test_interior(int(itype), int(edge), _ptr(ph), int(s)))
+
+
+def plic_fractions(g, tape, prec):
+    """Every cell's PLIC solid fraction (the calc_volume integrand), as float64."""
+    out = np.zeros(g.ncell, np.float64)
+    t, keep = tape_struct(tape)
+    lib().oc_plic_fractions(prec, C.byref(grid_struct(g)), C.byref(t), _ptr(out))
+    return out

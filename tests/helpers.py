@@ -54,3 +54,27 @@ def corners(vals_zyx, i, j, k):
 
 
 MC_CUBE = cc.CartesianGrid((0.0, 0.0, 0.0), (1, 1, 1), (1.0, 1.0, 1.0))
+
+
+FIELDS = ("kind", "ambiguous", "volume_fraction", "centroid", "face_fraction", "face_centroid_local",
+          "interface_centroid")
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.float64:
+        return a.view(np.uint64)
+    if a.dtype == np.float32:
+        return a.view(np.uint32)
+    return a
+
+
+def assert_cells_bitwise(dev: dict, ref: dict, fields=FIELDS, label=""):
+    """Every listed column equal bit for bit; on failure report how many cells differ and where."""
+    for f in fields:
+        a = bits(np.asarray(dev[f]).reshape(len(ref[f]), -1))
+        b = bits(np.asarray(ref[f]).reshape(len(ref[f]), -1))
+        bad = np.flatnonzero(np.any(a != b, axis=1))
+        assert bad.size == 0, (f"{label} {f}: {bad.size} cells differ, first {bad[:5].tolist()}: "
+                               f"dev {np.asarray(dev[f]).reshape(len(ref[f]), -1)[bad[0]]} "
+                               f"ref {np.asarray(ref[f]).reshape(len(ref[f]), -1)[bad[0]]}")

@@ -1,0 +1,113 @@
+"""Marching cubes on the B200 through the C ABI, against the oracle, bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import cc, po, XorShift, assert_cells_bitwise, bits
+
+pytestmark = pytest.mark.gpu
+W = cc.workloads
+TABLE = cc.mc_tables.project_table()
+DT = {0: torch.float32, 1: torch.float64}
+
+
+def run_dev(g, geo, prec, table=None):
+    cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=DT[prec], table=table)
+    cc.update_cache(cache, geo, g)
+    return cache.phi.cpu().numpy(), cache.to_host(), cache
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("n", [24, 35, 64])
+def test_sphere_and_csg_bitwise(prec, n):
+    for body, g in ((cc.Sphere((0.01, 0.02, -0.03), 1.0), cc.grid3(n)),
+                    (W.csg_body(0), W.csg_grid(n))):
+        tape = cc.flatten(body, 3)
+        phi, cols, _ = run_dev(g, tape, prec)
+        rphi, ref = po.mc_update(g, tape, TABLE, prec)
+        assert np.array_equal(bits(phi), bits(rphi)), "phi differs"
+        assert_cells_bitwise(cols, ref, label=f"n={n} prec={prec}")
+        assert (cols["kind"] == 2).sum() > 50
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_random_field_cells_from_phi(prec):
+    n = 35
+    g = cc.CartesianGrid((0.0, 0.0, 0.0), (n, n, n), (1.0, 1.0, 1.0))
+    rng = XorShift(31337)
+    vals = np.array([rng.randn() for _ in range((n + 1) ** 3)])
+    if prec == 0:
+        vals = vals.astype(np.float32)
+    for table in (TABLE, cc.mc_tables.probe_table()):
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=DT[prec], table=table)
+        cc.update_cache(cache, cc.NodalField(torch.as_tensor(vals)), g)
+        ref = po.mc_cells_from_phi(g, vals, table, prec)
+        assert_cells_bitwise(cache.to_host(), ref, label="random field")
+        assert (ref["kind"] == 2).sum() > 40000
+
+
+def test_trig_field_phi_close_cells_bitwise():
+    # sin() differs between CUDA's libm and glibc by an ulp: the cells are checked against the
+    # oracle run on the device's own phi, and phi against the oracle's within a few ulp.
+    g = cc.grid3(40)
+    tape = cc.flatten(cc.Trig(1.0, (2.7, 3.1, 2.3), -0.12), 3)
+    phi, cols, _ = run_dev(g, tape, 1)
+    rphi = po.sample_nodes(g, tape, 1)
+    assert np.max(np.abs(phi - rphi)) < 1e-14
+    assert_cells_bitwise(cols, po.mc_cells_from_phi(g, phi, TABLE, 1))
+    assert (cols["kind"] == 2).sum() > 1000
+
+
+def test_stretched_and_offset_grids():
+    for g in (cc.CartesianGrid((0.3, -1.1, 0.7), (48, 33, 17), (0.05, 0.07, 0.11)),
+              cc.CartesianGrid((-1.3, -1.25, -0.9), (128, 5, 40), (0.021, 0.5, 0.05))):
+        tape = cc.flatten(cc.Union(cc.Sphere((0.9, -0.2, 1.4), 0.8), cc.Box((1.0, 0.0, 1.2), (0.5, 0.3, 0.4))), 3)
+        for prec in (0, 1):
+            phi, cols, _ = run_dev(g, tape, prec)
+            rphi, ref = po.mc_update(g, tape, TABLE, prec)
+            assert np.array_equal(bits(phi), bits(rphi))
+            assert_cells_bitwise(cols, ref, label=str(g.n))
+
+
+def test_device_invariants_at_256():
+    # size-independent properties at the benchmark's shape: shared faces bitwise, closure exact,
+    # kind the sign pattern of the stored phi, uncut fields exact.
+    n = 256
+    g = W.csg_grid(n)
+    for prec in (0, 1):
+        phi, cols, cache = run_dev(g, W.csg_body(3), prec)
+        ff = cols["face_fraction"].reshape(n, n, n, 6)
+        assert np.array_equal(bits(ff[:, :, :-1, 1]), bits(ff[:, :, 1:, 0]))
+        assert np.array_equal(bits(ff[:, :-1, :, 3]), bits(ff[:, 1:, :, 2]))
+        assert np.array_equal(bits(ff[:-1, :, :, 5]), bits(ff[1:, :, :, 4]))
+        d = tuple(np.dtype(np.float32 if prec == 0 else np.float64).type(a) for a in g.d)
+        assert np.all(cc.readers.closure_residual(cols["face_fraction"], d) == 0)
+        eps = np.finfo(phi.dtype).eps
+        p = np.where(np.abs(phi) < eps, eps, phi).reshape(n + 1, n + 1, n + 1) >= 0
+        cnt = sum(p[a:a + n, b:b + n, c:c + n].astype(np.int32)
+                  for a in (0, 1) for b in (0, 1) for c in (0, 1))
+        kind = cols["kind"].reshape(n, n, n)
+        assert np.array_equal(kind, np.where(cnt == 8, 1, np.where(cnt == 0, 0, 2)).astype(np.int8))
+        vf = cols["volume_fraction"].reshape(n, n, n)
+        assert np.all(vf[kind == 1] == 1) and np.all(vf[kind == 0] == 0)
+        assert np.all((vf >= -1e-6) & (vf <= 1 + 1e-6))
+        rep = cc.cut_cell_report(cache)
+        hr = cc.readers.cut_cell_report(cols["kind"], cols["ambiguous"], cols["volume_fraction"])
+        assert (rep["cut"], rep["inside"], rep["outside"], rep["ambiguous"]) == \
+               (hr["cut"], hr["inside"], hr["outside"], hr["ambiguous"])
+        assert rep["min_volume_fraction"] == float(hr["min_volume_fraction"])
+        del cache
+
+
+def test_dimension_mismatch_and_moved_grid():
+    g = cc.CartesianGrid((-1.5, -1.5, -1.5), (24, 24, 24), (0.125, 0.125, 0.125))
+    sph = cc.Sphere((0.01, 0.02, -0.03), 1.0)
+    cache = cc.allocate_cache(g, cc.MarchingCubesCutCell())
+    host = cache.to_host()
+    assert np.all(host["kind"] == 1) and np.all(host["volume_fraction"] == 1)  # seeded as no body
+    with pytest.raises(cc.DimensionMismatch):
+        cc.update_cache(cache, sph, cc.CartesianGrid((0, 0, 0), (10, 10, 10), (0.1, 0.1, 0.1)))
+    moved = g.moved((0.013, -0.007, 0.021))
+    cc.update_cache(cache, sph, moved)
+    fresh = cc.update_cache(cc.allocate_cache(moved, cc.MarchingCubesCutCell()), sph, moved)
+    assert_cells_bitwise(cache.to_host(), fresh.to_host())
