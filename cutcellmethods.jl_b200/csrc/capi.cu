@@ -26,7 +26,10 @@ cc_status fail(cc_status s, const std::string& msg) {
   return s;
 }
 
-constexpr size_t TAPE_CAP = CC_TAPE_MAX_OPS * sizeof(cc_op) + CC_TAPE_MAX_PARAMS * sizeof(double) + 16;
+// Packed tapes: every op gets its own copy of its primitive's parameters padded to a multiple of 4
+// elements (at most 16) plus, for a smooth-min, its k -- at most 17 slots per op.
+constexpr int PACK_MAX_PARAMS = 17 * CC_TAPE_MAX_OPS;
+constexpr size_t TAPE_CAP = CC_TAPE_MAX_OPS * sizeof(cc_op) + PACK_MAX_PARAMS * sizeof(double) + 64;
 
 int prim_params(int opcode, int dim) {
   switch (opcode) {
@@ -103,25 +106,46 @@ struct cc_handle {
   unsigned char* table_dev = nullptr;
   size_t table_bytes = 0;
   cci::DevTable tb{};
+  unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
+  unsigned* cut_count = nullptr;
   double* vol_scratch = nullptr;  // calc_volume partials + result
   unsigned long long* rep_scratch = nullptr;  // report counters + min
 };
 
 namespace {
 
-// Narrow and upload a validated tape into the handle's device buffer, ordered on stream s.
+// Pack a validated tape for the device -- each primitive's parameter block moved to a 4-element
+// boundary (read there with vector loads), each smooth-min k copied beside the blocks, everything
+// narrowed to T -- and upload it into the handle's buffer, ordered on stream s.
 template <class T>
-cc_status upload_tape(cc_handle* h, const cc_optape* t, cudaStream_t s, cci::DevTape* out) {
+cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, cci::DevTape* out) {
   if (h->tape_pending) {
     const cudaError_t e = cudaEventSynchronize(h->tape_copied);
     if (e != cudaSuccess) return cuda_fail(e, "tape staging");
     h->tape_pending = false;
   }
-  const size_t ops_bytes = ((t->n_ops * sizeof(cc_op) + 7) / 8) * 8;
-  std::memcpy(h->tape_host, t->ops, t->n_ops * sizeof(cc_op));
+  const size_t ops_bytes = ((t->n_ops * sizeof(cc_op) + 15) / 16) * 16;
+  cc_op* ops = reinterpret_cast<cc_op*>(h->tape_host);
   T* p = reinterpret_cast<T*>(h->tape_host + ops_bytes);
-  for (int i = 0; i < t->n_params; ++i) p[i] = T(t->params[i]);
-  const size_t bytes = ops_bytes + t->n_params * sizeof(T);
+  int np = 0;
+  for (int i = 0; i < t->n_ops; ++i) {
+    cc_op op = t->ops[i];
+    if (op.opcode != CC_OP_NONE) {
+      const int cnt = prim_params(op.opcode, dim);
+      const int padded = ((cnt + 3) / 4) * 4;
+      for (int q = 0; q < padded; ++q) p[np + q] = q < cnt ? T(t->params[op.poff + q]) : T(0);
+      op.poff = uint16_t(np);
+      np += padded;
+    }
+    if (op.combine == CC_COMB_SMIN) {
+      p[np] = T(t->params[op.kparam]);
+      op.kparam = uint16_t(np);
+      np += 1;
+    }
+    ops[i] = op;
+  }
+  for (size_t b = t->n_ops * sizeof(cc_op); b < ops_bytes; ++b) h->tape_host[b] = 0;
+  const size_t bytes = ops_bytes + np * sizeof(T);
   cudaError_t e = cudaMemcpyAsync(h->tape_dev, h->tape_host, bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_fail(e, "tape upload");
   e = cudaEventRecord(h->tape_copied, s);
@@ -129,7 +153,7 @@ cc_status upload_tape(cc_handle* h, const cc_optape* t, cudaStream_t s, cci::Dev
   h->tape_pending = true;
   out->bytes = h->tape_dev;
   out->n_ops = t->n_ops;
-  out->n_params = t->n_params;
+  out->n_params = np;
   out->bytes_len = int(bytes);
   return CC_OK;
 }
@@ -208,6 +232,8 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   const bool tree = method == CC_MARCHING_SQUARES && n[1] == 0;
   for (int a = 0; a < (tree ? 1 : dim); ++a)
     if (n[a] < 1) return fail(CC_BAD_ARG, "every axis needs at least one cell");
+  if (method == CC_MARCHING_CUBES && double(n[0]) * double(n[1]) * double(n[2]) > 4294967295.0)
+    return fail(CC_TOO_LARGE, "marching cubes indexes at most 2^32 - 1 cells per cache");
   DeviceGuard dg(device);
   cc_handle* h = new cc_handle();
   h->device = device;
@@ -222,6 +248,11 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->tape_copied, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&h->vol_scratch, (2 * cci::calc_volume_blocks() + 2) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->rep_scratch, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess && method == CC_MARCHING_CUBES) {
+    const int64_t ncell = h->n[0] * h->n[1] * h->n[2];
+    e = cudaMalloc(&h->cut_list, size_t(ncell) * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&h->cut_count, sizeof(unsigned));
+  }
   if (e != cudaSuccess) {
     cc_handle_destroy(h);
     return cuda_fail(e, "cc_handle_create");
@@ -239,6 +270,8 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->table_dev) cudaFree(h->table_dev);
   if (h->vol_scratch) cudaFree(h->vol_scratch);
   if (h->rep_scratch) cudaFree(h->rep_scratch);
+  if (h->cut_list) cudaFree(h->cut_list);
+  if (h->cut_count) cudaFree(h->cut_count);
   delete h;
   return CC_OK;
 }
@@ -306,13 +339,13 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
   if (h->prec == CC_F64) {
-    if (body && (st = upload_tape<double>(h, body, s, &tape)) != CC_OK) return st;
+    if (body && (st = upload_tape<double>(h, body, 3, s, &tape)) != CC_OK) return st;
     e = cci::launch_mc<double>(dev_grid<double>(g), tape, static_cast<const double*>(phi_in),
-                               static_cast<double*>(phi_out), cols_of(cells), h->tb, s);
+                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s);
   } else {
-    if (body && (st = upload_tape<float>(h, body, s, &tape)) != CC_OK) return st;
+    if (body && (st = upload_tape<float>(h, body, 3, s, &tape)) != CC_OK) return st;
     e = cci::launch_mc<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
-                              static_cast<float*>(phi_out), cols_of(cells), h->tb, s);
+                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching cubes launch");
   return CC_OK;
@@ -340,11 +373,11 @@ static cc_status ms_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
   if (h->prec == CC_F64) {
-    if (body && (st = upload_tape<double>(h, body, s, &tape)) != CC_OK) return st;
+    if (body && (st = upload_tape<double>(h, body, 2, s, &tape)) != CC_OK) return st;
     e = cci::launch_ms<double>(dev_grid<double>(g), tape, static_cast<const double*>(phi_in),
                                static_cast<double*>(phi_out), cols_of(cells), s);
   } else {
-    if (body && (st = upload_tape<float>(h, body, s, &tape)) != CC_OK) return st;
+    if (body && (st = upload_tape<float>(h, body, 2, s, &tape)) != CC_OK) return st;
     e = cci::launch_ms<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
                               static_cast<float*>(phi_out), cols_of(cells), s);
   }
@@ -383,12 +416,12 @@ cc_status cc_ms_tree_update(cc_handle* h, const cc_tree* t, const cc_optape* bod
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
   if (h->prec == CC_F64) {
-    if ((st = upload_tape<double>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<double>(h, body, 2, s, &tape)) != CC_OK) return st;
     const double x0[2] = {t->x0[0], t->x0[1]};
     e = cci::launch_ms_tree<double>(x0, t->base_d, t->nleaves, t->level, t->coord, tape, static_cast<double*>(phi4),
                                     cols_of(cells), s);
   } else {
-    if ((st = upload_tape<float>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<float>(h, body, 2, s, &tape)) != CC_OK) return st;
     const float x0[2] = {float(t->x0[0]), float(t->x0[1])};
     e = cci::launch_ms_tree<float>(x0, t->base_d, t->nleaves, t->level, t->coord, tape, static_cast<float*>(phi4),
                                    cols_of(cells), s);
@@ -410,13 +443,13 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
   if (h->prec == CC_F64) {
-    if ((st = upload_tape<double>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     e = g->dim == 3 ? cci::launch_plic<double, 3>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
                                                   static_cast<double*>(intercepts), is_valid, s)
                     : cci::launch_plic<double, 2>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
                                                   static_cast<double*>(intercepts), is_valid, s);
   } else {
-    if ((st = upload_tape<float>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     e = g->dim == 3 ? cci::launch_plic<float, 3>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
                                                  static_cast<float*>(intercepts), is_valid, s)
                     : cci::launch_plic<float, 2>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
@@ -442,14 +475,14 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   cudaError_t e;
   double pd;
   if (h->prec == CC_F64) {
-    if ((st = upload_tape<double>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     const cci::DevGrid<double> dg2 = dev_grid<double>(g);
     e = g->dim == 3 ? cci::launch_calc_volume<double, 3>(dg2, tape, partial, res, s)
                     : cci::launch_calc_volume<double, 2>(dg2, tape, partial, res, s);
     pd = dg2.d[0] * dg2.d[1];
     if (g->dim == 3) pd = pd * dg2.d[2];
   } else {
-    if ((st = upload_tape<float>(h, body, s, &tape)) != CC_OK) return st;
+    if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     const cci::DevGrid<float> dg2 = dev_grid<float>(g);
     e = g->dim == 3 ? cci::launch_calc_volume<float, 3>(dg2, tape, partial, res, s)
                     : cci::launch_calc_volume<float, 2>(dg2, tape, partial, res, s);

@@ -148,23 +148,38 @@ __device__ __forceinline__ double dcos(double a) { return cos(a); }
 __device__ __forceinline__ float datan2(float y, float x) { return atan2f(y, x); }
 __device__ __forceinline__ double datan2(double y, double x) { return atan2(y, x); }
 
+// Primitive parameter blocks start on a 4-element boundary of the tape's parameter array (the
+// host packs them so), so a block is read with 16-byte vector loads.
+__device__ __forceinline__ void ldq(const float* p, float* o) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+}
+__device__ __forceinline__ void ldq(const double* p, double* o) {
+  const double2 a = *reinterpret_cast<const double2*>(p);
+  const double2 b = *reinterpret_cast<const double2*>(p + 2);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+
 // One primitive at the point x (SDFLibrary's sdf_value / get_sdf stand-ins).
 template <class T, int D, class S>
 __device__ __forceinline__ S tape_prim(const cc_op op, const T* __restrict__ p, const S* x) {
+  const T* b = p + op.poff;
   switch (op.opcode) {
     case CC_OP_SPHERE: {
-      const T* c = p + op.poff;
+      T c[4];
+      ldq(b, c);
       S u = (x[0] - c[0]) * (x[0] - c[0]);
 #pragma unroll
       for (int a = 1; a < D; ++a) u = u + (x[a] - c[a]) * (x[a] - c[a]);
       return dsqrt(u) - c[D];
     }
     case CC_OP_BOX: {
-      const T* c = p + op.poff;
-      const T* h = c + D;
+      T c[8];
+      ldq(b, c);
+      if (D == 3) ldq(b + 4, c + 4);
       S q[D];
 #pragma unroll
-      for (int a = 0; a < D; ++a) q[a] = dabs(x[a] - c[a]) - h[a];
+      for (int a = 0; a < D; ++a) q[a] = dabs(x[a] - c[a]) - c[D + a];
       const S zero = Lift<S, T>::c(T(0));
       S qa = val(q[0]) > T(0) ? q[0] : zero;
       S u = qa * qa;
@@ -179,7 +194,8 @@ __device__ __forceinline__ S tape_prim(const cc_op op, const T* __restrict__ p, 
     }
     case CC_OP_TORUS:
       if constexpr (D == 3) {
-        const T* c = p + op.poff;
+        T c[16];
+        ldq(b, c); ldq(b + 4, c + 4); ldq(b + 8, c + 8); ldq(b + 12, c + 12);
         const T* R = c + 3;
         const S d0 = x[0] - c[0], d1 = x[1] - c[1], d2 = x[2] - c[2];
         const S l0 = R[0] * d0 + R[1] * d1 + R[2] * d2;
@@ -191,25 +207,29 @@ __device__ __forceinline__ S tape_prim(const cc_op op, const T* __restrict__ p, 
         return Lift<S, T>::c(qnan<T>());
       }
     case CC_OP_PLANE: {
-      const T* pt = p + op.poff;
-      const T* n = pt + D;
-      S s = n[0] * (x[0] - pt[0]);
+      T c[8];
+      ldq(b, c);
+      if (D == 3) ldq(b + 4, c + 4);
+      S s = c[D] * (x[0] - c[0]);
 #pragma unroll
-      for (int a = 1; a < D; ++a) s = s + n[a] * (x[a] - pt[a]);
+      for (int a = 1; a < D; ++a) s = s + c[D + a] * (x[a] - c[a]);
       return s;
     }
     case CC_OP_TRIG: {
-      const T* q = p + op.poff;
+      T q[8];
+      ldq(b, q);
+      if (D == 3) ldq(b + 4, q + 4);
       S s = q[0] * dsin(q[1] * x[0]);
 #pragma unroll
       for (int a = 1; a < D; ++a) s = s * dsin(q[1 + a] * x[a]);
       return s + q[1 + D];
     }
     case CC_OP_CONST:
-      return Lift<S, T>::c(p[op.poff]);
+      return Lift<S, T>::c(b[0]);
     case CC_OP_STAR:
       if constexpr (D == 2) {
-        const T* q = p + op.poff;
+        T q[16];
+        ldq(b, q); ldq(b + 4, q + 4); ldq(b + 8, q + 8); ldq(b + 12, q + 12);
         const S dx = x[0] - q[0], dy = x[1] - q[1];
         const S rad = dsqrt(dx * dx + dy * dy);
         const S th = datan2(dy, dx);
@@ -271,18 +291,171 @@ __device__ __forceinline__ S tape_eval(const STape<T>& t, const S* x) {
   return acc;
 }
 
-// Copy a tape (ops then params, already narrowed to T) from global into shared memory.
+// Op-major evaluation of one tape at NB points at once (scalar T only): each op's dispatch and
+// parameter loads are paid once for all NB points, and the NB dependency chains interleave.
+// Per point the arithmetic is exactly tape_eval's, in the same order.
+template <class T, int D, int NB>
+__device__ __forceinline__ void tape_prim_multi(const cc_op op, const T* __restrict__ p, const T (&x)[NB][D], T (&v)[NB]) {
+  const T* b = p + op.poff;
+  switch (op.opcode) {
+    case CC_OP_SPHERE: {
+      T c[4];
+      ldq(b, c);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        T u = (x[q][0] - c[0]) * (x[q][0] - c[0]);
+#pragma unroll
+        for (int a = 1; a < D; ++a) u = u + (x[q][a] - c[a]) * (x[q][a] - c[a]);
+        v[q] = dsqrt(u) - c[D];
+      }
+      return;
+    }
+    case CC_OP_BOX: {
+      T c[8];
+      ldq(b, c);
+      if (D == 3) ldq(b + 4, c + 4);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        T qq[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) qq[a] = dabs(x[q][a] - c[a]) - c[D + a];
+        T qa = qq[0] > T(0) ? qq[0] : T(0);
+        T u = qa * qa;
+#pragma unroll
+        for (int a = 1; a < D; ++a) { qa = qq[a] > T(0) ? qq[a] : T(0); u = u + qa * qa; }
+        const T outside = dsqrt(u);
+        T m = qq[0];
+#pragma unroll
+        for (int a = 1; a < D; ++a) m = qq[a] > m ? qq[a] : m;
+        const T inside = m < T(0) ? m : T(0);
+        v[q] = outside + inside;
+      }
+      return;
+    }
+    case CC_OP_TORUS:
+      if constexpr (D == 3) {
+        T c[16];
+        ldq(b, c); ldq(b + 4, c + 4); ldq(b + 8, c + 8); ldq(b + 12, c + 12);
+        const T* R = c + 3;
+#pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          const T d0 = x[q][0] - c[0], d1 = x[q][1] - c[1], d2 = x[q][2] - c[2];
+          const T l0 = R[0] * d0 + R[1] * d1 + R[2] * d2;
+          const T l1 = R[3] * d0 + R[4] * d1 + R[5] * d2;
+          const T l2 = R[6] * d0 + R[7] * d1 + R[8] * d2;
+          const T qx = dsqrt(l0 * l0 + l1 * l1) - c[12];
+          v[q] = dsqrt(qx * qx + l2 * l2) - c[13];
+        }
+        return;
+      }
+      break;
+    case CC_OP_PLANE: {
+      T c[8];
+      ldq(b, c);
+      if (D == 3) ldq(b + 4, c + 4);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        T s = c[D] * (x[q][0] - c[0]);
+#pragma unroll
+        for (int a = 1; a < D; ++a) s = s + c[D + a] * (x[q][a] - c[a]);
+        v[q] = s;
+      }
+      return;
+    }
+    case CC_OP_TRIG: {
+      T c[8];
+      ldq(b, c);
+      if (D == 3) ldq(b + 4, c + 4);
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        T s = c[0] * dsin(c[1] * x[q][0]);
+#pragma unroll
+        for (int a = 1; a < D; ++a) s = s * dsin(c[1 + a] * x[q][a]);
+        v[q] = s + c[1 + D];
+      }
+      return;
+    }
+    case CC_OP_CONST: {
+      const T c = b[0];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) v[q] = c;
+      return;
+    }
+    default:
+      break;
+  }
+  // primitives without a multi-point form (and invalid opcodes) fall back point by point
+#pragma unroll
+  for (int q = 0; q < NB; ++q) v[q] = tape_prim<T, D, T>(op, p, x[q]);
+}
+
+template <class T, int D, int NB>
+__device__ __forceinline__ void tape_eval_multi(const STape<T>& t, const T (&x)[NB][D], T (&out)[NB]) {
+  T acc[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) acc[q] = T(0);
+  T st[CC_TAPE_MAX_STACK][NB];
+  int sp = 0;
+  bool have = false;
+  for (int i = 0; i < t.n_ops; ++i) {
+    const cc_op op = t.ops[i];
+    T v[NB];
+    if (op.opcode == CC_OP_NONE) {
+      if (op.combine == CC_COMB_NEG) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q) acc[q] = -acc[q];
+        continue;
+      }
+      --sp;
+#pragma unroll
+      for (int q = 0; q < NB; ++q) { v[q] = acc[q]; acc[q] = st[sp][q]; }
+    } else {
+      tape_prim_multi<T, D, NB>(op, t.p, x, v);
+    }
+    switch (op.combine) {
+      case CC_COMB_PUSH:
+        if (have) {
+#pragma unroll
+          for (int q = 0; q < NB; ++q) st[sp][q] = acc[q];
+          ++sp;
+        }
+#pragma unroll
+        for (int q = 0; q < NB; ++q) acc[q] = v[q];
+        have = true;
+        break;
+      case CC_COMB_MIN:
+#pragma unroll
+        for (int q = 0; q < NB; ++q) acc[q] = v[q] < acc[q] ? v[q] : acc[q];
+        break;
+      case CC_COMB_MAX:
+#pragma unroll
+        for (int q = 0; q < NB; ++q) acc[q] = v[q] > acc[q] ? v[q] : acc[q];
+        break;
+      default: {
+        const T k = op.combine == CC_COMB_SMIN ? t.p[op.kparam] : T(0);
+#pragma unroll
+        for (int q = 0; q < NB; ++q) acc[q] = tape_combine<T, T>(op.combine, acc[q], v[q], k);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) out[q] = acc[q];
+}
+
+// Copy a packed tape (ops, padded to 16 bytes, then the parameter blocks narrowed to T, each
+// starting on a 4-element boundary) from global into shared memory.
+__host__ __device__ __forceinline__ int tape_ops_bytes(int n_ops) { return ((n_ops * int(sizeof(cc_op)) + 15) / 16) * 16; }
 template <class T>
 __device__ __forceinline__ STape<T> load_tape(const unsigned char* __restrict__ gtape, int n_ops, int n_params,
                                               unsigned char* smem) {
-  const int bytes = n_ops * int(sizeof(cc_op)) + n_params * int(sizeof(T));
+  const int bytes = tape_ops_bytes(n_ops) + n_params * int(sizeof(T));
   const int words = (bytes + 7) / 8;
   const unsigned long long* src = reinterpret_cast<const unsigned long long*>(gtape);
   unsigned long long* dst = reinterpret_cast<unsigned long long*>(smem);
   for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = __ldg(src + w);
   STape<T> t;
   t.ops = reinterpret_cast<const cc_op*>(smem);
-  t.p = reinterpret_cast<const T*>(smem + ((n_ops * sizeof(cc_op) + 7) / 8) * 8);
+  t.p = reinterpret_cast<const T*>(smem + tape_ops_bytes(n_ops));
   t.n_ops = n_ops;
   return t;
 }

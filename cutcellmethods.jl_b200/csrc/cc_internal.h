@@ -42,9 +42,12 @@ struct Cols {
 
 // Marching cubes: sample (if phi_in == nullptr: sample from the tape into phi_out) and build
 // every cell. Returns the CUDA launch status.
+// `cut_list` (one slot per cell) and `cut_count` are scratch: the fill pass lists the cut band
+// there and the cut pass reads it back.
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
-                      const Cols& cols, const DevTable& tb, cudaStream_t s);
+                      const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
+                      cudaStream_t s);
 
 template <class T>
 cudaError_t launch_ms(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,

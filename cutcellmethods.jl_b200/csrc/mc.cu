@@ -1,20 +1,23 @@
 // mc.cu -- MarchingCubesCutCell update_cache! on sm_100a.
 //
-// One fused kernel replaces the reference's two KernelAbstractions launches
+// Two kernels replace the reference's two KernelAbstractions launches
 // (_sample_nodes_kernel! and _nodal_cells_kernel!, src/marching_squares/cache.jl:55-78):
 //
-//   * A CTA owns a pencil of 64 x 4 cells in (x, y) and marches KZ slices along z. Each slice it
-//     samples one new slab of 65 x 5 node values from the op-tape into shared memory (the slab
-//     below is kept from the previous slice), so a node is evaluated once per CTA and written
-//     to phi once, by the CTA that owns it.
-//   * Every thread classifies one cell from its eight corners. Uncut cells (all corners of one
-//     sign) get their fields directly: their face centroids are half the lattice edge lengths, a
-//     cheap affine fill. Cut cells are compacted with a warp ballot into a per-CTA queue and
-//     processed densely, one lane per cut cell, by the full construction of
-//     src/marching_cubes/moments.jl:275-346.
-//   * Results are staged per column in shared memory and leave as coalesced 16-byte stores of
-//     contiguous row spans of each StructArray column.
+//   * mc_fill_kernel: a CTA owns a pencil of TX x 4 cells in (x, y) and marches KZ slices along
+//     z. Each slice it samples one new slab of (TX+1) x 5 node values from the op-tape into shared
+//     memory (the slab below is kept from the previous slice), so a node is evaluated once per
+//     CTA and written to phi once, by the CTA that owns it. Every thread classifies one cell from
+//     its eight corners. Uncut cells (all corners of one sign) get their fields directly -- their
+//     face centroids are half the lattice edge lengths, a cheap affine fill -- into a
+//     double-buffered shared-memory staging tile that leaves as contiguous row spans of each
+//     StructArray column through the TMA bulk-copy engine (cp.async.bulk, shared -> global), so
+//     the SM's threads never issue the column stores. Cut cells are compacted with a warp ballot
+//     into a global work list.
+//   * mc_cut_kernel: one lane per listed cut cell runs the full construction of
+//     src/marching_cubes/moments.jl:275-346 densely and writes that cell's fields.
 #include <cstdint>
+#include <cstring>
+#include <cuda.h>
 #include "cc_device.cuh"
 #include "cc_internal.h"
 
@@ -26,13 +29,20 @@ using cci::DevGrid;
 using cci::DevTable;
 using cci::DevTape;
 
-constexpr int TX = 64;
-constexpr int TY = 4;
-constexpr int NT = TX * TY;  // threads per CTA, one cell each
-constexpr int NSX = TX + 1;
-constexpr int NSY = TY + 1;
-constexpr int NSLAB = NSX * NSY;
-constexpr int KZ = 16;  // z slices marched per CTA
+// Fill-kernel tile: TX cells along x (32 at Float32, 16 at Float64, so a staging buffer is about
+// 26 KB either way) by TY = 8 rows, one thread per cell, marching KZ slices along z. A slab of
+// (TX+1) x (TY+1) nodes serves TX x TY cells: 1.16 node evaluations per cell at Float32.
+template <class T> struct Tile {
+  static constexpr int TX = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int TY = 8;
+  static constexpr int NT = TX * TY;
+  static constexpr int NSX = TX + 1;
+  static constexpr int NSLAB = (TX + 1) * (TY + 1);
+  static constexpr int MINB = sizeof(T) == 4 ? 3 : 4;
+};
+constexpr int KZ = 32;  // z slices marched per CTA
+constexpr int NS = 4;   // node slabs sampled per round (one op-major tape pass per thread)
+constexpr int CUT_NT = 128;
 
 // MC_NODE_BITS (src/marching_cubes/marching_cubes.jl:106-107), bit of corner c along axis a.
 __host__ __device__ constexpr int cbit(int c, int a) {
@@ -212,7 +222,7 @@ __device__ __forceinline__ void put_vec<double>(double* dst, const double* v, in
 }
 
 template <class T>
-__device__ __forceinline__ void put_cell(const Stage<T>& st, int lc, int kind, int amb, T vf, const T c[3],
+__device__ __forceinline__ void put_cell(const Stage<T>& st, long long lc, int kind, int amb, T vf, const T c[3],
                                          const T ff[6], const T fcl[12], const T ic[3]) {
   st.kind[lc] = int8_t(kind);
   st.amb[lc] = uint8_t(amb);
@@ -229,7 +239,7 @@ __device__ __forceinline__ void put_cell(const Stage<T>& st, int lc, int kind, i
 // lower corner and `cs` the grid's cell size.
 template <class T>
 __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T org[3], const T cs[3],
-                                         const DevTable tb, const Stage<T> st, int lc) {
+                                         const DevTable tb, const Stage<T> st, long long lc) {
   T phi[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) phi[k] = nudge(phr[k]);
@@ -394,42 +404,100 @@ struct McArgs {
   T* phi_out;
   Cols cols;
   DevTable tb;
+  unsigned* cut_list;
+  unsigned* cut_count;
   int n_itiles, n_jtiles;
+  int use_tma;  // output columns leave through TMA tensor stores (maps below are valid)
 };
 
-// Shared-memory byte layout of one CTA.
+// One TMA tensor map per output column: kind, ambiguous, volume_fraction (n0 x n1 x n2), centroid
+// and interface_centroid (3 n0 x n1 x n2), face_fraction (6 n0 x n1 x n2), face_centroid_local
+// (12 x n0 x n1 x n2). A staged tile is exactly one box of each.
+struct ColumnMaps {
+  CUtensorMap m[7];
+};
+
+// TMA bulk copy engine, shared -> global (cp.async.bulk, sm_90+), and its group bookkeeping.
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst),
+               "r"((unsigned)__cvta_generic_to_shared(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read %0;\n" ::"n"(N) : "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_store3(const CUtensorMap* m, const void* ssrc, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(m),
+               "r"((unsigned)__cvta_generic_to_shared(ssrc)), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+__device__ __forceinline__ void tma_store4(const CUtensorMap* m, const void* ssrc, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];\n" ::"l"(m),
+               "r"((unsigned)__cvta_generic_to_shared(ssrc)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+
+// Shared-memory byte layout of one fill CTA: two staging buffers, two node slabs, the tape.
 template <class T>
 struct Layout {
+  using TL = Tile<T>;
+  static constexpr int NC = TL::NT;  // cells per staging buffer
   static constexpr int kind = 0;
-  static constexpr int amb = kind + NT;
-  static constexpr int vf = amb + NT;
-  static constexpr int c = vf + NT * int(sizeof(T));
-  static constexpr int ff = c + 3 * NT * int(sizeof(T));
-  static constexpr int fcl = ff + 6 * NT * int(sizeof(T));
-  static constexpr int ic = fcl + 12 * NT * int(sizeof(T));
-  static constexpr int stage_end = ic + 3 * NT * int(sizeof(T));
-  static constexpr int slab0 = stage_end;
-  static constexpr int slab1 = slab0 + ((NSLAB * int(sizeof(T)) + 15) / 16) * 16;
-  static constexpr int queue = slab1 + ((NSLAB * int(sizeof(T)) + 15) / 16) * 16;
-  static constexpr int counter = queue + NT * 2;
-  static constexpr int tape = ((counter + 4 + 15) / 16) * 16;
+  static constexpr int amb = kind + NC;
+  static constexpr int vf = amb + NC;
+  static constexpr int c = vf + NC * int(sizeof(T));
+  static constexpr int ff = c + 3 * NC * int(sizeof(T));
+  static constexpr int fcl = ff + 6 * NC * int(sizeof(T));
+  static constexpr int ic = fcl + 12 * NC * int(sizeof(T));
+  static constexpr int stage_bytes = ((ic + 3 * NC * int(sizeof(T)) + 127) / 128) * 128;
+  static constexpr int slab_bytes = ((TL::NSLAB * int(sizeof(T)) + 15) / 16) * 16;
+  static constexpr int slab0 = 2 * stage_bytes;
+  static constexpr int tape = slab0 + (NS + 1) * slab_bytes;
+  // TMA tensor stores read each staged column from a 128-byte aligned base
+  static_assert(amb % 128 == 0 && vf % 128 == 0 && c % 128 == 0 && ff % 128 == 0 && fcl % 128 == 0 &&
+                    ic % 128 == 0 && stage_bytes % 128 == 0,
+                "staged columns must start on 128-byte boundaries");
 };
 
 // bytes per staged row of output column `col` (kind, amb, vf, c, ff, fcl, ic) and its offset
 template <class T>
 __device__ __forceinline__ constexpr int col_bytes(int col) {
-  return col < 2 ? TX : (col == 2 ? 1 : col == 3 ? 3 : col == 4 ? 6 : col == 5 ? 12 : 3) * TX * int(sizeof(T));
+  return col < 2 ? Tile<T>::TX
+                 : (col == 2 ? 1 : col == 3 ? 3 : col == 4 ? 6 : col == 5 ? 12 : 3) * Tile<T>::TX * int(sizeof(T));
 }
 template <class T>
 __device__ __forceinline__ constexpr int col_offset(int col) {
   return col == 0 ? Layout<T>::kind : col == 1 ? Layout<T>::amb : col == 2 ? Layout<T>::vf : col == 3 ? Layout<T>::c
        : col == 4 ? Layout<T>::ff : col == 5 ? Layout<T>::fcl : Layout<T>::ic;
 }
+__device__ __forceinline__ constexpr int col_elem(int col, int tsize) {
+  return col < 2 ? 1 : (col == 2 ? 1 : col == 3 ? 3 : col == 4 ? 6 : col == 5 ? 12 : 3) * tsize;
+}
+
+template <class T>
+__device__ __forceinline__ Stage<T> stage_at(unsigned char* base) {
+  using L = Layout<T>;
+  Stage<T> st;
+  st.kind = reinterpret_cast<int8_t*>(base + L::kind);
+  st.amb = base + L::amb;
+  st.vf = reinterpret_cast<T*>(base + L::vf);
+  st.c = reinterpret_cast<T*>(base + L::c);
+  st.ff = reinterpret_cast<T*>(base + L::ff);
+  st.fcl = reinterpret_cast<T*>(base + L::fcl);
+  st.ic = reinterpret_cast<T*>(base + L::ic);
+  return st;
+}
 
 template <class T, bool SAMPLE>
-__global__ void __launch_bounds__(NT, 2) mc_kernel(const McArgs<T> A) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
+                                                                            const __grid_constant__ ColumnMaps maps) {
+  using TL = Tile<T>;
   using L = Layout<T>;
+  constexpr int TX = TL::TX, TY = TL::TY, NT = TL::NT, NSX = TL::NSX, NSLAB = TL::NSLAB;
+  extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x;
   const long long n0 = A.g.n[0], n1 = A.g.n[1], n2 = A.g.n[2];
   const long long nx = n0 + 1, ny = n1 + 1;
@@ -443,157 +511,201 @@ __global__ void __launch_bounds__(NT, 2) mc_kernel(const McArgs<T> A) {
 
   STape<T> tape;
   if (SAMPLE) tape = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem + L::tape);
-  T* slab[2] = {reinterpret_cast<T*>(smem + L::slab0), reinterpret_cast<T*>(smem + L::slab1)};
-  uint16_t* queue = reinterpret_cast<uint16_t*>(smem + L::queue);
-  int* qcount = reinterpret_cast<int*>(smem + L::counter);
-  Stage<T> st;
-  st.kind = reinterpret_cast<int8_t*>(smem + L::kind);
-  st.amb = smem + L::amb;
-  st.vf = reinterpret_cast<T*>(smem + L::vf);
-  st.c = reinterpret_cast<T*>(smem + L::c);
-  st.ff = reinterpret_cast<T*>(smem + L::ff);
-  st.fcl = reinterpret_cast<T*>(smem + L::fcl);
-  st.ic = reinterpret_cast<T*>(smem + L::ic);
-  if (tid == 0) *qcount = 0;
-  __syncthreads();
+  T* const ring = reinterpret_cast<T*>(smem + L::slab0);
+  constexpr int RS = L::slab_bytes / int(sizeof(T));  // ring slot stride, elements
+  if (SAMPLE) __syncthreads();
 
   const T x0 = A.g.x0[0], y0 = A.g.x0[1], z0 = A.g.x0[2];
   const T dx = A.g.d[0], dy = A.g.d[1], dz = A.g.d[2];
+  const long long nxy = nx * ny;
 
-  // Sample (or load) node slab z into buffer `buf`, writing phi for the nodes this CTA owns.
-  auto fill_slab = [&](long long z, int buf, bool own_slab) {
-    T* s = slab[buf];
-    const T zc = node_coord(z0, dz, z);
-    for (int v = tid; v < NSLAB; v += NT) {
-      const int tx = v % NSX, ty = v / NSX;
-      const long long i = i0 + tx, j = j0 + ty;
-      if (i > n0 || j > n1) continue;
-      const long long gi = i + nx * (j + ny * z);
-      T val;
+  // This thread's node slots for one sampling round of NS slabs, fixed for the whole march:
+  // which of the round's slabs, the slab index, coordinates, the node index in the z = 0 plane,
+  // and whether this CTA owns (writes) the node.
+  constexpr int NSL = (NS * NSLAB + NT - 1) / NT;
+  int sl_s[NSL], sl_v[NSL];
+  T sl_x[NSL], sl_y[NSL];
+  long long sl_g[NSL];
+  bool sl_ok[NSL], sl_own[NSL];
+#pragma unroll
+  for (int q = 0; q < NSL; ++q) {
+    const int flat = tid + q * NT;
+    const int s = flat / NSLAB, v = flat - s * NSLAB;
+    const int tx = v % NSX, ty = v / NSX;
+    const long long i = i0 + tx, j = j0 + ty;
+    sl_s[q] = s;
+    sl_v[q] = v;
+    sl_ok[q] = s < NS && i <= n0 && j <= n1;
+    sl_own[q] = (tx < TX || i == n0) && (ty < TY || j == n1);
+    sl_x[q] = node_coord(x0, dx, i);
+    sl_y[q] = node_coord(y0, dy, j);
+    sl_g[q] = i + nx * j;
+  }
+
+  // One round: slabs zbase, zbase+1, ... (slot s samples slab zbase + s, for slabs <= zlast),
+  // into ring slot z % (NS + 1); phi written for owned nodes of owned slabs. `first` samples
+  // only slab zbase (the first slab of the march).
+  auto sample_round = [&](long long zbase, long long zlast, bool first) {
+    T pts[NSL][3];
+    T val[NSL];
+    bool use[NSL];
+#pragma unroll
+    for (int q = 0; q < NSL; ++q) {
+      const long long z = zbase + sl_s[q];
+      use[q] = sl_ok[q] && z <= zlast && (!first || sl_s[q] == 0);
+      pts[q][0] = sl_x[q];
+      pts[q][1] = sl_y[q];
+      pts[q][2] = node_coord(z0, dz, (long long)(int)z);
+    }
+    if (SAMPLE) {
+      tape_eval_multi<T, 3, NSL>(tape, pts, val);
+    }
+#pragma unroll
+    for (int q = 0; q < NSL; ++q) {
+      if (!use[q]) continue;
+      const long long z = zbase + sl_s[q];
+      const long long gi = sl_g[q] + nxy * z;
+      T v;
       if (SAMPLE) {
-        T xyz[3] = {node_coord(x0, dx, i), node_coord(y0, dy, j), zc};
-        val = tape_eval<T, 3, T>(tape, xyz);
-        const bool own = own_slab && (tx < TX || i == n0) && (ty < TY || j == n1);
-        if (own) A.phi_out[gi] = val;
+        v = val[q];
+        const bool own_slab = z < k1 || z == n2;
+        if (own_slab && sl_own[q]) A.phi_out[gi] = v;
       } else {
-        val = A.phi_in[gi];
+        v = A.phi_in[gi];
       }
-      s[v] = val;
+      ring[(int)(z - k0) % (NS + 1) * RS + sl_v[q]] = v;
     }
   };
 
-  fill_slab(k0, k0 & 1, true);
+  sample_round(k0, k0, true);
 
   const int tx = tid % TX, ty = tid / TX;
   const long long ci = i0 + tx, cj = j0 + ty;
   const bool valid = ci < n0 && cj < n1;
-  // this thread's cell's lattice data, constant along z except for the z axis
   const T xa = node_coord(x0, dx, ci), xb = node_coord(x0, dx, ci + 1);
   const T ya = node_coord(y0, dy, cj), yb = node_coord(y0, dy, cj + 1);
-  const T lx = xb - xa, ly = yb - ya;
-  const T hx = T(0.5) * lx, hy = T(0.5) * ly;
+  const T hx = T(0.5) * (xb - xa), hy = T(0.5) * (yb - ya);
+  const T cx = xa + T(0.5) * dx, cy = ya + T(0.5) * dy;
   const int lc = ty * TX + tx;
   const int s00 = ty * NSX + tx;
-  const bool fast_store = (i0 + TX <= n0) && (n0 % 16 == 0);
+  const bool fast = A.use_tma != 0;
   const int rows = (int)((n1 - j0) < TY ? (n1 - j0) : TY);
   const int cnt = (int)((n0 - i0) < TX ? (n0 - i0) : TX);
+  unsigned char* gcol[7] = {reinterpret_cast<unsigned char*>(A.cols.kind), A.cols.amb,
+                            reinterpret_cast<unsigned char*>(A.cols.vf), reinterpret_cast<unsigned char*>(A.cols.c),
+                            reinterpret_cast<unsigned char*>(A.cols.ff), reinterpret_cast<unsigned char*>(A.cols.fcl),
+                            reinterpret_cast<unsigned char*>(A.cols.ic)};
 
   for (long long k = k0; k < k1; ++k) {
-    const int cur = k & 1;
-    fill_slab(k + 1, cur ^ 1, k + 1 < k1 || k + 1 == n2);
-    __syncthreads();  // slabs k and k+1 ready; staging free
+    const int sb = (int)((k - k0) & 1);
+    unsigned char* sbase = smem + sb * L::stage_bytes;
+    if (((k - k0) % NS) == 0) sample_round(k + 1, k1, false);
+    if (fast && tid == 0) bulk_wait_read<1>();  // staging buffer sb: its copy two slices ago has been read
+    __syncthreads();  // slabs k and k+1 ready; staging sb free
 
-    const T za = node_coord(z0, dz, k), zb = node_coord(z0, dz, k + 1);
+    const T za = node_coord(z0, dz, (long long)(int)k), zb = node_coord(z0, dz, (long long)(int)(k + 1));
     bool is_cut = false;
     if (valid) {
-      const T* sa = slab[cur];
-      const T* sb = slab[cur ^ 1];
-      T ph[8] = {sa[s00], sa[s00 + 1], sa[s00 + NSX + 1], sa[s00 + NSX],
-                 sb[s00], sb[s00 + 1], sb[s00 + NSX + 1], sb[s00 + NSX]};
+      const int rk = (int)(k - k0) % (NS + 1);
+      const T* sa = ring + rk * RS;
+      const T* sbb = ring + (rk == NS ? 0 : rk + 1) * RS;
+      const T ph[8] = {sa[s00], sa[s00 + 1], sa[s00 + NSX + 1], sa[s00 + NSX],
+                       sbb[s00], sbb[s00 + 1], sbb[s00 + NSX + 1], sbb[s00 + NSX]};
+      // nudge_zeros(v) >= 0  <=>  v > -eps  (and false for NaN, as there)
+      const T neps = -Eps<T>::v();
       int nout = 0;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) nout += nudge(ph[q]) >= T(0) ? 1 : 0;
+      for (int q = 0; q < 8; ++q) nout += ph[q] > neps ? 1 : 0;
       if (nout == 0 || nout == 8) {
-        const T lz = zb - za;
-        const T hz = T(0.5) * lz;
+        const T hz = T(0.5) * (zb - za);
         const T one = nout == 8 ? T(1) : T(0);
-        const T cen[3] = {xa + T(0.5) * dx, ya + T(0.5) * dy, za + T(0.5) * dz};
+        const T cen[3] = {cx, cy, za + T(0.5) * dz};
         const T ff[6] = {one, one, one, one, one, one};
         const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
-        put_cell<T>(st, lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+        put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
       } else {
         is_cut = true;
       }
     }
-    // warp-ballot compaction of the cut band into the CTA queue
+    // Warp-ballot compaction of the cut band into the global work list. A cut cell's staged slot
+    // is left as it is: the span is copied out whole and the cut kernel, which runs after this
+    // one in stream order, overwrites the cell.
     const unsigned m = __ballot_sync(0xffffffffu, is_cut);
     if (m) {
       const int lane = tid & 31;
-      int base = 0;
-      if (lane == 0) base = atomicAdd(qcount, __popc(m));
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(A.cut_count, (unsigned)__popc(m));
       base = __shfl_sync(0xffffffffu, base, 0);
-      if (is_cut) queue[base + __popc(m & ((1u << lane) - 1))] = uint16_t(lc);
+      if (is_cut) A.cut_list[base + __popc(m & ((1u << lane) - 1))] = (unsigned)(ci + n0 * (cj + n1 * k));
     }
-    __syncthreads();  // queue complete
+    if (fast) fence_proxy_async_smem();  // staged writes visible to the bulk-copy engine
+    __syncthreads();  // staging sb complete
 
-    const int nq = *qcount;
-    for (int qi = tid; qi < nq; qi += NT) {
-      const int c = queue[qi];
-      const int qx = c % TX, qy = c / TX;
-      const int s0 = qy * NSX + qx;
-      const T* sa = slab[cur];
-      const T* sb = slab[cur ^ 1];
-      const T ph[8] = {sa[s0], sa[s0 + 1], sa[s0 + NSX + 1], sa[s0 + NSX],
-                       sb[s0], sb[s0 + 1], sb[s0 + NSX + 1], sb[s0 + NSX]};
-      const long long gi = i0 + qx, gj = j0 + qy;
-      const T org[3] = {node_coord(x0, dx, gi), node_coord(y0, dy, gj), za};
-      const T l[3] = {node_coord(x0, dx, gi + 1) - org[0], node_coord(y0, dy, gj + 1) - org[1], zb - za};
-      const T cs[3] = {dx, dy, dz};
-      mc_cut_cell<T>(ph, l, org, cs, A.tb, st, c);
-    }
-    __syncthreads();  // staging complete
-    if (tid == 0) *qcount = 0;
-
-    // stream the staged rows out
     const long long row0 = i0 + n0 * (j0 + n1 * k);
-    unsigned char* gcol[7] = {reinterpret_cast<unsigned char*>(A.cols.kind), A.cols.amb,
-                              reinterpret_cast<unsigned char*>(A.cols.vf), reinterpret_cast<unsigned char*>(A.cols.c),
-                              reinterpret_cast<unsigned char*>(A.cols.ff), reinterpret_cast<unsigned char*>(A.cols.fcl),
-                              reinterpret_cast<unsigned char*>(A.cols.ic)};
-    const int esz[7] = {1, 1, int(sizeof(T)), 3 * int(sizeof(T)), 6 * int(sizeof(T)), 12 * int(sizeof(T)), 3 * int(sizeof(T))};
-    if (fast_store) {
-#pragma unroll
-      for (int col = 0; col < 7; ++col) {
-        const int rb = col_bytes<T>(col);
-        const int chunks = rb / 16;
-        const int total = rows * chunks;
-        for (int v = tid; v < total; v += NT) {
-          const int r = v / chunks;
-          const int w = (v - r * chunks) * 16;
-          const uint4 val = *reinterpret_cast<const uint4*>(smem + col_offset<T>(col) + r * rb + w);
-          unsigned char* dst = gcol[col] + (row0 + (long long)r * n0) * esz[col] + w;
-          *reinterpret_cast<uint4*>(dst) = val;
-        }
+    if (fast) {
+      // one thread stores the staged tile: one TMA box per column (the hardware clips the box
+      // at the grid's edge)
+      if (tid == 0) {
+        const int ci0 = (int)i0, cj0 = (int)j0, ck = (int)k;
+        tma_store3(&maps.m[0], sbase + col_offset<T>(0), ci0, cj0, ck);
+        tma_store3(&maps.m[1], sbase + col_offset<T>(1), ci0, cj0, ck);
+        tma_store3(&maps.m[2], sbase + col_offset<T>(2), ci0, cj0, ck);
+        tma_store3(&maps.m[3], sbase + col_offset<T>(3), 3 * ci0, cj0, ck);
+        tma_store3(&maps.m[4], sbase + col_offset<T>(4), 6 * ci0, cj0, ck);
+        tma_store4(&maps.m[5], sbase + col_offset<T>(5), 0, ci0, cj0, ck);
+        tma_store3(&maps.m[6], sbase + col_offset<T>(6), 3 * ci0, cj0, ck);
+        bulk_commit();
       }
     } else {
       for (int r = 0; r < rows; ++r) {
         const long long rowc = row0 + (long long)r * n0;
 #pragma unroll
         for (int col = 0; col < 7; ++col) {
-          const int nb = cnt * esz[col];
-          const unsigned char* src = smem + col_offset<T>(col) + r * col_bytes<T>(col);
-          unsigned char* dst = gcol[col] + rowc * esz[col];
+          const int es = col_elem(col, int(sizeof(T)));
+          const unsigned char* src = sbase + col_offset<T>(col) + r * col_bytes<T>(col);
+          unsigned char* dst = gcol[col] + rowc * es;
           if (col >= 2) {
-            // T-sized elements: the column is T-aligned
-            const T* s = reinterpret_cast<const T*>(src);
-            T* d = reinterpret_cast<T*>(dst);
-            for (int v = tid; v < nb / int(sizeof(T)); v += NT) d[v] = s[v];
+            const T* s2 = reinterpret_cast<const T*>(src);
+            T* d2 = reinterpret_cast<T*>(dst);
+            const int ne = cnt * es / int(sizeof(T));
+            for (int v = tid; v < ne; v += NT) d2[v] = s2[v];
           } else {
-            for (int v = tid; v < nb; v += NT) dst[v] = src[v];
+            for (int v = tid; v < cnt; v += NT) dst[v] = src[v];
           }
         }
       }
     }
+  }
+  if (fast && tid == 0) bulk_wait<0>();  // all tensor stores complete before the CTA retires
+}
+
+template <class T, bool SAMPLE>
+__global__ void __launch_bounds__(CUT_NT) mc_cut_kernel(const McArgs<T> A) {
+  const long long n0 = A.g.n[0], n1 = A.g.n[1];
+  const long long nx = n0 + 1, ny = n1 + 1;
+  const T* phi = SAMPLE ? A.phi_out : A.phi_in;
+  Stage<T> st;
+  st.kind = A.cols.kind;
+  st.amb = A.cols.amb;
+  st.vf = static_cast<T*>(A.cols.vf);
+  st.c = static_cast<T*>(A.cols.c);
+  st.ff = static_cast<T*>(A.cols.ff);
+  st.fcl = static_cast<T*>(A.cols.fcl);
+  st.ic = static_cast<T*>(A.cols.ic);
+  const T cs[3] = {A.g.d[0], A.g.d[1], A.g.d[2]};
+  const unsigned total = *A.cut_count;
+  for (unsigned q = blockIdx.x * CUT_NT + threadIdx.x; q < total; q += gridDim.x * CUT_NT) {
+    const long long ci = A.cut_list[q];
+    const long long i = ci % n0, j = (ci / n0) % n1, k = ci / (n0 * n1);
+    const long long b0 = i + nx * (j + ny * k);
+    const long long bz = nx * ny;
+    const T ph[8] = {phi[b0], phi[b0 + 1], phi[b0 + nx + 1], phi[b0 + nx],
+                     phi[b0 + bz], phi[b0 + bz + 1], phi[b0 + bz + nx + 1], phi[b0 + bz + nx]};
+    const T org[3] = {node_coord(A.g.x0[0], A.g.d[0], i), node_coord(A.g.x0[1], A.g.d[1], j),
+                      node_coord(A.g.x0[2], A.g.d[2], k)};
+    const T l[3] = {node_coord(A.g.x0[0], A.g.d[0], i + 1) - org[0], node_coord(A.g.x0[1], A.g.d[1], j + 1) - org[1],
+                    node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
+    mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
   }
 }
 
@@ -604,11 +716,75 @@ constexpr int smem_bytes(int tape_bytes) {
 
 }  // namespace
 
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// The seven column maps of a marching-cubes cache, or false where TMA cannot address the columns
+// (a row of the kind column is not a multiple of 16 bytes, a base not 16-byte aligned, or a
+// dimension past 2^31); the fill kernel then stores with its threads.
+template <class T>
+bool make_column_maps(const DevGrid<T>& g, const Cols& cols, ColumnMaps* maps) {
+  using TL = Tile<T>;
+  const long long n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  if (n0 % 16 != 0 || 12 * n0 >= 0x7fffffffLL || n1 >= 0x7fffffffLL || n2 >= 0x7fffffffLL) return false;
+  void* base[7] = {cols.kind, cols.amb, cols.vf, cols.c, cols.ff, cols.fcl, cols.ic};
+  for (void* b : base)
+    if (reinterpret_cast<uintptr_t>(b) & 15u) return false;
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  const CUtensorMapDataType tt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const cuuint64_t es = sizeof(T);
+  const int width[7] = {1, 1, 1, 3, 6, 12, 3};
+  for (int c = 0; c < 7; ++c) {
+    const CUtensorMapDataType dt = c < 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : tt;
+    const cuuint64_t e = c < 2 ? 1 : es;
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r;
+    if (c == 5) {
+      const cuuint64_t dims[4] = {12, (cuuint64_t)n0, (cuuint64_t)n1, (cuuint64_t)n2};
+      const cuuint64_t strides[3] = {12 * e, 12 * e * n0, 12 * e * n0 * n1};
+      const cuuint32_t box[4] = {12, (cuuint32_t)TL::TX, (cuuint32_t)TL::TY, 1};
+      r = enc(&maps->m[c], dt, 4, base[c], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+      const cuuint64_t w = width[c];
+      const cuuint64_t dims[3] = {w * n0, (cuuint64_t)n1, (cuuint64_t)n2};
+      const cuuint64_t strides[2] = {w * e * n0, w * e * n0 * n1};
+      const cuuint32_t box[3] = {(cuuint32_t)(w * TL::TX), (cuuint32_t)TL::TY, 1};
+      r = enc(&maps->m[c], dt, 3, base[c], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    if (r != CUDA_SUCCESS) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
 namespace cci {
 
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
-                      const Cols& cols, const DevTable& tb, cudaStream_t s) {
+                      const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
+                      cudaStream_t s) {
+  using TL = Tile<T>;
   McArgs<T> a;
   a.g = g;
   a.tape = tape;
@@ -616,29 +792,38 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   a.phi_out = phi_out;
   a.cols = cols;
   a.tb = tb;
-  a.n_itiles = int((g.n[0] + TX - 1) / TX);
-  a.n_jtiles = int((g.n[1] + TY - 1) / TY);
+  a.cut_list = cut_list;
+  a.cut_count = cut_count;
+  ColumnMaps maps;
+  std::memset(&maps, 0, sizeof maps);
+  a.use_tma = make_column_maps<T>(g, cols, &maps) ? 1 : 0;
+  a.n_itiles = int((g.n[0] + TL::TX - 1) / TL::TX);
+  a.n_jtiles = int((g.n[1] + TL::TY - 1) / TL::TY);
   const long long nk = (g.n[2] + KZ - 1) / KZ;
   const long long blocks = (long long)a.n_itiles * a.n_jtiles * nk;
   if (blocks <= 0 || blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaMemsetAsync(cut_count, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
   const bool sample = phi_in == nullptr;
   const int sm = smem_bytes<T>(sample ? tape.bytes_len : 0);
-  cudaError_t e;
+  const int cut_blocks = 148 * 8;
   if (sample) {
-    e = cudaFuncSetAttribute(mc_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
-    mc_kernel<T, true><<<unsigned(blocks), NT, sm, s>>>(a);
+    mc_fill_kernel<T, true><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    mc_cut_kernel<T, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
   } else {
-    e = cudaFuncSetAttribute(mc_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
-    mc_kernel<T, false><<<unsigned(blocks), NT, sm, s>>>(a);
+    mc_fill_kernel<T, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    mc_cut_kernel<T, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
   }
   return cudaGetLastError();
 }
 
 template cudaError_t launch_mc<float>(const DevGrid<float>&, const DevTape&, const float*, float*,
-                                      const Cols&, const DevTable&, cudaStream_t);
+                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t);
 template cudaError_t launch_mc<double>(const DevGrid<double>&, const DevTape&, const double*, double*,
-                                       const Cols&, const DevTable&, cudaStream_t);
+                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t);
 
 }  // namespace cci
