@@ -52,6 +52,8 @@ EXPORTS = {
     "cc_calc_volume": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_report": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                   C.c_void_p, C.c_void_p],
+    "cc_mc_cells_from_phi_noalloc": [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                     C.c_void_p, C.c_void_p],
     "cc_version": [],
     "cc_last_error": [],
 }

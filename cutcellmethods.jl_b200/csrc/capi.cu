@@ -95,6 +95,10 @@ struct DeviceGuard {
 
 }  // namespace
 
+namespace cci {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace cci
+
 struct cc_handle {
   int device = 0, method = 0, dim = 3, prec = 0;
   int64_t n[3] = {0, 0, 0};

@@ -1,6 +1,7 @@
 // cc_internal.h -- launch interfaces between the C ABI (capi.cu) and the kernel files.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 #include "../../include/cutcell_b200.h"
 
@@ -68,6 +69,9 @@ int calc_volume_blocks();
 template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial,
                                double* out, cudaStream_t s);
+
+// Record the message cc_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* amb, const void* vf,
                           int is_f64, unsigned long long* counts, double* vmin, cudaStream_t s);

@@ -253,6 +253,24 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
                     const void* volume_fraction, int64_t counts[5],
                     double* min_volume_fraction, void* stream);
 
+/* Marching cubes from a caller-supplied nodal field WITHOUT allocating: no counterpart in the
+ * reference. For callers that may not let a library allocate device memory -- a solver whose
+ * device memory comes from its own pool, budgeted up front, or a time-stepping loop where a
+ * cudaMalloc (which can synchronize the device) mid-step is not acceptable. Same inputs and
+ * outputs as cc_mc_cells_from_phi, plus the device index, the precision (CC_F32 / CC_F64) and the
+ * tiling table as a HOST blob (validated, then copied into the library's static scratch). No
+ * handle: the scratch (the table's device copy and the cut-band work list) is one file-scope
+ * __device__ array of 32 MiB + 64.25 KiB that every GPU loading the library holds until exit.
+ *   - Grids of more than 8,388,608 (2^23) cells are rejected with CC_TOO_LARGE.
+ *   - The first call on a device looks up that array's device address (cudaGetSymbolAddress);
+ *     make that first call before any stream capture.
+ *   - Every call reuses the same array: calls that overlap on the GPU (other streams, other host
+ *     threads) race. Serialize them, e.g. on one stream.
+ * Calls no cudaMalloc, cudaFree or other allocating routine. */
+cc_status cc_mc_cells_from_phi_noalloc(int32_t device, int32_t prec, const cc_grid* g, const void* table,
+                                       size_t table_bytes, const void* phi, const cc_cells* cells,
+                                       void* stream);
+
 /* Library version string. */
 const char* cc_version(void);
 /* Last CUDA error text seen by the library on this thread ("" if none). */
