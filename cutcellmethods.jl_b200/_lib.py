@@ -54,6 +54,19 @@ EXPORTS = {
                   C.c_void_p, C.c_void_p],
     "cc_mc_cells_from_phi_noalloc": [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                      C.c_void_p, C.c_void_p],
+    "cc_mlp_create": [C.c_int32, C.c_void_p],
+    "cc_mlp_destroy": [C.c_void_p],
+    "cc_mlp_set_params": [C.c_void_p, C.c_void_p, C.c_int32],
+    "cc_mlp_get_params": [C.c_void_p, C.c_void_p, C.c_int32],
+    "cc_mlp_train": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_float,
+                     C.c_uint64, C.c_void_p, C.c_void_p],
+    "cc_mlp_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint64, C.c_int32,
+                    C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_mlp_predict": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "cc_mc_learned_samples": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "cc_mc_update_learned": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_float, C.c_void_p, C.c_void_p],
     "cc_version": [],
     "cc_last_error": [],
 }

@@ -26,9 +26,10 @@ cc_status fail(cc_status s, const std::string& msg) {
   return s;
 }
 
-// Packed tapes: every op gets its own copy of its primitive's parameters padded to a multiple of 4
-// elements (at most 16) plus, for a smooth-min, its k -- at most 17 slots per op.
-constexpr int PACK_MAX_PARAMS = 17 * CC_TAPE_MAX_OPS;
+// Packed tapes: every op gets its own copy of its primitive's parameters, started on a 4-element
+// boundary and padded to a multiple of 4 elements (at most 16), plus, for a smooth-min, its k --
+// at most 3 + 16 + 1 = 20 slots per op.
+constexpr int PACK_MAX_PARAMS = 20 * CC_TAPE_MAX_OPS;
 constexpr size_t TAPE_CAP = CC_TAPE_MAX_OPS * sizeof(cc_op) + PACK_MAX_PARAMS * sizeof(double) + 64;
 
 int prim_params(int opcode, int dim) {
@@ -99,22 +100,6 @@ namespace cci {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace cci
 
-struct cc_handle {
-  int device = 0, method = 0, dim = 3, prec = 0;
-  int64_t n[3] = {0, 0, 0};
-  bool tree = false;
-  unsigned char* tape_dev = nullptr;
-  unsigned char* tape_host = nullptr;  // pinned staging
-  cudaEvent_t tape_copied = nullptr;
-  bool tape_pending = false;
-  unsigned char* table_dev = nullptr;
-  size_t table_bytes = 0;
-  cci::DevTable tb{};
-  unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
-  unsigned* cut_count = nullptr;
-  double* vol_scratch = nullptr;  // calc_volume partials + result
-  unsigned long long* rep_scratch = nullptr;  // report counters + min
-};
 
 namespace {
 
@@ -135,6 +120,9 @@ cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s,
   for (int i = 0; i < t->n_ops; ++i) {
     cc_op op = t->ops[i];
     if (op.opcode != CC_OP_NONE) {
+      // a primitive's parameters start on a 4-element boundary: the device reads them with
+      // vector loads (an SMIN constant before them may have left np unaligned)
+      while (np % 4) p[np++] = T(0);
       const int cnt = prim_params(op.opcode, dim);
       const int padded = ((cnt + 3) / 4) * 4;
       for (int q = 0; q < padded; ++q) p[np + q] = q < cnt ? T(t->params[op.poff + q]) : T(0);
@@ -218,6 +206,16 @@ bool isotropic(const cc_grid* g) {
 }
 
 }  // namespace
+
+namespace cci {
+cc_status validate_body(const cc_optape* t, int dim) { return validate_tape(t, dim); }
+cc_status upload_body_f64(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, DevTape* out) {
+  return upload_tape<double>(h, t, dim, s, out);
+}
+cc_status upload_body_f32(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, DevTape* out) {
+  return upload_tape<float>(h, t, dim, s, out);
+}
+}  // namespace cci
 
 extern "C" {
 

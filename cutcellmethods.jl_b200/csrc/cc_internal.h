@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include "../../include/cutcell_b200.h"
 
+struct cc_handle;
+
 namespace cci {
 
 // Device view of a tiling table blob (include/cutcell_b200.h).
@@ -45,10 +47,27 @@ struct Cols {
 // every cell. Returns the CUDA launch status.
 // `cut_list` (one slot per cell) and `cut_count` are scratch: the fill pass lists the cut band
 // there and the cut pass reads it back.
+// With with_cut false only the fill pass runs (the cut band is listed, not built).
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s);
+                      cudaStream_t s, bool with_cut = true);
+
+// The learned correction (learned.cu).
+int mlp_nparam();
+template <class T>
+cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
+                                  const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
+                                  unsigned long long* fallback, int* err, cudaStream_t s);
+cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, long long n,
+                             unsigned long long seed, int step, int tiles, float* grad, float* loss, int* err,
+                             cudaStream_t s);
+cudaError_t launch_mlp_adam(float* P, float* m, float* v, const float* grad, int tiles, int step, float lr,
+                            cudaStream_t s);
+cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, float* out, int* err, cudaStream_t s);
+cudaError_t launch_labels(const DevGrid<double>& g, const DevTape& tape, const float* phi, const float* vf,
+                          const DevTable& tb, const unsigned* list, long long n, float* feats, float* labels,
+                          float* plain, cudaStream_t s);
 
 template <class T>
 cudaError_t launch_ms(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
@@ -73,7 +92,32 @@ cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double*
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);
 
+// Validate an op-tape for a dim-dimensional grid, and pack + upload it (narrowed to double) into
+// the handle's tape buffer on stream s.
+cc_status validate_body(const cc_optape* t, int dim);
+cc_status upload_body_f64(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, DevTape* out);
+cc_status upload_body_f32(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, DevTape* out);
+
 cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* amb, const void* vf,
                           int is_f64, unsigned long long* counts, double* vmin, cudaStream_t s);
 
 }  // namespace cci
+
+// The library-side state of one cache (created at allocate_cache time, include/cutcell_b200.h).
+struct cc_handle {
+  int device = 0, method = 0, dim = 3, prec = 0;
+  int64_t n[3] = {0, 0, 0};
+  bool tree = false;
+  unsigned char* tape_dev = nullptr;
+  unsigned char* tape_host = nullptr;  // pinned staging
+  cudaEvent_t tape_copied = nullptr;
+  bool tape_pending = false;
+  unsigned char* table_dev = nullptr;
+  size_t table_bytes = 0;
+  cci::DevTable tb{};
+  unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
+  unsigned* cut_count = nullptr;
+  double* vol_scratch = nullptr;  // calc_volume partials + result
+  unsigned long long* rep_scratch = nullptr;  // report counters + min
+};
+

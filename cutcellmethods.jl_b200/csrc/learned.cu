@@ -1,0 +1,697 @@
+// learned.cu -- the learned volume-fraction correction on sm_100a tensor cores (tcgen05).
+//
+// A small MLP, 8 -> 64 -> 64 -> 1 with GELU hidden layers and a sigmoid output, maps a cut
+// cell's corner values scaled by the cell size (phi / h, marching-cubes corner order) to a
+// corrected fluid volume fraction. It is trained on the fluid fractions that marching cubes gives
+// the same cells at 8x sub-refinement. Only a cut cell's volume_fraction is replaced; kind and the
+// face fractions stay the plain construction's, so watertightness and the shared-face identities
+// survive. Where the prediction is not finite or strays more than `bound` from the plain value,
+// the plain value is kept.
+//
+// Every GEMM runs on the 5th-generation tensor cores: BF16 operands staged in shared memory in the
+// K-major "interleaved" layout (8-row x 16-byte core matrices), FP32 accumulators in tensor memory
+// (TMEM), one tcgen05.mma per K = 16 step issued by one thread, completion signalled through an
+// mbarrier by tcgen05.commit, results read back with tcgen05.ld (warp w reads TMEM lanes 32w..).
+// A CTA works on tiles of 128 samples (the MMA's M): row t of every activation tile is sample t,
+// which thread t owns.
+//
+//   forward   H1 = X W1^T (K 16)        A1 = gelu(H1 + b1)
+//             H2 = A1 W2^T (K 64)       z = gelu(H2 + b2) . w3 + b3,  p = sigmoid(z)
+//   backward  dW2 = dH2^T A1 (K = 128 samples),  dA1 = dH2 W2 (K 64),  dW1 = dH1^T X (K = 128)
+//
+// Training writes per-CTA partial gradients to fixed slots and a second kernel sums them in CTA
+// order and takes an Adam step, so training is deterministic.
+#include <cstdint>
+#include <cstring>
+#include <cuda_bf16.h>
+#include "cc_device.cuh"
+#include "cc_internal.h"
+#include "mc_cell.cuh"
+
+namespace {
+
+using namespace ccd;
+using namespace ccmc;
+using cci::Cols;
+using cci::DevGrid;
+using cci::DevTape;
+
+constexpr int TILE = 128;  // samples per tile = MMA M = threads per CTA
+constexpr int H = 64;      // hidden width
+constexpr int KIN = 16;    // 8 inputs padded to one K step
+
+// FP32 parameter vector layout
+constexpr int P_W1 = 0;            // [64][8]  (row = output unit)
+constexpr int P_B1 = P_W1 + 64 * 8;
+constexpr int P_W2 = P_B1 + 64;    // [64][64]
+constexpr int P_B2 = P_W2 + 64 * 64;
+constexpr int P_W3 = P_B2 + 64;    // [64]
+constexpr int P_B3 = P_W3 + 64;
+constexpr int NPARAM = P_B3 + 1;   // 4801
+
+constexpr long long WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a tile gives up
+
+// ---------------------------------------------------------------------------------------------
+// tcgen05 / mbarrier primitives
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: K-major, no swizzle. lbo = bytes between core matrices
+// adjacent along K, sbo = bytes between core matrices adjacent along M (or N).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version 1 (sm_100)
+  return d;                // base offset 0, layout type 0 = no swizzle
+}
+// Instruction descriptor, kind::f16: BF16 A and B, FP32 accumulator, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() { asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* m, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on an MMA commit: false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try_wait(m, parity)) return true;
+  return false;
+}
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane, waited for before use.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of bf16 element (r, k) of an [R x K] tile stored K-major as 8x8 core matrices:
+// core (r/8, k/8) at ((r/8)(K/8) + k/8) * 128 bytes, element at (r%8)*16 + (k%8)*2 within it.
+__device__ __forceinline__ int kmaj(int r, int k, int K) {
+  return ((((r >> 3) * (K >> 3)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
+}
+__device__ __forceinline__ void put_bf16(unsigned char* tile, int r, int k, int K, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(tile + kmaj(r, k, K)) = __float2bfloat16_rn(v);
+}
+// D[M x N] (+)= A[M x K] B[N x K]^T over K / 16 MMAs; tiles in the layout above.
+__device__ __forceinline__ void gemm_kmaj(uint32_t tmem_d, const unsigned char* A, const unsigned char* B, int M,
+                                          int N, int K) {
+  const uint32_t idesc = umma_idesc(M, N);
+  const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+  for (int s = 0; s < K / 16; ++s) {
+    const uint64_t da = umma_desc(smem_u32(A) + 256u * s, 128u, sbo);
+    const uint64_t db = umma_desc(smem_u32(B) + 256u * s, 128u, sbo);
+    umma_bf16(tmem_d, da, db, idesc, s > 0 ? 1u : 0u);
+  }
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// Shared-memory layout (bytes) of an MLP CTA.
+struct MlpLayout {
+  static constexpr int X = 0;                          // [128 x 16] bf16
+  static constexpr int W1 = X + TILE * KIN * 2;        // [64 x 16]
+  static constexpr int A1 = W1 + H * KIN * 2;          // [128 x 64]
+  static constexpr int W2 = A1 + TILE * H * 2;         // [64 x 64]
+  static constexpr int W2T = W2 + H * H * 2;           // [64 x 64] (training)
+  static constexpr int DH2 = W2T + H * H * 2;          // [128 x 64]
+  static constexpr int DH2T = DH2 + TILE * H * 2;      // [128 x 128], rows 64.. zero
+  static constexpr int A1T = DH2T + TILE * TILE * 2;   // [64 x 128]
+  static constexpr int DH1T = A1T + H * TILE * 2;      // [128 x 128], rows 64.. zero
+  static constexpr int XT = DH1T + TILE * TILE * 2;    // [16 x 128], rows 8.. zero
+  static constexpr int H1 = XT + KIN * TILE * 2;       // f32 [128][65]
+  static constexpr int PAR = H1 + TILE * 65 * 4;       // f32 b1[64] b2[64] w3[64] b3, then 4 scratch
+  static constexpr int PAR_FLOATS = 3 * H + 8;
+  static constexpr int MISC = PAR + PAR_FLOATS * 4;    // mbarrier, tmem base, flags
+  static constexpr int INFER_BYTES = W2T;              // inference needs X, W1, A1, W2 only
+  static constexpr int INFER_SMEM = INFER_BYTES + PAR_FLOATS * 4 + 64;
+  static constexpr int TRAIN_BYTES = MISC + 64;
+};
+
+struct MlpShared {
+  unsigned char* base;
+  float* par;
+  uint64_t* mbar;
+  uint32_t* tmem;
+  int* flag;
+};
+
+__device__ __forceinline__ MlpShared mlp_shared(unsigned char* smem, bool train) {
+  MlpShared s;
+  s.base = smem;
+  const int misc = train ? MlpLayout::MISC : MlpLayout::INFER_BYTES + MlpLayout::PAR_FLOATS * 4;
+  s.par = reinterpret_cast<float*>(smem + (train ? MlpLayout::PAR : MlpLayout::INFER_BYTES));
+  s.mbar = reinterpret_cast<uint64_t*>(smem + ((misc + 7) / 8) * 8);
+  s.tmem = reinterpret_cast<uint32_t*>(s.mbar + 1);
+  s.flag = reinterpret_cast<int*>(s.tmem + 1);
+  return s;
+}
+
+// Stage the weights (FP32 master copy -> BF16 tiles) and biases of the network.
+__device__ void stage_weights(const float* __restrict__ P, const MlpShared& s, bool train) {
+  unsigned char* b = s.base;
+  for (int e = threadIdx.x; e < H * KIN; e += TILE) {
+    const int j = e / KIN, k = e % KIN;
+    put_bf16(b + MlpLayout::W1, j, k, KIN, k < 8 ? P[P_W1 + j * 8 + k] : 0.0f);
+  }
+  for (int e = threadIdx.x; e < H * H; e += TILE) {
+    const int j = e / H, i = e % H;
+    const float w = P[P_W2 + j * H + i];
+    put_bf16(b + MlpLayout::W2, j, i, H, w);
+    if (train) put_bf16(b + MlpLayout::W2T, i, j, H, w);
+  }
+  // par: b1[64], b2[64], w3[64], b3
+  for (int e = threadIdx.x; e < 3 * H + 1; e += TILE)
+    s.par[e] = e < H ? P[P_B1 + e] : e < 2 * H ? P[P_B2 + e - H] : e < 3 * H ? P[P_W3 + e - 2 * H] : P[P_B3];
+}
+
+// One tile's forward pass. x: this thread's 8 inputs (zeros for a padding row). Returns p and, in
+// training, keeps what the backward pass needs in shared memory / TMEM. `phase` is the running
+// mbarrier parity. Returns false if an MMA never completed.
+__device__ bool mlp_forward(const MlpShared& s, uint32_t tmem, const float x[8], bool train, uint32_t& phase, float& z_out) {
+  unsigned char* b = s.base;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < KIN; ++k) put_bf16(b + MlpLayout::X, t, k, KIN, k < 8 ? x[k] : 0.0f);
+  if (train) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) put_bf16(b + MlpLayout::XT, k, t, TILE, x[k]);
+  }
+  fence_async_smem();
+  __syncthreads();
+  if (t == 0) {
+    tc_fence_after();
+    gemm_kmaj(tmem, b + MlpLayout::X, b + MlpLayout::W1, TILE, H, KIN);
+    umma_commit(s.mbar);
+  }
+  const bool ok1 = mbar_wait(s.mbar, phase);
+  phase ^= 1u;
+  if (__syncthreads_or(!ok1)) return false;
+  tc_fence_after();
+  const uint32_t lane_addr = tmem + ((uint32_t)(32 * (t / 32)) << 16);
+  float* h1row = reinterpret_cast<float*>(b + MlpLayout::H1) + t * 65;
+  for (int c = 0; c < H / 16; ++c) {
+    float v[16];
+    tmem_ld16(lane_addr + 16 * c, v);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int j = 16 * c + q;
+      const float h = v[q] + s.par[j];
+      const float a = gelu(h);
+      put_bf16(b + MlpLayout::A1, t, j, H, a);
+      if (train) {
+        h1row[j] = h;
+        put_bf16(b + MlpLayout::A1T, j, t, TILE, a);
+      }
+    }
+  }
+  tc_fence_before();
+  fence_async_smem();
+  __syncthreads();
+  if (t == 0) {
+    tc_fence_after();
+    gemm_kmaj(tmem, b + MlpLayout::A1, b + MlpLayout::W2, TILE, H, H);
+    umma_commit(s.mbar);
+  }
+  const bool ok2 = mbar_wait(s.mbar, phase);
+  phase ^= 1u;
+  if (__syncthreads_or(!ok2)) return false;
+  tc_fence_after();
+  float z = 0.0f;
+  for (int c = 0; c < H / 16; ++c) {
+    float v[16];
+    tmem_ld16(lane_addr + 16 * c, v);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int j = 16 * c + q;
+      z = z + gelu(v[q] + s.par[H + j]) * s.par[2 * H + j];
+    }
+  }
+  z_out = z + s.par[3 * H];
+  return true;
+}
+
+__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
+
+// Sum over the 128 threads of the CTA, in a fixed order; every thread gets the result.
+__device__ __forceinline__ float cta_sum(float v, float* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = v;
+  __syncthreads();
+  const float r = (red[0] + red[1]) + (red[2] + red[3]);
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Training: one tile of 128 samples per CTA per step; per-CTA partial gradients in grad[cta][].
+__global__ void __launch_bounds__(TILE, 1)
+    mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ feats, const float* __restrict__ labels,
+                     long long n, unsigned long long seed, int step, float inv_batch, float* __restrict__ grad,
+                     float* __restrict__ loss, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const MlpShared s = mlp_shared(smem, true);
+  const int t = threadIdx.x;
+  unsigned char* b = s.base;
+  stage_weights(P, s, true);
+  // rows 64..127 of the transposed gradient tiles stay zero (M is padded to 128)
+  for (int e = t; e < TILE * TILE / 2; e += TILE) {
+    const int r = 64 + e / TILE, k = e % TILE;
+    put_bf16(b + MlpLayout::DH2T, r, k, TILE, 0.0f);
+    put_bf16(b + MlpLayout::DH1T, r, k, TILE, 0.0f);
+  }
+  for (int e = t; e < 8 * TILE; e += TILE) put_bf16(b + MlpLayout::XT, 8 + e / TILE, e % TILE, TILE, 0.0f);
+  if (t == 0) { mbar_init(s.mbar, 1); *s.flag = 0; }
+  if (t < 32) { tmem_alloc(s.tmem, 128); tmem_relinquish(); }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s.tmem;
+  uint32_t phase = 0;
+  float* red = s.par + 3 * H + 4;  // 4 floats of scratch past b3
+  float* g = grad + (long long)blockIdx.x * NPARAM;
+
+  // the sample: a counter-based hash of (seed, step, slot), uniform over the data set
+  unsigned long long hsh = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(step * (long long)gridDim.x * TILE +
+                                                                                  blockIdx.x * TILE + t + 1));
+  hsh ^= hsh >> 33; hsh *= 0xff51afd7ed558ccdull; hsh ^= hsh >> 33; hsh *= 0xc4ceb9fe1a85ec53ull; hsh ^= hsh >> 33;
+  const long long idx = (long long)(hsh % (unsigned long long)n);
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = feats[idx * 8 + k];
+  const float y = labels[idx];
+
+  bool ok = true;
+  float z = 0.0f;
+  do {
+    if (!mlp_forward(s, tmem, x, true, phase, z)) { ok = false; break; }
+    const float p = sigmoidf_(z);
+    const float e = p - y;
+    const float l = cta_sum(e * e, red);
+    if (t == 0) loss[blockIdx.x] = l;
+    const float dz = 2.0f * e * inv_batch * p * (1.0f - p);
+    const float db3 = cta_sum(dz, red);
+    if (t == 0) g[P_B3] = db3;
+    // layer 3 and the gradient into H2, from the still-resident H2 accumulator in TMEM
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * (t / 32)) << 16);
+    for (int c = 0; c < H / 16; ++c) {
+      float v[16];
+      tmem_ld16(lane_addr + 16 * c, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int j = 16 * c + q;
+        const float h2 = v[q] + s.par[H + j];
+        const float a2 = gelu(h2);
+        const float dw3 = cta_sum(dz * a2, red);
+        if (t == 0) g[P_W3 + j] = dw3;
+        const float dh2 = dz * s.par[2 * H + j] * gelu_grad(h2);
+        const float db2 = cta_sum(dh2, red);
+        if (t == 0) g[P_B2 + j] = db2;
+        put_bf16(b + MlpLayout::DH2, t, j, H, dh2);
+        put_bf16(b + MlpLayout::DH2T, j, t, TILE, dh2);
+      }
+    }
+    tc_fence_before();
+    fence_async_smem();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+      gemm_kmaj(tmem, b + MlpLayout::DH2T, b + MlpLayout::A1T, TILE, H, TILE);       // dW2 -> cols 0..63
+      gemm_kmaj(tmem + H, b + MlpLayout::DH2, b + MlpLayout::W2T, TILE, H, H);       // dA1 -> cols 64..127
+      umma_commit(s.mbar);
+    }
+    const bool ok3 = mbar_wait(s.mbar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok3)) { ok = false; break; }
+    tc_fence_after();
+    const float* h1row = reinterpret_cast<const float*>(b + MlpLayout::H1) + t * 65;
+    for (int c = 0; c < H / 16; ++c) {
+      float v[16];
+      tmem_ld16(lane_addr + H + 16 * c, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int i = 16 * c + q;
+        const float dh1 = v[q] * gelu_grad(h1row[i]);
+        const float db1 = cta_sum(dh1, red);
+        if (t == 0) g[P_B1 + i] = db1;
+        put_bf16(b + MlpLayout::DH1T, i, t, TILE, dh1);
+      }
+    }
+    if (t < 64) {  // TMEM lanes 0..63 hold dW2's rows (output units)
+      for (int c = 0; c < H / 16; ++c) {
+        float v[16];
+        tmem_ld16(lane_addr + 16 * c, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) g[P_W2 + t * H + 16 * c + q] = v[q];
+      }
+    }
+    tc_fence_before();
+    fence_async_smem();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+      gemm_kmaj(tmem, b + MlpLayout::DH1T, b + MlpLayout::XT, TILE, KIN, TILE);    // dW1 -> cols 0..15
+      umma_commit(s.mbar);
+    }
+    const bool ok4 = mbar_wait(s.mbar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok4)) { ok = false; break; }
+    tc_fence_after();
+    if (t < 64) {
+      float v[16];
+      tmem_ld16(lane_addr, v);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) g[P_W1 + t * 8 + k] = v[k];
+    }
+  } while (false);
+  if (!ok && t == 0) atomicExch(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (t < 32) tmem_dealloc(tmem, 128);
+}
+
+// Sum the per-CTA gradients in CTA order and take one Adam step.
+__global__ void mlp_adam_kernel(float* __restrict__ P, float* __restrict__ m, float* __restrict__ v,
+                                const float* __restrict__ grad, int nblk, int step, float lr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NPARAM) return;
+  float g = 0.0f;
+  for (int b = 0; b < nblk; ++b) g += grad[(long long)b * NPARAM + i];
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float mi = b1 * m[i] + (1.0f - b1) * g;
+  const float vi = b2 * v[i] + (1.0f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / (1.0f - powf(b1, (float)(step + 1)));
+  const float vh = vi / (1.0f - powf(b2, (float)(step + 1)));
+  P[i] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+// Forward only, over given samples (the inference path without the cut construction).
+__global__ void __launch_bounds__(TILE, 1)
+    mlp_predict_kernel(const float* __restrict__ P, const float* __restrict__ feats, long long n, float* __restrict__ out,
+                       int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const MlpShared s = mlp_shared(smem, false);
+  const int t = threadIdx.x;
+  stage_weights(P, s, false);
+  if (t == 0) mbar_init(s.mbar, 1);
+  if (t < 32) { tmem_alloc(s.tmem, 64); tmem_relinquish(); }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s.tmem;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (long long base = (long long)blockIdx.x * TILE; base < n; base += (long long)gridDim.x * TILE) {
+    const long long q = base + t;
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = q < n ? feats[q * 8 + k] : 0.0f;
+    float z;
+    if (!mlp_forward(s, tmem, x, false, phase, z)) { ok = false; break; }
+    if (q < n) out[q] = sigmoidf_(z);
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (t < 32) tmem_dealloc(tmem, 64);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused cut-band kernel with the learned correction: each CTA takes tiles of 128 listed cut cells,
+// one per thread, builds their plain moments (writing every field), then runs the network on the
+// tile and replaces the volume fraction where the prediction is accepted.
+template <class T>
+struct LearnedArgs {
+  DevGrid<T> g;
+  const T* phi;
+  cci::Cols cols;
+  DevTable tb;
+  const unsigned* cut_list;
+  const unsigned* cut_count;
+  const float* P;
+  float bound;
+  unsigned long long* fallback;
+  int* err;
+};
+
+template <class T>
+__global__ void __launch_bounds__(TILE, 1) mc_cut_learned_kernel(const LearnedArgs<T> A) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const MlpShared s = mlp_shared(smem, false);
+  const int t = threadIdx.x;
+  stage_weights(A.P, s, false);
+  if (t == 0) mbar_init(s.mbar, 1);
+  if (t < 32) { tmem_alloc(s.tmem, 64); tmem_relinquish(); }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s.tmem;
+  uint32_t phase = 0;
+  const long long n0 = A.g.n[0], n1 = A.g.n[1];
+  const long long nx = n0 + 1, ny = n1 + 1;
+  Stage<T> st;
+  st.kind = A.cols.kind;
+  st.amb = A.cols.amb;
+  st.vf = static_cast<T*>(A.cols.vf);
+  st.c = static_cast<T*>(A.cols.c);
+  st.ff = static_cast<T*>(A.cols.ff);
+  st.fcl = static_cast<T*>(A.cols.fcl);
+  st.ic = static_cast<T*>(A.cols.ic);
+  const T cs[3] = {A.g.d[0], A.g.d[1], A.g.d[2]};
+  const float inv_h = 1.0f / float(A.g.d[0]);
+  const long long total = *A.cut_count;
+  unsigned long long fb = 0;
+  bool ok = true;
+  for (long long base = (long long)blockIdx.x * TILE; base < total; base += (long long)gridDim.x * TILE) {
+    const long long q = base + t;
+    float x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long ci = -1;
+    T plain = T(0);
+    if (q < total) {
+      ci = A.cut_list[q];
+      const long long i = ci % n0, j = (ci / n0) % n1, k = ci / (n0 * n1);
+      const long long b0 = i + nx * (j + ny * k);
+      const long long bz = nx * ny;
+      const T ph[8] = {A.phi[b0], A.phi[b0 + 1], A.phi[b0 + nx + 1], A.phi[b0 + nx],
+                       A.phi[b0 + bz], A.phi[b0 + bz + 1], A.phi[b0 + bz + nx + 1], A.phi[b0 + bz + nx]};
+      const T org[3] = {node_coord(A.g.x0[0], A.g.d[0], i), node_coord(A.g.x0[1], A.g.d[1], j),
+                        node_coord(A.g.x0[2], A.g.d[2], k)};
+      const T l[3] = {node_coord(A.g.x0[0], A.g.d[0], i + 1) - org[0], node_coord(A.g.x0[1], A.g.d[1], j + 1) - org[1],
+                      node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
+      mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
+      plain = st.vf[ci];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = float(ph[c]) * inv_h;
+    }
+    float z;
+    if (!mlp_forward(s, tmem, x, false, phase, z)) { ok = false; break; }
+    if (q < total) {
+      const float p = sigmoidf_(z);
+      const bool accept = p >= 0.0f && p <= 1.0f && fabsf(p - float(plain)) <= A.bound;
+      if (accept) st.vf[ci] = T(p);
+      else ++fb;
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (fb) atomicAdd(A.fallback, fb);
+  if (!ok && t == 0) atomicExch(A.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (t < 32) tmem_dealloc(tmem, 64);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Training samples: for each listed cut cell, its features (8 corner phi / h), its plain volume
+// fraction and the label -- the fluid fraction marching cubes gives it at 8x sub-refinement, the
+// body resampled at the 9^3 sub-nodes (Float64, on the global refined lattice x0 + m d/8).
+constexpr int LBL_NT = 128;
+constexpr int LBL_SUB_BYTES = ((729 * 8 + 15) / 16) * 16;  // staged columns then start 16-byte aligned
+__global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, const DevTape tape, const float* __restrict__ phi,
+                                                      const float* __restrict__ vf, const DevTable tb,
+                                                      const unsigned* __restrict__ list, long long n,
+                                                      float* __restrict__ feats, float* __restrict__ labels,
+                                                      float* __restrict__ plain) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  double* sub = reinterpret_cast<double*>(smem);                    // 729 sub-node values
+  unsigned char* stg = smem + LBL_SUB_BYTES;                        // one cell slot per thread
+  double* red = reinterpret_cast<double*>(stg + LBL_NT * 208);      // 4 partials
+  unsigned char* tp = reinterpret_cast<unsigned char*>(red + 4);
+  const STape<double> t = load_tape<double>(tape.bytes, tape.n_ops, tape.n_params, tp);
+  __syncthreads();
+  Stage<double> st;
+  st.kind = reinterpret_cast<int8_t*>(stg);
+  st.amb = stg + LBL_NT;
+  st.vf = reinterpret_cast<double*>(stg + 2 * LBL_NT);
+  st.c = st.vf + LBL_NT;
+  st.ff = st.c + 3 * LBL_NT;
+  st.fcl = st.ff + 6 * LBL_NT;
+  st.ic = st.fcl + 12 * LBL_NT;
+  const long long n0 = g.n[0], n1 = g.n[1];
+  const long long nx = n0 + 1, ny = n1 + 1;
+  const double sd[3] = {g.d[0] / 8.0, g.d[1] / 8.0, g.d[2] / 8.0};
+  const float inv_hf = 1.0f / float(g.d[0]);
+  for (long long q = blockIdx.x; q < n; q += gridDim.x) {
+    const long long ci = list[q];
+    const long long i = ci % n0, j = (ci / n0) % n1, k = ci / (n0 * n1);
+    for (int v = threadIdx.x; v < 729; v += LBL_NT) {
+      const int a = v % 9, b = (v / 9) % 9, c = v / 81;
+      const double xyz[3] = {node_coord(g.x0[0], sd[0], 8 * i + a), node_coord(g.x0[1], sd[1], 8 * j + b),
+                             node_coord(g.x0[2], sd[2], 8 * k + c)};
+      sub[v] = tape_eval<double, 3, double>(t, xyz);
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int sc = threadIdx.x; sc < 512; sc += LBL_NT) {
+      const int a = sc % 8, b = (sc / 8) % 8, c = sc / 64;
+      const int s0 = a + 9 * (b + 9 * c);
+      const double ph[8] = {sub[s0], sub[s0 + 1], sub[s0 + 10], sub[s0 + 9],
+                            sub[s0 + 81], sub[s0 + 82], sub[s0 + 91], sub[s0 + 90]};
+      int nout = 0;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) nout += nudge(ph[e]) >= 0.0 ? 1 : 0;
+      if (nout == 8) acc += 1.0;
+      else if (nout > 0) {
+        const double org[3] = {node_coord(g.x0[0], sd[0], 8 * i + a), node_coord(g.x0[1], sd[1], 8 * j + b),
+                               node_coord(g.x0[2], sd[2], 8 * k + c)};
+        const double l[3] = {node_coord(g.x0[0], sd[0], 8 * i + a + 1) - org[0],
+                             node_coord(g.x0[1], sd[1], 8 * j + b + 1) - org[1],
+                             node_coord(g.x0[2], sd[2], 8 * k + c + 1) - org[2]};
+        mc_cut_cell<double>(ph, l, org, sd, tb, st, threadIdx.x);
+        acc += st.vf[threadIdx.x];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      labels[q] = float(((red[0] + red[1]) + (red[2] + red[3])) / 512.0);
+      plain[q] = vf[ci];
+    }
+    if (threadIdx.x < 8) {
+      const int e = threadIdx.x;
+      const long long b0 = i + nx * (j + ny * k);
+      const long long off[8] = {0, 1, nx + 1, nx, nx * ny, nx * ny + 1, nx * ny + nx + 1, nx * ny + nx};
+      feats[q * 8 + e] = phi[b0 + off[e]] * inv_hf;  // as the learned update forms them
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// =============================================================================================
+namespace cci {
+
+int mlp_nparam() { return NPARAM; }
+
+template <class T>
+cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
+                                  const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
+                                  unsigned long long* fallback, int* err, cudaStream_t s) {
+  LearnedArgs<T> a{g, phi, cols, tb, cut_list, cut_count, P, bound, fallback, err};
+  const int sm = MlpLayout::INFER_SMEM;
+  cudaError_t e = cudaFuncSetAttribute(mc_cut_learned_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  mc_cut_learned_kernel<T><<<148 * 2, TILE, sm, s>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t launch_mc_cut_learned<float>(const DevGrid<float>&, const float*, const Cols&, const DevTable&,
+                                                  const unsigned*, const unsigned*, const float*, float,
+                                                  unsigned long long*, int*, cudaStream_t);
+template cudaError_t launch_mc_cut_learned<double>(const DevGrid<double>&, const double*, const Cols&, const DevTable&,
+                                                   const unsigned*, const unsigned*, const float*, float,
+                                                   unsigned long long*, int*, cudaStream_t);
+
+// One training step's gradients: per-CTA partials in grad[tiles][NPARAM], per-CTA squared-error
+// sums in loss[tiles].
+cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, long long n,
+                             unsigned long long seed, int step, int tiles, float* grad, float* loss, int* err,
+                             cudaStream_t s) {
+  const int sm = MlpLayout::TRAIN_BYTES;
+  cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  mlp_train_kernel<<<tiles, TILE, sm, s>>>(P, feats, labels, n, seed, step, 1.0f / float(tiles * TILE), grad, loss, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_adam(float* P, float* m, float* v, const float* grad, int tiles, int step, float lr,
+                            cudaStream_t s) {
+  mlp_adam_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(P, m, v, grad, tiles, step, lr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, float* out, int* err, cudaStream_t s) {
+  const int sm = MlpLayout::INFER_SMEM;
+  cudaError_t e = cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  long long tiles = (n + TILE - 1) / TILE;
+  const int grid = (int)(tiles < 148 * 2 ? (tiles < 1 ? 1 : tiles) : 148 * 2);
+  mlp_predict_kernel<<<grid, TILE, sm, s>>>(P, feats, n, out, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_labels(const DevGrid<double>& g, const DevTape& tape, const float* phi, const float* vf,
+                          const DevTable& tb, const unsigned* list, long long n, float* feats, float* labels,
+                          float* plain, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int sm = LBL_SUB_BYTES + LBL_NT * 208 + 4 * 8 + ((tape.bytes_len + 15) / 16) * 16;
+  cudaError_t e = cudaFuncSetAttribute(label_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  const long long grid = n < 148 * 8 ? n : 148 * 8;
+  label_kernel<<<(unsigned)grid, LBL_NT, sm, s>>>(g, tape, phi, vf, tb, list, n, feats, labels, plain);
+  return cudaGetLastError();
+}
+
+}  // namespace cci

@@ -190,20 +190,45 @@ __global__ void calc_volume_final(const double* partial, int nb, double* out) {
 }
 
 // cut_cell_report, src/cut_cell.jl:302-319: counts by kind, ambiguous, smallest cut fraction.
+// Each thread takes 16 cells at a time with 16-byte loads of the kind and ambiguous columns (the
+// caller guarantees 16-byte aligned columns for the vector part; the tail is scalar).
+template <class T>
+__device__ __forceinline__ void report_cell(int k, int a, T v, unsigned long long& cut, unsigned long long& ins,
+                                            unsigned long long& out, unsigned long long& am, T& vmin) {
+  cut += k == 2;
+  ins += k == 0;
+  out += k == 1;
+  am += a != 0;
+  if (k == 2 && v > T(0) && v < vmin) vmin = v;
+}
+
 template <class T>
 __global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_t* __restrict__ kind,
                                                     const uint8_t* __restrict__ amb, const T* __restrict__ vf,
-                                                    unsigned long long* counts, unsigned long long* vmin_bits) {
+                                                    unsigned long long* counts, unsigned long long* vmin_bits,
+                                                    int vec_ok) {
   unsigned long long cut = 0, ins = 0, out = 0, am = 0;
   T vmin = T(1);
-  for (long long i = blockIdx.x * (long long)NT + threadIdx.x; i < ncell; i += (long long)gridDim.x * NT) {
-    const int k = kind[i];
-    cut += k == 2;
-    ins += k == 0;
-    out += k == 1;
-    am += amb[i] != 0;
-    if (k == 2) { const T v = vf[i]; if (v > T(0) && v < vmin) vmin = v; }
+  const long long nvec = vec_ok ? ncell / 16 : 0;
+  for (long long g = blockIdx.x * (long long)NT + threadIdx.x; g < nvec; g += (long long)gridDim.x * NT) {
+    const uint4 kk = reinterpret_cast<const uint4*>(kind)[g];
+    const uint4 aa = reinterpret_cast<const uint4*>(amb)[g];
+    const unsigned kw[4] = {kk.x, kk.y, kk.z, kk.w};
+    const unsigned aw[4] = {aa.x, aa.y, aa.z, aa.w};
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int k = (int)(signed char)((kw[w] >> (8 * b)) & 0xffu);
+        const int a = (int)((aw[w] >> (8 * b)) & 0xffu);
+        // the fraction is only read for cut cells, which are few
+        const T v = k == 2 ? vf[16 * g + 4 * w + b] : T(1);
+        report_cell<T>(k, a, v, cut, ins, out, am, vmin);
+      }
+    }
   }
+  for (long long i = 16 * nvec + blockIdx.x * (long long)NT + threadIdx.x; i < ncell; i += (long long)gridDim.x * NT)
+    report_cell<T>(kind[i], amb[i], kind[i] == 2 ? vf[i] : T(1), cut, ins, out, am, vmin);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     cut += __shfl_down_sync(0xffffffffu, cut, o);
@@ -257,12 +282,13 @@ cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double*
 
 cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* amb, const void* vf, int is_f64,
                           unsigned long long* counts, double* vmin, cudaStream_t s) {
-  const int nb = blocks_for(ncell, 8);
+  const int nb = blocks_for((ncell + 15) / 16, 8);
   unsigned long long* vb = reinterpret_cast<unsigned long long*>(vmin);
+  const int vec_ok = ((reinterpret_cast<uintptr_t>(kind) | reinterpret_cast<uintptr_t>(amb)) & 15u) == 0;
   if (is_f64)
-    report_kernel<double><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const double*>(vf), counts, vb);
+    report_kernel<double><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const double*>(vf), counts, vb, vec_ok);
   else
-    report_kernel<float><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const float*>(vf), counts, vb);
+    report_kernel<float><<<nb, NT, 0, s>>>(ncell, kind, amb, static_cast<const float*>(vf), counts, vb, vec_ok);
   return cudaGetLastError();
 }
 

@@ -253,6 +253,44 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
                     const void* volume_fraction, int64_t counts[5],
                     double* min_volume_fraction, void* stream);
 
+/* ---- learned volume-fraction correction ----------------------------------------------------
+ * An MLP 8 -> 64 -> 64 -> 1 (GELU, sigmoid output; BF16 tensor-core GEMMs with FP32 accumulate)
+ * mapping a cut cell's corner values over the cell size (phi / h, MC_NODE_BITS order) to its fluid
+ * volume fraction, trained on 8x sub-refined marching cubes (the BASELINE learned-correction
+ * workload; no counterpart function in the reference, whose plain marching cubes it corrects).
+ * Parameters: FP32, CC_MLP_NPARAM of them: W1[64][8] b1[64] W2[64][64] b2[64] w3[64] b3. */
+#define CC_MLP_NPARAM 4801
+#define CC_MLP_MAX_TILES 1184
+typedef struct cc_mlp cc_mlp;
+cc_status cc_mlp_create(int32_t device, cc_mlp** out);
+cc_status cc_mlp_destroy(cc_mlp* m);
+/* host <-> device parameters; setting them also resets the Adam moments and step */
+cc_status cc_mlp_set_params(cc_mlp* m, const float* params, int32_t n);
+cc_status cc_mlp_get_params(cc_mlp* m, float* params, int32_t n);
+/* `steps` Adam steps (learning rate lr) of mean-squared error on device samples feats[n][8],
+ * labels[n]; each step draws tiles*128 samples by a counter-based hash of (seed, step, slot).
+ * Blocking; *last_loss receives the final step's mean squared error. */
+cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t steps,
+                       int32_t tiles, float lr, uint64_t seed, float* last_loss, void* stream);
+/* The gradient (summed over tiles) and mean squared error of one step's sample draw, without
+ * updating: for checking the backward kernels. grad is a host array of CC_MLP_NPARAM floats. */
+cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t tiles,
+                      uint64_t seed, int32_t step, float* grad, float* loss, void* stream);
+/* Predictions out[n] for device features feats[n][8]. */
+cc_status cc_mlp_predict(cc_mlp* m, const float* feats, int64_t n, float* out, void* stream);
+/* Training samples from the cut cells of the last update on h (a Float32 marching-cubes handle):
+ * feats[i][8] = corner phi / d[0], plain[i] = its plain volume fraction, labels[i] = the fluid
+ * fraction of marching cubes at 8x sub-refinement of `body` (Float64). Blocking; at most
+ * `capacity` cells, *count receives how many were written. */
+cc_status cc_mc_learned_samples(cc_handle* h, const cc_grid* g, const cc_optape* body, const void* phi,
+                                const cc_cells* cells, float* feats, float* labels, float* plain,
+                                int64_t capacity, int64_t* count, void* stream);
+/* cc_mc_update with the learned correction of cut cells' volume fractions; *n_fallback (if not
+ * NULL; then blocking) receives how many cut cells kept the plain value. */
+cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* body, void* phi,
+                               const cc_cells* cells, const cc_mlp* mlp, float bound, int64_t* n_fallback,
+                               void* stream);
+
 /* Marching cubes from a caller-supplied nodal field WITHOUT allocating: no counterpart in the
  * reference. For callers that may not let a library allocate device memory -- a solver whose
  * device memory comes from its own pool, budgeted up front, or a time-stepping loop where a

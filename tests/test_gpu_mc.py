@@ -30,6 +30,29 @@ def test_sphere_and_csg_bitwise(prec, n):
         assert (cols["kind"] == 2).sum() > 50
 
 
+def smooth_bodies():
+    """Smooth-min tapes: a smooth union of bare primitives (every primitive carries its own k),
+    and one nested with sharp combines, a negation and a subtraction."""
+    yield W.smooth_blob(3), W.unit_grid(35)
+    yield W.smooth_blob(8), cc.CartesianGrid((0.05, -0.02, 0.0), (40, 36, 33), (0.024, 0.029, 0.031))
+    nested = cc.SmoothUnion(cc.Sphere((0.2, 0.1, 0.0), 0.5),
+                            cc.Subtraction(cc.Box((0.0, 0.0, 0.0), (0.6, 0.3, 0.4)), cc.Sphere((0.3, 0.0, 0.2), 0.25)),
+                            cc.Negate(cc.Sphere((0.0, 0.0, 0.0), 1.5)),
+                            cc.Torus((0.0, 0.1, -0.1), 0.55, 0.1, np.eye(3)), k=0.07)
+    yield nested, W.csg_grid(48)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_smooth_min_tapes_bitwise(prec):
+    for body, g in smooth_bodies():
+        tape = cc.flatten(body, 3)
+        phi, cols, _ = run_dev(g, tape, prec)
+        rphi, ref = po.mc_update(g, tape, TABLE, prec)
+        assert np.array_equal(bits(phi), bits(rphi)), "phi differs"
+        assert_cells_bitwise(cols, ref, label="smooth-min")
+        assert (cols["kind"] == 2).sum() > 50
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_random_field_cells_from_phi(prec):
     n = 35

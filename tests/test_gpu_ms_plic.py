@@ -60,7 +60,11 @@ def test_plic_bitwise(prec):
               cc.Union(cc.Circle((0.02, 0.03), 0.31), cc.Box((0.25, 0.10), (0.09, 0.09)))),
              (cc.CartesianGrid((-1.5,) * 3, (24,) * 3, (0.125,) * 3), cc.Sphere((0.01, 0.02, -0.03), 1.0)),
              (cc.workloads.unit_grid(40), cc.workloads.sphere_cloud(1, 64)),
-             (cc.CartesianGrid((-1.5, -1.5), (3, 3), (1.0, 1.0)), cc.Circle((0.0, 0.0), 1.0))]
+             (cc.CartesianGrid((-1.5, -1.5), (3, 3), (1.0, 1.0)), cc.Circle((0.0, 0.0), 1.0)),
+             (cc.workloads.unit_grid(36), cc.workloads.smooth_blob(5)),
+             (cc.CartesianIsoGrid((-0.6, -0.6), (0.6, 0.6), 0.04),
+              cc.SmoothUnion(cc.Circle((0.1, 0.0), 0.3), cc.Box((-0.2, 0.1), (0.15, 0.2)),
+                             cc.Subtraction(cc.Circle((0.0, -0.2), 0.3), cc.Circle((0.0, -0.3), 0.1)), k=0.05))]
     for g, body in cases:
         tape = cc.flatten(body, g.dim)
         cache = cc.update_cache(cc.allocate_cache(g, cc.PLICCutCell(), dtype=DT[prec]), tape, g)
