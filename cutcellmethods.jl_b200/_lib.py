@@ -12,7 +12,7 @@ import threading
 from . import build as _build
 
 CC_OK, CC_DIM_MISMATCH, CC_ANISOTROPIC, CC_BACKEND_MISMATCH, CC_BAD_TAPE, CC_DEVICE_TIMEOUT, \
-    CC_CUDA_ERR, CC_BAD_ARG, CC_BAD_TABLE, CC_NO_TABLE, CC_TOO_LARGE = range(11)
+    CC_CUDA_ERR, CC_BAD_ARG, CC_BAD_TABLE, CC_NO_TABLE, CC_TOO_LARGE, CC_BAD_FILE = range(12)
 CC_F32, CC_F64, CC_MIXED = 0, 1, 2
 CC_MARCHING_SQUARES, CC_MARCHING_CUBES, CC_PLIC = 0, 1, 2
 
@@ -58,13 +58,14 @@ EXPORTS = {
     "cc_mlp_destroy": [C.c_void_p],
     "cc_mlp_set_params": [C.c_void_p, C.c_void_p, C.c_int32],
     "cc_mlp_get_params": [C.c_void_p, C.c_void_p, C.c_int32],
-    "cc_mlp_train": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_float,
-                     C.c_uint64, C.c_void_p, C.c_void_p],
-    "cc_mlp_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint64, C.c_int32,
-                    C.c_void_p, C.c_void_p, C.c_void_p],
-    "cc_mlp_predict": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "cc_mlp_train": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
+                     C.c_int32, C.c_float, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p],
+    "cc_mlp_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
+                    C.c_uint64, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_mlp_predict": [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p],
+    "cc_mlp_read_weights": [C.c_char_p, C.c_void_p, C.c_int32],
     "cc_mc_learned_samples": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                              C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "cc_mc_update_learned": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_float, C.c_void_p, C.c_void_p],
     "cc_version": [],

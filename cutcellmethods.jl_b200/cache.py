@@ -52,7 +52,7 @@ def _check(status):
     if status == _lib.CC_DIM_MISMATCH:
         raise DimensionMismatch(status, msg)
     if status in (_lib.CC_ANISOTROPIC, _lib.CC_BACKEND_MISMATCH, _lib.CC_BAD_ARG, _lib.CC_BAD_TAPE,
-                  _lib.CC_BAD_TABLE, _lib.CC_NO_TABLE, _lib.CC_TOO_LARGE):
+                  _lib.CC_BAD_TABLE, _lib.CC_NO_TABLE, _lib.CC_TOO_LARGE, _lib.CC_BAD_FILE):
         raise ArgumentError(status, msg)
     raise CCError(status, msg)
 

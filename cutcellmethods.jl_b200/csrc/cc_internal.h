@@ -59,15 +59,16 @@ template <class T>
 cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
                                   const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
                                   unsigned long long* fallback, int* err, cudaStream_t s);
-cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, long long n,
-                             unsigned long long seed, int step, int tiles, float* grad, float* loss, int* err,
-                             cudaStream_t s);
+cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, const float* plain,
+                             const float* weights, long long n, unsigned long long seed, int step, int tiles,
+                             bool augment, float* grad, float* loss, int* err, cudaStream_t s);
 cudaError_t launch_mlp_adam(float* P, float* m, float* v, const float* grad, int tiles, int step, float lr,
                             cudaStream_t s);
-cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, float* out, int* err, cudaStream_t s);
+cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, bool correction, float* out, int* err,
+                               cudaStream_t s);
 cudaError_t launch_labels(const DevGrid<double>& g, const DevTape& tape, const float* phi, const float* vf,
                           const DevTable& tb, const unsigned* list, long long n, float* feats, float* labels,
-                          float* plain, cudaStream_t s);
+                          float* plain, int64_t* index, cudaStream_t s);
 
 template <class T>
 cudaError_t launch_ms(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,

@@ -1,12 +1,24 @@
 // learned.cu -- the learned volume-fraction correction on sm_100a tensor cores (tcgen05).
 //
-// A small MLP, 8 -> 64 -> 64 -> 1 with GELU hidden layers and a sigmoid output, maps a cut
-// cell's corner values scaled by the cell size (phi / h, marching-cubes corner order) to a
-// corrected fluid volume fraction. It is trained on the fluid fractions that marching cubes gives
-// the same cells at 8x sub-refinement. Only a cut cell's volume_fraction is replaced; kind and the
-// face fractions stay the plain construction's, so watertightness and the shared-face identities
-// survive. Where the prediction is not finite or strays more than `bound` from the plain value,
-// the plain value is kept.
+// A small MLP, 8 -> 64 -> 64 -> 1 with GELU hidden layers and a sigmoid output p, corrects the
+// fluid volume fraction that marching cubes gives a cut cell from the cell's corner values scaled
+// by the cell size (x = phi / h, marching-cubes corner order). It is trained on the fluid
+// fractions that marching cubes gives the same cells at 8x sub-refinement. Only a cut cell's
+// volume_fraction is replaced; kind and the face fractions stay the plain construction's, so
+// watertightness and the shared-face identities survive. Where the correction is not finite,
+// exceeds `bound` or takes the value out of [0, 1], the plain value is kept.
+//
+// The correction is first order in the curvature. Marching cubes is exact for a planar
+// interface, and its volume error on a curved one is about h / R. In the corner values the
+// curvature shows only as the four non-linear Walsh components q (the xy, xz, yz and xyz
+// patterns of the 8 corners), of size about h / R. Scale-free features cannot tell a fine
+// grid's small correction from a coarse grid's large one, so a network fed x directly, trained on
+// coarse grids, over-corrects fine ones. So the network sees x with its non-linear part rescaled
+// to a fixed norm K0,
+//     x~ = lin(x) + quad(x) K0 / |quad(x)|,      s = |quad(x)| / K0,
+// and the correction is homogeneous of degree one in the curvature:
+//     corrected = plain + s * CORR * (2 p(x~) - 1),      CORR = CC_MLP_CORRECTION_SCALE.
+// A planar cell (quad = 0) is left as it is.
 //
 // Every GEMM runs on the 5th-generation tensor cores: BF16 operands staged in shared memory in the
 // K-major "interleaved" layout (8-row x 16-byte core matrices), FP32 accumulators in tensor memory
@@ -15,15 +27,25 @@
 // A CTA works on tiles of 128 samples (the MMA's M): row t of every activation tile is sample t,
 // which thread t owns.
 //
-//   forward   H1 = X W1^T (K 16)        A1 = gelu(H1 + b1)
-//             H2 = A1 W2^T (K 64)       z = gelu(H2 + b2) . w3 + b3,  p = sigmoid(z)
+// Precision. The curvature of the interface shows in the corner values only as second
+// differences of order (h / R) -- a few 1e-3 of the values themselves on fine grids, below one
+// BF16 rounding step. So the forward GEMMs run split: every operand v is a BF16 pair
+// hi = bf16(v), lo = bf16(v - hi), and a product is hi*hi + lo*hi + hi*lo (three MMAs into the
+// same FP32 accumulator), about 16 significant bits. The backward GEMMs use the high parts only
+// (a gradient needs no such precision).
+//
+//   forward   H1 = X W1^T (K 16, x3)     A1 = gelu(H1 + b1)
+//             H2 = A1 W2^T (K 64, x3)    z = gelu(H2 + b2) . w3 + b3,  p = sigmoid(z)
 //   backward  dW2 = dH2^T A1 (K = 128 samples),  dA1 = dH2 W2 (K 64),  dW1 = dH1^T X (K = 128)
 //
-// Training writes per-CTA partial gradients to fixed slots and a second kernel sums them in CTA
-// order and takes an Adam step, so training is deterministic.
+// Training minimises the mean over a step's samples of w |c - (label - plain)| (c the correction
+// above, w a per-sample weight), or, without plain fractions, the mean squared error of p
+// against the labels (the network alone). It writes per-CTA partial gradients to fixed slots and
+// a second kernel sums them in CTA order and takes an Adam step, so training is deterministic.
 #include <cstdint>
 #include <cstring>
 #include <cuda_bf16.h>
+#include "../../include/cutcell_b200.h"
 #include "cc_device.cuh"
 #include "cc_internal.h"
 #include "mc_cell.cuh"
@@ -39,6 +61,8 @@ using cci::DevTape;
 constexpr int TILE = 128;  // samples per tile = MMA M = threads per CTA
 constexpr int H = 64;      // hidden width
 constexpr int KIN = 16;    // 8 inputs padded to one K step
+constexpr float CORR = CC_MLP_CORRECTION_SCALE;
+constexpr float K0 = CC_MLP_CURVATURE_NORM;
 
 // FP32 parameter vector layout
 constexpr int P_W1 = 0;            // [64][8]  (row = output unit)
@@ -48,6 +72,7 @@ constexpr int P_B2 = P_W2 + 64 * 64;
 constexpr int P_W3 = P_B2 + 64;    // [64]
 constexpr int P_B3 = P_W3 + 64;
 constexpr int NPARAM = P_B3 + 1;   // 4801
+static_assert(NPARAM == CC_MLP_NPARAM, "parameter layout");
 
 constexpr long long WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a tile gives up
 
@@ -128,19 +153,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 __device__ __forceinline__ int kmaj(int r, int k, int K) {
   return ((((r >> 3) * (K >> 3)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
 }
-__device__ __forceinline__ void put_bf16(unsigned char* tile, int r, int k, int K, float v) {
-  *reinterpret_cast<__nv_bfloat16*>(tile + kmaj(r, k, K)) = __float2bfloat16_rn(v);
+__device__ __forceinline__ unsigned short bf16_bits(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+__device__ __forceinline__ float bf16_val(unsigned short b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
+// v = hi + lo to about 16 significant bits, both BF16
+__device__ __forceinline__ void split_bf16(float v, unsigned short& hi, unsigned short& lo) {
+  hi = bf16_bits(v);
+  lo = bf16_bits(v - bf16_val(hi));
 }
-// D[M x N] (+)= A[M x K] B[N x K]^T over K / 16 MMAs; tiles in the layout above.
+__device__ __forceinline__ void put_bits(unsigned char* tile, int r, int k, int K, unsigned short b) {
+  *reinterpret_cast<unsigned short*>(tile + kmaj(r, k, K)) = b;
+}
+__device__ __forceinline__ void put_bf16(unsigned char* tile, int r, int k, int K, float v) {
+  put_bits(tile, r, k, K, bf16_bits(v));
+}
+// Row r, columns k0..k0+7 (k0 a multiple of 8): one 16-byte store.
+__device__ __forceinline__ void put_row8(unsigned char* tile, int r, int k0, int K, const unsigned short (&b)[8]) {
+  uint4 w;
+  w.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
+  w.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
+  w.z = (uint32_t)b[4] | ((uint32_t)b[5] << 16);
+  w.w = (uint32_t)b[6] | ((uint32_t)b[7] << 16);
+  *reinterpret_cast<uint4*>(tile + kmaj(r, k0, K)) = w;
+}
+// D[M x N] (+)= A[M x K] B[N x K]^T over K / 16 MMAs; tiles in the layout above. With acc false
+// the first MMA overwrites D.
 __device__ __forceinline__ void gemm_kmaj(uint32_t tmem_d, const unsigned char* A, const unsigned char* B, int M,
-                                          int N, int K) {
+                                          int N, int K, bool acc) {
   const uint32_t idesc = umma_idesc(M, N);
   const uint32_t sbo = (uint32_t)(K / 8) * 128u;
   for (int s = 0; s < K / 16; ++s) {
     const uint64_t da = umma_desc(smem_u32(A) + 256u * s, 128u, sbo);
     const uint64_t db = umma_desc(smem_u32(B) + 256u * s, 128u, sbo);
-    umma_bf16(tmem_d, da, db, idesc, s > 0 ? 1u : 0u);
+    umma_bf16(tmem_d, da, db, idesc, (acc || s > 0) ? 1u : 0u);
   }
+}
+// D = A B^T in split precision: Ah Bh + Al Bh + Ah Bl.
+__device__ __forceinline__ void gemm_split(uint32_t tmem_d, const unsigned char* Ah, const unsigned char* Al,
+                                           const unsigned char* Bh, const unsigned char* Bl, int M, int N, int K) {
+  gemm_kmaj(tmem_d, Ah, Bh, M, N, K, false);
+  gemm_kmaj(tmem_d, Al, Bh, M, N, K, true);
+  gemm_kmaj(tmem_d, Ah, Bl, M, N, K, true);
 }
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -150,100 +202,135 @@ __device__ __forceinline__ float gelu_grad(float x) {
 
 // Shared-memory layout (bytes) of an MLP CTA.
 struct MlpLayout {
-  static constexpr int X = 0;                          // [128 x 16] bf16
-  static constexpr int W1 = X + TILE * KIN * 2;        // [64 x 16]
-  static constexpr int A1 = W1 + H * KIN * 2;          // [128 x 64]
-  static constexpr int W2 = A1 + TILE * H * 2;         // [64 x 64]
-  static constexpr int W2T = W2 + H * H * 2;           // [64 x 64] (training)
-  static constexpr int DH2 = W2T + H * H * 2;          // [128 x 64]
-  static constexpr int DH2T = DH2 + TILE * H * 2;      // [128 x 128], rows 64.. zero
-  static constexpr int A1T = DH2T + TILE * TILE * 2;   // [64 x 128]
-  static constexpr int DH1T = A1T + H * TILE * 2;      // [128 x 128], rows 64.. zero
-  static constexpr int XT = DH1T + TILE * TILE * 2;    // [16 x 128], rows 8.. zero
-  static constexpr int H1 = XT + KIN * TILE * 2;       // f32 [128][65]
-  static constexpr int PAR = H1 + TILE * 65 * 4;       // f32 b1[64] b2[64] w3[64] b3, then 4 scratch
-  static constexpr int PAR_FLOATS = 3 * H + 8;
-  static constexpr int MISC = PAR + PAR_FLOATS * 4;    // mbarrier, tmem base, flags
-  static constexpr int INFER_BYTES = W2T;              // inference needs X, W1, A1, W2 only
+  static constexpr int XH = 0;                          // [128 x 16] inputs, high parts
+  static constexpr int XL = XH + TILE * KIN * 2;        // low parts
+  static constexpr int W1H = XL + TILE * KIN * 2;       // [64 x 16]
+  static constexpr int W1L = W1H + H * KIN * 2;
+  static constexpr int A1H = W1L + H * KIN * 2;         // [128 x 64]
+  static constexpr int A1L = A1H + TILE * H * 2;
+  static constexpr int W2H = A1L + TILE * H * 2;        // [64 x 64]
+  static constexpr int W2L = W2H + H * H * 2;
+  static constexpr int INFER_BYTES = W2L + H * H * 2;   // all that inference reads
+  static constexpr int W2T = INFER_BYTES;               // [64 x 64] W2^T, high parts (training)
+  static constexpr int DH2 = W2T + H * H * 2;           // [128 x 64]
+  static constexpr int DH2T = DH2 + TILE * H * 2;       // [128 x 128], rows 64.. zero
+  static constexpr int A1T = DH2T + TILE * TILE * 2;    // [64 x 128], high parts
+  static constexpr int DH1T = A1T + H * TILE * 2;       // [128 x 128], rows 64.. zero
+  static constexpr int XT = DH1T + TILE * TILE * 2;     // [16 x 128]: rows 0..7 high, 8..15 low parts
+  static constexpr int H1 = XT + KIN * TILE * 2;        // f32 [128][65]
+  static constexpr int TRAIN_PAR = H1 + TILE * 65 * 4;
+  static constexpr int PAR_FLOATS = 3 * H + 8;          // b1[64] b2[64] w3[64] b3, then 4 scratch
+  static constexpr int RED_FLOATS = 4 * 3 * H;          // per-warp partial sums of db1, db2, dw3
   static constexpr int INFER_SMEM = INFER_BYTES + PAR_FLOATS * 4 + 64;
-  static constexpr int TRAIN_BYTES = MISC + 64;
+  static constexpr int TRAIN_BYTES = TRAIN_PAR + (PAR_FLOATS + RED_FLOATS) * 4 + 64;
 };
+static_assert(MlpLayout::TRAIN_BYTES <= 227 * 1024, "training CTA exceeds shared memory");
 
 struct MlpShared {
   unsigned char* base;
   float* par;
+  float* red;  // training only
   uint64_t* mbar;
   uint32_t* tmem;
-  int* flag;
 };
 
 __device__ __forceinline__ MlpShared mlp_shared(unsigned char* smem, bool train) {
   MlpShared s;
   s.base = smem;
-  const int misc = train ? MlpLayout::MISC : MlpLayout::INFER_BYTES + MlpLayout::PAR_FLOATS * 4;
-  s.par = reinterpret_cast<float*>(smem + (train ? MlpLayout::PAR : MlpLayout::INFER_BYTES));
+  const int par = train ? MlpLayout::TRAIN_PAR : MlpLayout::INFER_BYTES;
+  s.par = reinterpret_cast<float*>(smem + par);
+  s.red = s.par + MlpLayout::PAR_FLOATS;
+  const int misc = par + (MlpLayout::PAR_FLOATS + (train ? MlpLayout::RED_FLOATS : 0)) * 4;
   s.mbar = reinterpret_cast<uint64_t*>(smem + ((misc + 7) / 8) * 8);
   s.tmem = reinterpret_cast<uint32_t*>(s.mbar + 1);
-  s.flag = reinterpret_cast<int*>(s.tmem + 1);
   return s;
 }
 
-// Stage the weights (FP32 master copy -> BF16 tiles) and biases of the network.
+// Stage the weights (FP32 master copy -> BF16 high/low tiles) and biases of the network.
 __device__ void stage_weights(const float* __restrict__ P, const MlpShared& s, bool train) {
   unsigned char* b = s.base;
   for (int e = threadIdx.x; e < H * KIN; e += TILE) {
     const int j = e / KIN, k = e % KIN;
-    put_bf16(b + MlpLayout::W1, j, k, KIN, k < 8 ? P[P_W1 + j * 8 + k] : 0.0f);
+    unsigned short hi, lo;
+    split_bf16(k < 8 ? P[P_W1 + j * 8 + k] : 0.0f, hi, lo);
+    put_bits(b + MlpLayout::W1H, j, k, KIN, hi);
+    put_bits(b + MlpLayout::W1L, j, k, KIN, lo);
   }
   for (int e = threadIdx.x; e < H * H; e += TILE) {
     const int j = e / H, i = e % H;
-    const float w = P[P_W2 + j * H + i];
-    put_bf16(b + MlpLayout::W2, j, i, H, w);
-    if (train) put_bf16(b + MlpLayout::W2T, i, j, H, w);
+    unsigned short hi, lo;
+    split_bf16(P[P_W2 + j * H + i], hi, lo);
+    put_bits(b + MlpLayout::W2H, j, i, H, hi);
+    put_bits(b + MlpLayout::W2L, j, i, H, lo);
+    if (train) put_bits(b + MlpLayout::W2T, i, j, H, hi);
   }
   // par: b1[64], b2[64], w3[64], b3
   for (int e = threadIdx.x; e < 3 * H + 1; e += TILE)
     s.par[e] = e < H ? P[P_B1 + e] : e < 2 * H ? P[P_B2 + e - H] : e < 3 * H ? P[P_W3 + e - 2 * H] : P[P_B3];
 }
 
-// One tile's forward pass. x: this thread's 8 inputs (zeros for a padding row). Returns p and, in
-// training, keeps what the backward pass needs in shared memory / TMEM. `phase` is the running
-// mbarrier parity. Returns false if an MMA never completed.
-__device__ bool mlp_forward(const MlpShared& s, uint32_t tmem, const float x[8], bool train, uint32_t& phase, float& z_out) {
+// Wait for the MMAs committed to the CTA's mbarrier; false on every thread if any thread's wait
+// ran out.
+__device__ __forceinline__ bool mma_done(const MlpShared& s, uint32_t& phase) {
+  const bool ok = mbar_wait(s.mbar, phase);
+  phase ^= 1u;
+  if (__syncthreads_or(!ok)) return false;
+  tc_fence_after();
+  return true;
+}
+
+// One tile's forward pass. x: this thread's 8 inputs (zeros for a padding row). In training,
+// keeps what the backward pass needs in shared memory and the H2 accumulator in TMEM columns
+// 0..63. `phase` is the running mbarrier parity. Returns false if an MMA never completed.
+__device__ bool mlp_forward(const MlpShared& s, uint32_t tmem, const float x[8], bool train, uint32_t& phase,
+                            float& z_out) {
   unsigned char* b = s.base;
   const int t = threadIdx.x;
+  {
+    unsigned short hi[8], lo[8];
+    const unsigned short zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int k = 0; k < KIN; ++k) put_bf16(b + MlpLayout::X, t, k, KIN, k < 8 ? x[k] : 0.0f);
-  if (train) {
+    for (int k = 0; k < 8; ++k) split_bf16(x[k], hi[k], lo[k]);
+    put_row8(b + MlpLayout::XH, t, 0, KIN, hi);
+    put_row8(b + MlpLayout::XH, t, 8, KIN, zero);
+    put_row8(b + MlpLayout::XL, t, 0, KIN, lo);
+    put_row8(b + MlpLayout::XL, t, 8, KIN, zero);
+    if (train) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) put_bf16(b + MlpLayout::XT, k, t, TILE, x[k]);
+      for (int k = 0; k < 8; ++k) {
+        put_bits(b + MlpLayout::XT, k, t, TILE, hi[k]);
+        put_bits(b + MlpLayout::XT, 8 + k, t, TILE, lo[k]);
+      }
+    }
   }
   fence_async_smem();
   __syncthreads();
   if (t == 0) {
     tc_fence_after();
-    gemm_kmaj(tmem, b + MlpLayout::X, b + MlpLayout::W1, TILE, H, KIN);
+    gemm_split(tmem, b + MlpLayout::XH, b + MlpLayout::XL, b + MlpLayout::W1H, b + MlpLayout::W1L, TILE, H, KIN);
     umma_commit(s.mbar);
   }
-  const bool ok1 = mbar_wait(s.mbar, phase);
-  phase ^= 1u;
-  if (__syncthreads_or(!ok1)) return false;
-  tc_fence_after();
+  if (!mma_done(s, phase)) return false;
   const uint32_t lane_addr = tmem + ((uint32_t)(32 * (t / 32)) << 16);
   float* h1row = reinterpret_cast<float*>(b + MlpLayout::H1) + t * 65;
   for (int c = 0; c < H / 16; ++c) {
     float v[16];
     tmem_ld16(lane_addr + 16 * c, v);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int j = 16 * c + q;
-      const float h = v[q] + s.par[j];
-      const float a = gelu(h);
-      put_bf16(b + MlpLayout::A1, t, j, H, a);
-      if (train) {
-        h1row[j] = h;
-        put_bf16(b + MlpLayout::A1T, j, t, TILE, a);
+    for (int half = 0; half < 2; ++half) {
+      unsigned short hi[8], lo[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = 16 * c + 8 * half + q;
+        const float h = v[8 * half + q] + s.par[j];
+        split_bf16(gelu(h), hi[q], lo[q]);
+        if (train) {
+          h1row[j] = h;
+          put_bits(b + MlpLayout::A1T, j, t, TILE, hi[q]);
+        }
       }
+      put_row8(b + MlpLayout::A1H, t, 16 * c + 8 * half, H, hi);
+      put_row8(b + MlpLayout::A1L, t, 16 * c + 8 * half, H, lo);
     }
   }
   tc_fence_before();
@@ -251,13 +338,10 @@ __device__ bool mlp_forward(const MlpShared& s, uint32_t tmem, const float x[8],
   __syncthreads();
   if (t == 0) {
     tc_fence_after();
-    gemm_kmaj(tmem, b + MlpLayout::A1, b + MlpLayout::W2, TILE, H, H);
+    gemm_split(tmem, b + MlpLayout::A1H, b + MlpLayout::A1L, b + MlpLayout::W2H, b + MlpLayout::W2L, TILE, H, H);
     umma_commit(s.mbar);
   }
-  const bool ok2 = mbar_wait(s.mbar, phase);
-  phase ^= 1u;
-  if (__syncthreads_or(!ok2)) return false;
-  tc_fence_after();
+  if (!mma_done(s, phase)) return false;
   float z = 0.0f;
   for (int c = 0; c < H / 16; ++c) {
     float v[16];
@@ -274,37 +358,90 @@ __device__ bool mlp_forward(const MlpShared& s, uint32_t tmem, const float x[8],
 
 __device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
 
-// Sum over the 128 threads of the CTA, in a fixed order; every thread gets the result.
-__device__ __forceinline__ float cta_sum(float v, float* red) {
+__device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// Sum over the 128 threads of the CTA, in a fixed order; every thread gets the result.
+__device__ __forceinline__ float cta_sum(float v, float* red4) {
+  v = warp_sum(v);
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = v;
+  if ((threadIdx.x & 31) == 0) red4[threadIdx.x / 32] = v;
   __syncthreads();
-  const float r = (red[0] + red[1]) + (red[2] + red[3]);
+  const float r = (red4[0] + red4[1]) + (red4[2] + red4[3]);
   __syncthreads();
   return r;
+}
+
+// The image of marching-cubes corner c under cube symmetry `sym` (0..47): the axes permuted by
+// sym % 6, then reflected along the axes whose bit is set in sym / 6. Corner bits in
+// marching-cubes order: c0 (0,0,0) c1 (1,0,0) c2 (1,1,0) c3 (0,1,0), c4..c7 the same at z = 1.
+__device__ __forceinline__ int sym_corner(int c, unsigned sym) {
+  const int b[3] = {((c & 3) == 1 || (c & 3) == 2) ? 1 : 0, (c & 3) >= 2 ? 1 : 0, c >= 4 ? 1 : 0};
+  const unsigned char perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  const unsigned pi = sym % 6u, f = sym / 6u;
+  int o[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) o[a] = b[perm[pi][a]] ^ (int)((f >> a) & 1u);
+  return 4 * o[2] + (o[1] ? (o[0] ? 2 : 3) : (o[0] ? 1 : 0));
+}
+
+// The network input of a cell, x~ = lin(x) + quad(x) K0 / |quad(x)|, and the scale s = |quad(x)| /
+// K0 of its correction (0 for a cell whose corner values are exactly trilinear-free, which keeps
+// x). quad(x) is the projection of x on the corner patterns sx*sy, sx*sz, sy*sz and sx*sy*sz
+// (s = -1 / +1 per corner bit), which are orthogonal to the constant and linear ones.
+__device__ __forceinline__ void homogenize(const float x[8], float xt[8], float& s) {
+  const float sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+  const float sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+  const float sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  float qxy = 0.0f, qxz = 0.0f, qyz = 0.0f, qxyz = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    qxy += sx[c] * sy[c] * x[c];
+    qxz += sx[c] * sz[c] * x[c];
+    qyz += sy[c] * sz[c] * x[c];
+    qxyz += sx[c] * sy[c] * sz[c] * x[c];
+  }
+  qxy *= 0.125f; qxz *= 0.125f; qyz *= 0.125f; qxyz *= 0.125f;
+  float quad[8], nn = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    quad[c] = qxy * (sx[c] * sy[c]) + qxz * (sx[c] * sz[c]) + qyz * (sy[c] * sz[c]) + qxyz * (sx[c] * sy[c] * sz[c]);
+    nn += quad[c] * quad[c];
+  }
+  const float qn = sqrtf(nn);
+  if (!(qn > 0.0f)) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) xt[c] = x[c];
+    s = 0.0f;
+    return;
+  }
+  const float f = K0 / qn - 1.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) xt[c] = x[c] + quad[c] * f;
+  s = qn / K0;
 }
 
 // ---------------------------------------------------------------------------------------------
 // Training: one tile of 128 samples per CTA per step; per-CTA partial gradients in grad[cta][].
 __global__ void __launch_bounds__(TILE, 1)
     mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ feats, const float* __restrict__ labels,
-                     long long n, unsigned long long seed, int step, float inv_batch, float* __restrict__ grad,
+                     const float* __restrict__ plain, const float* __restrict__ weights, long long n,
+                     unsigned long long seed, int step, int augment, float inv_batch, float* __restrict__ grad,
                      float* __restrict__ loss, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem[];
   const MlpShared s = mlp_shared(smem, true);
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, warp = t / 32, lane = t & 31;
   unsigned char* b = s.base;
   stage_weights(P, s, true);
   // rows 64..127 of the transposed gradient tiles stay zero (M is padded to 128)
   for (int e = t; e < TILE * TILE / 2; e += TILE) {
     const int r = 64 + e / TILE, k = e % TILE;
-    put_bf16(b + MlpLayout::DH2T, r, k, TILE, 0.0f);
-    put_bf16(b + MlpLayout::DH1T, r, k, TILE, 0.0f);
+    put_bits(b + MlpLayout::DH2T, r, k, TILE, 0);
+    put_bits(b + MlpLayout::DH1T, r, k, TILE, 0);
   }
-  for (int e = t; e < 8 * TILE; e += TILE) put_bf16(b + MlpLayout::XT, 8 + e / TILE, e % TILE, TILE, 0.0f);
-  if (t == 0) { mbar_init(s.mbar, 1); *s.flag = 0; }
+  if (t == 0) mbar_init(s.mbar, 1);
   if (t < 32) { tmem_alloc(s.tmem, 128); tmem_relinquish(); }
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   tc_fence_before();
@@ -312,47 +449,73 @@ __global__ void __launch_bounds__(TILE, 1)
   tc_fence_after();
   const uint32_t tmem = *s.tmem;
   uint32_t phase = 0;
-  float* red = s.par + 3 * H + 4;  // 4 floats of scratch past b3
+  float* red4 = s.par + 3 * H + 4;  // 4 floats of scratch past b3
   float* g = grad + (long long)blockIdx.x * NPARAM;
 
-  // the sample: a counter-based hash of (seed, step, slot), uniform over the data set
+  // the sample: a counter-based hash of (seed, step, slot), uniform over the data set; its high
+  // bits pick the cube symmetry applied to it
   unsigned long long hsh = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(step * (long long)gridDim.x * TILE +
                                                                                   blockIdx.x * TILE + t + 1));
   hsh ^= hsh >> 33; hsh *= 0xff51afd7ed558ccdull; hsh ^= hsh >> 33; hsh *= 0xc4ceb9fe1a85ec53ull; hsh ^= hsh >> 33;
   const long long idx = (long long)(hsh % (unsigned long long)n);
-  float x[8];
+  const unsigned sym = augment ? (unsigned)((hsh >> 40) % 48ull) : 0u;
+  float xr[8], x[8], sc = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) x[k] = feats[idx * 8 + k];
-  const float y = labels[idx];
+  for (int k = 0; k < 8; ++k) xr[sym_corner(k, sym)] = feats[idx * 8 + k];
+  const bool corr_mode = plain != nullptr;
+  if (corr_mode) homogenize(xr, x, sc);
+  else {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = xr[k];
+  }
+  // the target: p itself, or the correction that turns the plain fraction into the label
+  const float y = corr_mode ? labels[idx] - plain[idx] : labels[idx];
+  const float w = weights ? weights[idx] : 1.0f;
 
   bool ok = true;
   float z = 0.0f;
   do {
     if (!mlp_forward(s, tmem, x, true, phase, z)) { ok = false; break; }
     const float p = sigmoidf_(z);
-    const float e = p - y;
-    const float l = cta_sum(e * e, red);
+    float l, dz;
+    if (corr_mode) {  // w |c - y|, c = s CORR (2p - 1)
+      const float e = sc * CORR * (2.0f * p - 1.0f) - y;
+      const float sg = e > 0.0f ? 1.0f : (e < 0.0f ? -1.0f : 0.0f);
+      l = w * fabsf(e);
+      dz = inv_batch * w * sg * sc * (2.0f * CORR) * p * (1.0f - p);
+    } else {          // w (p - y)^2
+      const float e = p - y;
+      l = w * e * e;
+      dz = 2.0f * e * inv_batch * w * p * (1.0f - p);
+    }
+    l = cta_sum(l, red4);
     if (t == 0) loss[blockIdx.x] = l;
-    const float dz = 2.0f * e * inv_batch * p * (1.0f - p);
-    const float db3 = cta_sum(dz, red);
+    const float db3 = cta_sum(dz, red4);
     if (t == 0) g[P_B3] = db3;
     // layer 3 and the gradient into H2, from the still-resident H2 accumulator in TMEM
-    const uint32_t lane_addr = tmem + ((uint32_t)(32 * (t / 32)) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
     for (int c = 0; c < H / 16; ++c) {
       float v[16];
       tmem_ld16(lane_addr + 16 * c, v);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int j = 16 * c + q;
-        const float h2 = v[q] + s.par[H + j];
-        const float a2 = gelu(h2);
-        const float dw3 = cta_sum(dz * a2, red);
-        if (t == 0) g[P_W3 + j] = dw3;
-        const float dh2 = dz * s.par[2 * H + j] * gelu_grad(h2);
-        const float db2 = cta_sum(dh2, red);
-        if (t == 0) g[P_B2 + j] = db2;
-        put_bf16(b + MlpLayout::DH2, t, j, H, dh2);
-        put_bf16(b + MlpLayout::DH2T, j, t, TILE, dh2);
+      for (int half = 0; half < 2; ++half) {
+        unsigned short d16[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = 16 * c + 8 * half + q;
+          const float h2 = v[8 * half + q] + s.par[H + j];
+          const float a2 = gelu(h2);
+          const float dw3 = warp_sum(dz * a2);
+          const float dh2 = dz * s.par[2 * H + j] * gelu_grad(h2);
+          const float db2 = warp_sum(dh2);
+          if (lane == 0) {
+            s.red[(warp * 3 + 2) * H + j] = dw3;
+            s.red[(warp * 3 + 1) * H + j] = db2;
+          }
+          d16[q] = bf16_bits(dh2);
+          put_bits(b + MlpLayout::DH2T, j, t, TILE, d16[q]);
+        }
+        put_row8(b + MlpLayout::DH2, t, 16 * c + 8 * half, H, d16);
       }
     }
     tc_fence_before();
@@ -360,14 +523,11 @@ __global__ void __launch_bounds__(TILE, 1)
     __syncthreads();
     if (t == 0) {
       tc_fence_after();
-      gemm_kmaj(tmem, b + MlpLayout::DH2T, b + MlpLayout::A1T, TILE, H, TILE);       // dW2 -> cols 0..63
-      gemm_kmaj(tmem + H, b + MlpLayout::DH2, b + MlpLayout::W2T, TILE, H, H);       // dA1 -> cols 64..127
+      gemm_kmaj(tmem, b + MlpLayout::DH2T, b + MlpLayout::A1T, TILE, H, TILE, false);   // dW2 -> cols 0..63
+      gemm_kmaj(tmem + H, b + MlpLayout::DH2, b + MlpLayout::W2T, TILE, H, H, false);   // dA1 -> cols 64..127
       umma_commit(s.mbar);
     }
-    const bool ok3 = mbar_wait(s.mbar, phase);
-    phase ^= 1u;
-    if (__syncthreads_or(!ok3)) { ok = false; break; }
-    tc_fence_after();
+    if (!mma_done(s, phase)) { ok = false; break; }
     const float* h1row = reinterpret_cast<const float*>(b + MlpLayout::H1) + t * 65;
     for (int c = 0; c < H / 16; ++c) {
       float v[16];
@@ -376,8 +536,8 @@ __global__ void __launch_bounds__(TILE, 1)
       for (int q = 0; q < 16; ++q) {
         const int i = 16 * c + q;
         const float dh1 = v[q] * gelu_grad(h1row[i]);
-        const float db1 = cta_sum(dh1, red);
-        if (t == 0) g[P_B1 + i] = db1;
+        const float db1 = warp_sum(dh1);
+        if (lane == 0) s.red[(warp * 3 + 0) * H + i] = db1;
         put_bf16(b + MlpLayout::DH1T, i, t, TILE, dh1);
       }
     }
@@ -394,18 +554,20 @@ __global__ void __launch_bounds__(TILE, 1)
     __syncthreads();
     if (t == 0) {
       tc_fence_after();
-      gemm_kmaj(tmem, b + MlpLayout::DH1T, b + MlpLayout::XT, TILE, KIN, TILE);    // dW1 -> cols 0..15
+      gemm_kmaj(tmem, b + MlpLayout::DH1T, b + MlpLayout::XT, TILE, KIN, TILE, false);  // dW1 -> cols 0..15
       umma_commit(s.mbar);
     }
-    const bool ok4 = mbar_wait(s.mbar, phase);
-    phase ^= 1u;
-    if (__syncthreads_or(!ok4)) { ok = false; break; }
-    tc_fence_after();
+    if (!mma_done(s, phase)) { ok = false; break; }
     if (t < 64) {
       float v[16];
       tmem_ld16(lane_addr, v);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) g[P_W1 + t * 8 + k] = v[k];
+      for (int k = 0; k < 8; ++k) g[P_W1 + t * 8 + k] = v[k] + v[8 + k];  // high + low parts of x
+      // the bias and output-weight gradients: the four warps' partial sums, in warp order
+      const float* r = s.red;
+      g[P_B1 + t] = (r[0 * H + t] + r[3 * H + t]) + (r[6 * H + t] + r[9 * H + t]);
+      g[P_B2 + t] = (r[1 * H + t] + r[4 * H + t]) + (r[7 * H + t] + r[10 * H + t]);
+      g[P_W3 + t] = (r[2 * H + t] + r[5 * H + t]) + (r[8 * H + t] + r[11 * H + t]);
     }
   } while (false);
   if (!ok && t == 0) atomicExch(err, 1);
@@ -431,10 +593,11 @@ __global__ void mlp_adam_kernel(float* __restrict__ P, float* __restrict__ m, fl
   P[i] -= lr * mh / (sqrtf(vh) + eps);
 }
 
-// Forward only, over given samples (the inference path without the cut construction).
-__global__ void __launch_bounds__(TILE, 1)
-    mlp_predict_kernel(const float* __restrict__ P, const float* __restrict__ feats, long long n, float* __restrict__ out,
-                       int* __restrict__ err) {
+// Forward only, over given samples (the inference path without the cut construction): p, or with
+// `correction` the correction s CORR (2p - 1) of the homogenized features.
+__global__ void __launch_bounds__(TILE)
+    mlp_predict_kernel(const float* __restrict__ P, const float* __restrict__ feats, long long n, int correction,
+                       float* __restrict__ out, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem[];
   const MlpShared s = mlp_shared(smem, false);
   const int t = threadIdx.x;
@@ -450,12 +613,20 @@ __global__ void __launch_bounds__(TILE, 1)
   bool ok = true;
   for (long long base = (long long)blockIdx.x * TILE; base < n; base += (long long)gridDim.x * TILE) {
     const long long q = base + t;
-    float x[8];
+    float xr[8], x[8], sc = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) x[k] = q < n ? feats[q * 8 + k] : 0.0f;
+    for (int k = 0; k < 8; ++k) xr[k] = q < n ? feats[q * 8 + k] : 0.0f;
+    if (correction) homogenize(xr, x, sc);
+    else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = xr[k];
+    }
     float z;
     if (!mlp_forward(s, tmem, x, false, phase, z)) { ok = false; break; }
-    if (q < n) out[q] = sigmoidf_(z);
+    if (q < n) {
+      const float p = sigmoidf_(z);
+      out[q] = correction ? sc * CORR * (2.0f * p - 1.0f) : p;
+    }
     tc_fence_before();
     __syncthreads();
   }
@@ -468,7 +639,7 @@ __global__ void __launch_bounds__(TILE, 1)
 // ---------------------------------------------------------------------------------------------
 // Fused cut-band kernel with the learned correction: each CTA takes tiles of 128 listed cut cells,
 // one per thread, builds their plain moments (writing every field), then runs the network on the
-// tile and replaces the volume fraction where the prediction is accepted.
+// tile and replaces the volume fraction where the correction is accepted.
 template <class T>
 struct LearnedArgs {
   DevGrid<T> g;
@@ -484,7 +655,7 @@ struct LearnedArgs {
 };
 
 template <class T>
-__global__ void __launch_bounds__(TILE, 1) mc_cut_learned_kernel(const LearnedArgs<T> A) {
+__global__ void __launch_bounds__(TILE) mc_cut_learned_kernel(const LearnedArgs<T> A) {
   extern __shared__ __align__(128) unsigned char smem[];
   const MlpShared s = mlp_shared(smem, false);
   const int t = threadIdx.x;
@@ -514,7 +685,7 @@ __global__ void __launch_bounds__(TILE, 1) mc_cut_learned_kernel(const LearnedAr
   bool ok = true;
   for (long long base = (long long)blockIdx.x * TILE; base < total; base += (long long)gridDim.x * TILE) {
     const long long q = base + t;
-    float x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float x[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sc = 0.0f;
     long long ci = -1;
     T plain = T(0);
     if (q < total) {
@@ -530,15 +701,19 @@ __global__ void __launch_bounds__(TILE, 1) mc_cut_learned_kernel(const LearnedAr
                       node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
       mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
       plain = st.vf[ci];
+      float xr[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) x[c] = float(ph[c]) * inv_h;
+      for (int c = 0; c < 8; ++c) xr[c] = float(ph[c]) * inv_h;
+      homogenize(xr, x, sc);
     }
     float z;
     if (!mlp_forward(s, tmem, x, false, phase, z)) { ok = false; break; }
     if (q < total) {
       const float p = sigmoidf_(z);
-      const bool accept = p >= 0.0f && p <= 1.0f && fabsf(p - float(plain)) <= A.bound;
-      if (accept) st.vf[ci] = T(p);
+      const float corr = sc * CORR * (2.0f * p - 1.0f);
+      const T v = plain + T(corr);
+      const bool accept = isfinite(corr) && fabsf(corr) <= A.bound && v >= T(0) && v <= T(1);
+      if (accept) st.vf[ci] = v;
       else ++fb;
     }
     tc_fence_before();
@@ -553,7 +728,7 @@ __global__ void __launch_bounds__(TILE, 1) mc_cut_learned_kernel(const LearnedAr
 
 // ---------------------------------------------------------------------------------------------
 // Training samples: for each listed cut cell, its features (8 corner phi / h), its plain volume
-// fraction and the label -- the fluid fraction marching cubes gives it at 8x sub-refinement, the
+// fraction, its linear index and the label -- the fluid fraction marching cubes gives it at 8x sub-refinement, the
 // body resampled at the 9^3 sub-nodes (Float64, on the global refined lattice x0 + m d/8).
 constexpr int LBL_NT = 128;
 constexpr int LBL_SUB_BYTES = ((729 * 8 + 15) / 16) * 16;  // staged columns then start 16-byte aligned
@@ -561,7 +736,7 @@ __global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, 
                                                       const float* __restrict__ vf, const DevTable tb,
                                                       const unsigned* __restrict__ list, long long n,
                                                       float* __restrict__ feats, float* __restrict__ labels,
-                                                      float* __restrict__ plain) {
+                                                      float* __restrict__ plain, int64_t* __restrict__ index) {
   extern __shared__ __align__(128) unsigned char smem[];
   double* sub = reinterpret_cast<double*>(smem);                    // 729 sub-node values
   unsigned char* stg = smem + LBL_SUB_BYTES;                        // one cell slot per thread
@@ -618,6 +793,7 @@ __global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, 
     if (threadIdx.x == 0) {
       labels[q] = float(((red[0] + red[1]) + (red[2] + red[3])) / 512.0);
       plain[q] = vf[ci];
+      if (index) index[q] = ci;
     }
     if (threadIdx.x < 8) {
       const int e = threadIdx.x;
@@ -644,7 +820,7 @@ cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols&
   const int sm = MlpLayout::INFER_SMEM;
   cudaError_t e = cudaFuncSetAttribute(mc_cut_learned_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
-  mc_cut_learned_kernel<T><<<148 * 2, TILE, sm, s>>>(a);
+  mc_cut_learned_kernel<T><<<148 * 3, TILE, sm, s>>>(a);
   return cudaGetLastError();
 }
 template cudaError_t launch_mc_cut_learned<float>(const DevGrid<float>&, const float*, const Cols&, const DevTable&,
@@ -656,13 +832,14 @@ template cudaError_t launch_mc_cut_learned<double>(const DevGrid<double>&, const
 
 // One training step's gradients: per-CTA partials in grad[tiles][NPARAM], per-CTA squared-error
 // sums in loss[tiles].
-cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, long long n,
-                             unsigned long long seed, int step, int tiles, float* grad, float* loss, int* err,
-                             cudaStream_t s) {
+cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, const float* plain,
+                             const float* weights, long long n, unsigned long long seed, int step, int tiles,
+                             bool augment, float* grad, float* loss, int* err, cudaStream_t s) {
   const int sm = MlpLayout::TRAIN_BYTES;
   cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
-  mlp_train_kernel<<<tiles, TILE, sm, s>>>(P, feats, labels, n, seed, step, 1.0f / float(tiles * TILE), grad, loss, err);
+  mlp_train_kernel<<<tiles, TILE, sm, s>>>(P, feats, labels, plain, weights, n, seed, step, augment ? 1 : 0,
+                                           1.0f / float(tiles * TILE), grad, loss, err);
   return cudaGetLastError();
 }
 
@@ -672,25 +849,26 @@ cudaError_t launch_mlp_adam(float* P, float* m, float* v, const float* grad, int
   return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, float* out, int* err, cudaStream_t s) {
+cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, bool correction, float* out, int* err,
+                               cudaStream_t s) {
   const int sm = MlpLayout::INFER_SMEM;
   cudaError_t e = cudaFuncSetAttribute(mlp_predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   long long tiles = (n + TILE - 1) / TILE;
-  const int grid = (int)(tiles < 148 * 2 ? (tiles < 1 ? 1 : tiles) : 148 * 2);
-  mlp_predict_kernel<<<grid, TILE, sm, s>>>(P, feats, n, out, err);
+  const int grid = (int)(tiles < 148 * 3 ? (tiles < 1 ? 1 : tiles) : 148 * 3);
+  mlp_predict_kernel<<<grid, TILE, sm, s>>>(P, feats, n, correction ? 1 : 0, out, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_labels(const DevGrid<double>& g, const DevTape& tape, const float* phi, const float* vf,
                           const DevTable& tb, const unsigned* list, long long n, float* feats, float* labels,
-                          float* plain, cudaStream_t s) {
+                          float* plain, int64_t* index, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int sm = LBL_SUB_BYTES + LBL_NT * 208 + 4 * 8 + ((tape.bytes_len + 15) / 16) * 16;
   cudaError_t e = cudaFuncSetAttribute(label_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   const long long grid = n < 148 * 8 ? n : 148 * 8;
-  label_kernel<<<(unsigned)grid, LBL_NT, sm, s>>>(g, tape, phi, vf, tb, list, n, feats, labels, plain);
+  label_kernel<<<(unsigned)grid, LBL_NT, sm, s>>>(g, tape, phi, vf, tb, list, n, feats, labels, plain, index);
   return cudaGetLastError();
 }
 

@@ -1,5 +1,6 @@
 // learned_api.cu -- C ABI of the learned volume-fraction correction (include/cutcell_b200.h).
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -149,14 +150,16 @@ cc_status cc_mlp_get_params(cc_mlp* m, float* params, int32_t n) {
   return e == cudaSuccess ? CC_OK : cuda_fail(e, "cc_mlp_get_params");
 }
 
-cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t steps, int32_t tiles,
-                       float lr, uint64_t seed, float* last_loss, void* stream) {
+cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, const float* plain,
+                       const float* weights, int64_t n, int32_t steps, int32_t tiles, float lr, uint64_t seed,
+                       int32_t augment, float* last_loss, void* stream) {
   if (!m || !feats || !labels || n < 1 || steps < 0 || tiles < 1 || tiles > CC_MLP_MAX_TILES)
     return fail(CC_BAD_ARG, "bad training arguments");
   Dev dg(m->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   for (int k = 0; k < steps; ++k) {
-    cudaError_t e = cci::launch_mlp_grads(m->P, feats, labels, n, seed, m->step, tiles, m->grad, m->loss, m->err, s);
+    cudaError_t e = cci::launch_mlp_grads(m->P, feats, labels, plain, weights, n, seed, m->step, tiles, augment != 0,
+                                          m->grad, m->loss, m->err, s);
     if (e == cudaSuccess) e = cci::launch_mlp_adam(m->P, m->m, m->v, m->grad, tiles, m->step, lr, s);
     if (e != cudaSuccess) return cuda_fail(e, "cc_mlp_train");
     ++m->step;
@@ -174,13 +177,15 @@ cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, int64
   return CC_OK;
 }
 
-cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t tiles, uint64_t seed,
-                      int32_t step, float* grad, float* loss, void* stream) {
+cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, const float* plain, const float* weights,
+                      int64_t n, int32_t tiles, uint64_t seed, int32_t step, int32_t augment, float* grad, float* loss,
+                      void* stream) {
   if (!m || !feats || !labels || !grad || n < 1 || tiles < 1 || tiles > CC_MLP_MAX_TILES)
     return fail(CC_BAD_ARG, "bad arguments");
   Dev dg(m->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaError_t e = cci::launch_mlp_grads(m->P, feats, labels, n, seed, step, tiles, m->grad, m->loss, m->err, s);
+  cudaError_t e = cci::launch_mlp_grads(m->P, feats, labels, plain, weights, n, seed, step, tiles, augment != 0,
+                                        m->grad, m->loss, m->err, s);
   if (e != cudaSuccess) return cuda_fail(e, "cc_mlp_grad");
   cc_status st = check_err(m, s);
   if (st != CC_OK) return st;
@@ -201,19 +206,54 @@ cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, int64_
   return CC_OK;
 }
 
-cc_status cc_mlp_predict(cc_mlp* m, const float* feats, int64_t n, float* out, void* stream) {
+cc_status cc_mlp_predict(cc_mlp* m, const float* feats, int64_t n, int32_t correction, float* out, void* stream) {
   if (!m || !feats || !out || n < 0) return fail(CC_BAD_ARG, "bad arguments");
   if (n == 0) return CC_OK;
   Dev dg(m->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const cudaError_t e = cci::launch_mlp_predict(m->P, feats, n, out, m->err, s);
+  const cudaError_t e = cci::launch_mlp_predict(m->P, feats, n, correction != 0, out, m->err, s);
   if (e != cudaSuccess) return cuda_fail(e, "cc_mlp_predict");
   return check_err(m, s);
 }
 
+cc_status cc_mlp_read_weights(const char* path, float* params, int32_t n) {
+  if (!path || !params || n != CC_MLP_NPARAM) return fail(CC_BAD_ARG, "expected CC_MLP_NPARAM parameters");
+  std::FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(CC_BAD_FILE, std::string("cannot open weights file ") + path);
+  unsigned char head[64];
+  std::vector<unsigned char> body(size_t(n) * 4);
+  const bool full = std::fread(head, 1, 64, f) == 64 && std::fread(body.data(), 1, body.size(), f) == body.size();
+  const bool at_end = full && std::fgetc(f) == EOF;
+  std::fclose(f);
+  if (!full || !at_end) return fail(CC_BAD_FILE, "weights file has the wrong length");
+  uint32_t version, count;
+  float corr, curv;
+  uint64_t sum;
+  std::memcpy(&version, head + 8, 4);
+  std::memcpy(&count, head + 12, 4);
+  std::memcpy(&corr, head + 16, 4);
+  std::memcpy(&curv, head + 20, 4);
+  std::memcpy(&sum, head + 24, 8);
+  if (std::memcmp(head, "CCB2MLP1", 8) != 0) return fail(CC_BAD_FILE, "not a weights file (magic)");
+  if (version != 1) return fail(CC_BAD_FILE, "unsupported weights file version");
+  if (count != uint32_t(CC_MLP_NPARAM)) return fail(CC_BAD_FILE, "weights file holds another network");
+  if (corr != CC_MLP_CORRECTION_SCALE || curv != CC_MLP_CURVATURE_NORM)
+    return fail(CC_BAD_FILE, "weights file was trained for other correction constants");
+  for (int i = 32; i < 64; ++i)
+    if (head[i] != 0) return fail(CC_BAD_FILE, "weights file header reserved bytes are not zero");
+  uint64_t h = 0xCBF29CE484222325ull;  // FNV-1a 64
+  for (unsigned char b : body) {
+    h ^= b;
+    h *= 0x100000001B3ull;
+  }
+  if (h != sum) return fail(CC_BAD_FILE, "weights file checksum mismatch");
+  std::memcpy(params, body.data(), body.size());  // little-endian host
+  return CC_OK;
+}
+
 cc_status cc_mc_learned_samples(cc_handle* h, const cc_grid* g, const cc_optape* body, const void* phi,
-                                const cc_cells* cells, float* feats, float* labels, float* plain, int64_t capacity,
-                                int64_t* count, void* stream) {
+                                const cc_cells* cells, float* feats, float* labels, float* plain, int64_t* index,
+                                int64_t capacity, int64_t* count, void* stream) {
   cc_status st = check_mc(h, g);
   if (st != CC_OK) return st;
   if (h->prec != CC_F32) return fail(CC_BAD_ARG, "training samples are drawn from a Float32 cache");
@@ -230,7 +270,7 @@ cc_status cc_mc_learned_samples(cc_handle* h, const cc_grid* g, const cc_optape*
   cci::DevTape tape{nullptr, 0, 0, 0};
   if ((st = cci::upload_body_f64(h, body, 3, s, &tape)) != CC_OK) return st;
   e = cci::launch_labels(grid_of<double>(g), tape, static_cast<const float*>(phi),
-                         static_cast<const float*>(cells->volume_fraction), h->tb, h->cut_list, n, feats, labels, plain, s);
+                         static_cast<const float*>(cells->volume_fraction), h->tb, h->cut_list, n, feats, labels, plain, index, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "cc_mc_learned_samples");
   *count = n;

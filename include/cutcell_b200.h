@@ -56,7 +56,8 @@ typedef enum {
   CC_BAD_ARG = 7,
   CC_BAD_TABLE = 8,
   CC_NO_TABLE = 9,
-  CC_TOO_LARGE = 10
+  CC_TOO_LARGE = 10,
+  CC_BAD_FILE = 11
 } cc_status;
 
 /* Precision of a cache: the element type T of its columns. CC_MIXED stores
@@ -254,38 +255,66 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
                     double* min_volume_fraction, void* stream);
 
 /* ---- learned volume-fraction correction ----------------------------------------------------
- * An MLP 8 -> 64 -> 64 -> 1 (GELU, sigmoid output; BF16 tensor-core GEMMs with FP32 accumulate)
- * mapping a cut cell's corner values over the cell size (phi / h, MC_NODE_BITS order) to its fluid
- * volume fraction, trained on 8x sub-refined marching cubes (the BASELINE learned-correction
- * workload; no counterpart function in the reference, whose plain marching cubes it corrects).
+ * An MLP 8 -> 64 -> 64 -> 1 (GELU hidden layers, sigmoid output p; tensor-core GEMMs on BF16
+ * operands with FP32 accumulate) that corrects marching cubes' fluid volume fraction of a cut
+ * cell from its corner values over the cell size, x = phi / d[0] in MC_NODE_BITS order. There is
+ * no counterpart function in the reference, whose plain marching cubes
+ * (src/marching_cubes/moments.jl:275-346) this corrects. The correction is first order in the
+ * curvature: with quad(x) the projection of x on the four non-linear corner patterns (xy, xz,
+ * yz, xyz of the -1/+1 corner bits) and lin(x) = x - quad(x), the network sees
+ *     x~ = lin(x) + quad(x) * CC_MLP_CURVATURE_NORM / |quad(x)|
+ * and the cell's fraction becomes
+ *     corrected = plain + s * CC_MLP_CORRECTION_SCALE * (2 p(x~) - 1),  s = |quad(x)| / CC_MLP_CURVATURE_NORM
+ * (planar cells, quad = 0, keep the plain value). It is trained on the fluid fractions of
+ * marching cubes at 8x sub-refinement. The inputs, the first-layer weights, the hidden
+ * activations and the second-layer weights enter the GEMMs as BF16 high + low pairs (hi*hi +
+ * lo*hi + hi*lo), about 16 significant bits.
  * Parameters: FP32, CC_MLP_NPARAM of them: W1[64][8] b1[64] W2[64][64] b2[64] w3[64] b3. */
 #define CC_MLP_NPARAM 4801
 #define CC_MLP_MAX_TILES 1184
+#define CC_MLP_CORRECTION_SCALE 0.0625f
+#define CC_MLP_CURVATURE_NORM 0.02f
 typedef struct cc_mlp cc_mlp;
 cc_status cc_mlp_create(int32_t device, cc_mlp** out);
 cc_status cc_mlp_destroy(cc_mlp* m);
 /* host <-> device parameters; setting them also resets the Adam moments and step */
 cc_status cc_mlp_set_params(cc_mlp* m, const float* params, int32_t n);
 cc_status cc_mlp_get_params(cc_mlp* m, float* params, int32_t n);
-/* `steps` Adam steps (learning rate lr) of mean-squared error on device samples feats[n][8],
- * labels[n]; each step draws tiles*128 samples by a counter-based hash of (seed, step, slot).
- * Blocking; *last_loss receives the final step's mean squared error. */
-cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t steps,
-                       int32_t tiles, float lr, uint64_t seed, float* last_loss, void* stream);
-/* The gradient (summed over tiles) and mean squared error of one step's sample draw, without
- * updating: for checking the backward kernels. grad is a host array of CC_MLP_NPARAM floats. */
-cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, int64_t n, int32_t tiles,
-                      uint64_t seed, int32_t step, float* grad, float* loss, void* stream);
-/* Predictions out[n] for device features feats[n][8]. */
-cc_status cc_mlp_predict(cc_mlp* m, const float* feats, int64_t n, float* out, void* stream);
+/* `steps` Adam steps (learning rate lr) on device samples feats[n][8]. With plain fractions
+ * (plain != NULL) the loss is the mean of w[i] |c_i - (labels[i] - plain[i])|, c_i the
+ * correction above; with plain NULL it is the mean of w[i] (p_i - labels[i])^2 on the raw
+ * features (the network alone). w = weights, or 1 where weights is NULL. Each step draws
+ * tiles*128 samples by a counter-based hash of (seed, step, slot); with augment != 0 the same
+ * hash also picks one of the 48 symmetries of the cube per sample and permutes its corner values
+ * accordingly. Blocking; *last_loss receives the final step's loss. */
+cc_status cc_mlp_train(cc_mlp* m, const float* feats, const float* labels, const float* plain,
+                       const float* weights, int64_t n, int32_t steps, int32_t tiles, float lr, uint64_t seed,
+                       int32_t augment, float* last_loss, void* stream);
+/* The gradient (summed over tiles) and loss of one step's sample draw, without updating: for
+ * checking the backward kernels. grad is a host array of CC_MLP_NPARAM floats. */
+cc_status cc_mlp_grad(cc_mlp* m, const float* feats, const float* labels, const float* plain, const float* weights,
+                      int64_t n, int32_t tiles, uint64_t seed, int32_t step, int32_t augment, float* grad,
+                      float* loss, void* stream);
+/* For device features feats[n][8]: the network output p of the raw features (correction == 0),
+ * or the correction s * CC_MLP_CORRECTION_SCALE * (2 p(x~) - 1) (correction != 0). */
+cc_status cc_mlp_predict(cc_mlp* m, const float* feats, int64_t n, int32_t correction, float* out, void* stream);
+/* Read a weights file into the host array params[n] (n = CC_MLP_NPARAM), checking it: a 64-byte
+ * little-endian header -- magic "CCB2MLP1", u32 version 1, u32 parameter count, f32
+ * CC_MLP_CORRECTION_SCALE, f32 CC_MLP_CURVATURE_NORM, u64 FNV-1a-64 of the parameter bytes, 32
+ * zero bytes -- then the FP32 parameters. Host only (no device is touched); CC_BAD_FILE when the
+ * file is missing, short, or any field or the checksum disagrees. */
+cc_status cc_mlp_read_weights(const char* path, float* params, int32_t n);
 /* Training samples from the cut cells of the last update on h (a Float32 marching-cubes handle):
  * feats[i][8] = corner phi / d[0], plain[i] = its plain volume fraction, labels[i] = the fluid
- * fraction of marching cubes at 8x sub-refinement of `body` (Float64). Blocking; at most
- * `capacity` cells, *count receives how many were written. */
+ * fraction of marching cubes at 8x sub-refinement of `body` (Float64), index[i] (if not NULL) =
+ * the cell's linear index. Blocking; at most `capacity` cells, *count receives how many were
+ * written. */
 cc_status cc_mc_learned_samples(cc_handle* h, const cc_grid* g, const cc_optape* body, const void* phi,
-                                const cc_cells* cells, float* feats, float* labels, float* plain,
+                                const cc_cells* cells, float* feats, float* labels, float* plain, int64_t* index,
                                 int64_t capacity, int64_t* count, void* stream);
-/* cc_mc_update with the learned correction of cut cells' volume fractions; *n_fallback (if not
+/* cc_mc_update with the learned correction of cut cells' volume fractions. A cut cell keeps its
+ * plain value where p is not finite, the correction's magnitude exceeds `bound` (a negative
+ * bound rejects every prediction) or the corrected fraction leaves [0, 1]; *n_fallback (if not
  * NULL; then blocking) receives how many cut cells kept the plain value. */
 cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* body, void* phi,
                                const cc_cells* cells, const cc_mlp* mlp, float bound, int64_t* n_fallback,
