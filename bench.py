@@ -12,6 +12,14 @@ larger than the 126 MB L2, so no flush is needed between steps).
   uploaded from the host every step, update_cache blocks, and the cut-cell report is read back.
 * ``roofline``: algorithmic bytes (output columns + phi) / average update duration against the
   measured HBM copy bandwidth.
+* ``fp64``: the same update in Float64.
+* ``learned``: the learned volume-fraction correction (packaged weights) on an unseen seeded
+  smooth-min body (``workloads.smooth_blob(5002)``, 4..12 spheres in [0,1]^3) at the same size,
+  Float32: the cut cells' volume-fraction L1 error against marching cubes at 8x sub-refinement,
+  plain and learned, the fallback rate, and the plain and learned update times on the same cache
+  (CUDA events). Equal error: plain marching cubes' convergence order p is measured between n/2
+  and n on the same body; plain reaches the learned error at n * (L1_plain / L1_learned)^(1/p)
+  cells per axis, which costs (that / n)^3 plain updates at n.
 * ``cpu_baseline`` / ``--impl reference``: the oracle (a C++ restatement of the reference's CPU
   path, all host threads) on a bounded slab of the same workload -- the reference itself is Julia
   and cannot run here.
@@ -43,21 +51,22 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every period_ms while the timed regions run."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=200):
         self.index = index
+        self.period_ms = period_ms
         self.rows = []
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -132,7 +141,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-METRIC = "MarchingCubesCutCell update_cache! cells/s at 512^3 (Float32)"
+METRIC = "MC cells/s at 512\u00b3 FP32 vs FP64 and learned vs plain at equal vol-frac L1 error"
 
 
 def config(args):
@@ -164,22 +173,23 @@ def run_ours(args, rank, world, dist):
         if dist:
             dist.barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        with ClockSampler(dev.index) as clk:
-            torch.cuda.synchronize(dev)
-            t0 = torch.cuda.Event(enable_timing=True)
-            t1 = torch.cuda.Event(enable_timing=True)
-            t0.record(s)
-            for a, b in ev:
-                a.record(s)
-                cc.update_cache(cache, tape, g, sync=False)
-                b.record(s)
-            t1.record(s)
-            torch.cuda.synchronize(dev)
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(s)
+        for a, b in ev:
+            a.record(s)
+            cc.update_cache(cache, tape, g, sync=False)
+            b.record(s)
+        t1.record(s)
+        torch.cuda.synchronize(dev)
         total_ms = t0.elapsed_time(t1)
         per = [a.elapsed_time(b) for a, b in ev]
-        return cache, total_ms, per, clk.summary()
+        return cache, total_ms, per
 
-    cache, total_ms, per, clocks = timed_updates(torch.float32)
+    # clocks are sampled over every timed region (Float32, end to end, Float64, learned)
+    clk = ClockSampler(dev.index, period_ms=100).__enter__()
+    cache, total_ms, per = timed_updates(torch.float32)
     if dist:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -210,11 +220,15 @@ def run_ours(args, rank, world, dist):
     torch.cuda.empty_cache()
 
     # Float64 at the same size
-    cache64, total64, per64, _ = timed_updates(torch.float64)
+    cache64, total64, per64 = timed_updates(torch.float64)
     del cache64
     torch.cuda.empty_cache()
     ms64 = total64 / args.steps
     bytes64 = cc.workloads.mc_bytes_per_update(n, 8)
+
+    learned = None if args.no_learned else learned_block(args, dev, cc)
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
 
     if rank != 0:
         return
@@ -223,19 +237,83 @@ def run_ours(args, rank, world, dist):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded CSG body, no dataset)",
             "config": config(args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": bytes_per},
+                         "frac": achieved / peak, "traffic": traffic_per_update(n), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_per,
+                         "per": "one update (fill + cut-band launch), CUDA events",
+                         "traffic_source": "ncu dram__bytes_read+write of fill and cut at 256^3, scaled by cells"},
             "e2e": {"value": world * n ** 3 / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(ops_bytes),
                     "d2h_bytes_per_step": 48},
-            "gpu_launches": args.steps,
+            "gpu_launches": 2 * args.steps,  # per update: the fill kernel and the cut-band kernel
             "clocks": clocks,
             "fp64": {"value": world * n ** 3 / (ms64 * 1e-3), "ms_per_step": ms64,
                      "roofline_frac": bytes64 / (statistics.mean(per64) * 1e-3) / 1e9 / peak},
+            "learned": learned,
             "report": rep}
     if not args.no_cpu and world == 1:
         v, threads, sample = cpu_port_rate(n, 0)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port", "sample": sample}
     print(json.dumps(line), flush=True)
+
+
+def traffic_per_update(n):
+    """DRAM bytes of one Float32 update of the CSG workload, from one ncu capture of the fill and
+    cut-band kernels at 256^3 (fill 1.7377 GB written + 3.9 MB read; cut 21.3 MB for 99,771 cut
+    cells), scaled by cells (x8 per doubling of n for the fill, x4 for the cut band's surface)."""
+    if n < 64:
+        return None
+    s = n / 256.0
+    return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
+
+
+def learned_block(args, dev, cc):
+    """Accuracy and cost of the learned correction against plain marching cubes (see the module
+    docstring)."""
+    import importlib
+    import math
+    import torch
+    L = importlib.import_module("cutcell_b200.learned")
+    n, seed, bound = args.n, 5002, 0.05
+    m = L.pretrained(dev)
+    g = cc.workloads.unit_grid(n)
+    body = cc.workloads.smooth_blob(seed)
+    tape = cc.flatten(body, 3)
+    f, lab, pl, idx = L.body_samples(seed, n, dev, with_index=True)
+    _, lab2, pl2 = L.body_samples(seed, n // 2, dev)
+    cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32, device=dev)
+    nfb = L.update_cache_learned(cache, tape, g, m, bound=bound)
+    vf = cache.cells.volume_fraction.reshape(-1)[idx]
+    l1p = (lab - pl).abs().mean().item()
+    l1l = (lab - vf).abs().mean().item()
+    l1p_half = (lab2 - pl2).abs().mean().item()
+    s = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(args.steps):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / args.steps
+
+    ms_plain = timed(lambda: cc.update_cache(cache, tape, g, sync=False))
+    ms_learned = timed(lambda: L.update_cache_learned(cache, tape, g, m, bound=bound, count_fallback=False))
+    order = math.log2(l1p_half / l1p)
+    n_eq = n * (l1p / l1l) ** (1.0 / order)
+    cost_eq = (n_eq / n) ** 3 * ms_plain
+    del cache
+    torch.cuda.empty_cache()
+    return {"body": f"workloads.smooth_blob({seed}) over [0,1]^3 at {n}^3, Float32 (not a training body)",
+            "weights": os.path.basename(L.default_weights_path()), "cut_cells": int(f.shape[0]),
+            "l1_plain": l1p, "l1_learned": l1l, "gain": l1p / l1l, "fallback": int(nfb),
+            "fallback_rate": nfb / f.shape[0], "bound": bound,
+            "ms_plain": ms_plain, "ms_learned": ms_learned, "time_ratio": ms_learned / ms_plain,
+            "cells_per_s_plain": n ** 3 / (ms_plain * 1e-3), "cells_per_s_learned": n ** 3 / (ms_learned * 1e-3),
+            "equal_error": {"plain_l1_at_half_n": l1p_half, "plain_order": order, "plain_n_for_learned_l1": n_eq,
+                            "plain_ms_at_that_n": cost_eq, "learned_speedup_at_equal_l1": cost_eq / ms_learned}}
 
 
 def main():
@@ -247,6 +325,7 @@ def main():
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--prec", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
