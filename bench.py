@@ -12,7 +12,10 @@ larger than the 126 MB L2, so no flush is needed between steps).
   uploaded from the host every step, update_cache blocks, and the cut-cell report is read back.
 * ``roofline``: algorithmic bytes (output columns + phi) / average update duration against the
   measured HBM copy bandwidth.
-* ``fp64``: the same update in Float64.
+* ``fp64``: the same update in Float64; ``mixed``: in mixed precision (Float32 columns and
+  arithmetic with Float64 islands). ``precision``: every column's max / mean absolute error of
+  the Float32 and mixed updates against the Float64 one, and the cells whose kind or ambiguous
+  flag differ.
 * ``learned``: the learned volume-fraction correction (packaged weights) on an unseen seeded
   smooth-min body (``workloads.smooth_blob(5002)``, 4..12 spheres in [0,1]^3) at the same size,
   Float32: the cut cells' volume-fraction L1 error against marching cubes at 8x sub-refinement,
@@ -164,8 +167,8 @@ def run_ours(args, rank, world, dist):
     tape = cc.flatten(body, 3)
     peak, peak_kind = measured_peak()
 
-    def timed_updates(dtype):
-        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=dtype, device=dev)
+    def timed_updates(dtype, precision="plain"):
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=dtype, device=dev, precision=precision)
         s = torch.cuda.current_stream(dev)
         for _ in range(args.warmup):
             cc.update_cache(cache, tape, g, sync=False)
@@ -216,15 +219,18 @@ def run_ours(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     ops_bytes = tape.ops.nbytes + tape.params.nbytes
-    del cache
-    torch.cuda.empty_cache()
 
-    # Float64 at the same size
+    # Float64 and mixed precision at the same size, then every field's error against Float64
     cache64, total64, per64 = timed_updates(torch.float64)
-    del cache64
-    torch.cuda.empty_cache()
     ms64 = total64 / args.steps
     bytes64 = cc.workloads.mc_bytes_per_update(n, 8)
+    cachem, totalm, perm = timed_updates(torch.float32, "mixed")
+    msm = totalm / args.steps
+    precision = {"reference": "the Float64 update of the same body and grid (bit-identical to the Float64 oracle)",
+                 "float32": field_errors(cache, cache64), "mixed": field_errors(cachem, cache64)}
+    del cache, cache64, cachem
+    torch.cuda.empty_cache()
+    precision["degenerate_deciders"] = degenerate_decider_errors(cc, dev)
 
     learned = None if args.no_learned else learned_block(args, dev, cc)
     clk.__exit__(None, None, None)
@@ -247,12 +253,76 @@ def run_ours(args, rank, world, dist):
             "clocks": clocks,
             "fp64": {"value": world * n ** 3 / (ms64 * 1e-3), "ms_per_step": ms64,
                      "roofline_frac": bytes64 / (statistics.mean(per64) * 1e-3) / 1e9 / peak},
+            "mixed": {"value": world * n ** 3 / (msm * 1e-3), "ms_per_step": msm,
+                      "roofline_frac": bytes_per / (statistics.mean(perm) * 1e-3) / 1e9 / peak},
+            "precision": precision,
             "learned": learned,
             "report": rep}
     if not args.no_cpu and world == 1:
         v, threads, sample = cpu_port_rate(n, 0)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port", "sample": sample}
     print(json.dumps(line), flush=True)
+
+
+def field_errors(c, ref, chunk=1 << 23):
+    """Max and mean absolute error of every column of cache ``c`` against cache ``ref`` (same
+    grid), over all cells and over the cells whose eight corner values classify the same in both
+    (marching cubes' nudged signs, phi > -eps(T): there the difference is the arithmetic's;
+    elsewhere a value within eps(Float32) of zero, or a sampled value near zero, flipped side),
+    and the cells whose kind or ambiguous flag differ. Computed on the device in chunks."""
+    import torch
+    import torch.nn.functional as F
+    n = c.cells.kind.numel()
+    nn = [x + 1 for x in c.n]
+    # the signs marching cubes classifies by: nudge_zeros(phi) >= 0, i.e. phi > -eps(T)
+    e_c, e_r = torch.finfo(c.phi.dtype).eps, torch.finfo(ref.phi.dtype).eps
+    flip = ((c.phi > -e_c) != (ref.phi > -e_r)).reshape(1, 1, nn[2], nn[1], nn[0]).float()
+    same = (F.max_pool3d(flip, 2, stride=1) == 0).reshape(-1)
+    del flip
+    out = {"cells_with_a_flipped_corner_sign": int(n - same.sum().item())}
+    for f in ("volume_fraction", "centroid", "face_fraction", "face_centroid_local", "interface_centroid"):
+        a = getattr(c.cells, f).reshape(n, -1)
+        b = getattr(ref.cells, f).reshape(n, -1)
+        mx = sm = mxs = 0.0
+        for s0 in range(0, n, chunk):
+            d = (a[s0:s0 + chunk].double() - b[s0:s0 + chunk]).abs()
+            mx = max(mx, d.max().item())
+            sm += d.sum().item()
+            ds = d[same[s0:s0 + chunk]]
+            if ds.numel():
+                mxs = max(mxs, ds.max().item())
+        out[f] = {"max": mx, "mean": sm / a.numel(), "max_same_signs": mxs}
+    d = (c.phi.double() - ref.phi).abs()
+    out["phi"] = {"max": d.max().item(), "mean": d.mean().item()}
+    del d
+    out["kind_mismatch"] = int((c.cells.kind != ref.cells.kind).sum().item())
+    out["ambiguous_mismatch"] = int((c.cells.ambiguous != ref.cells.ambiguous).sum().item())
+    return out
+
+
+def degenerate_decider_errors(cc, dev, n=128, seed=7):
+    """Marching cubes from a nodal field built to stress the asymptotic deciders -- corner values
+    +-(4096 + k 2^-11), k < 64, random signs, so every ambiguous face's determinant is a
+    difference of nearly equal products -- in Float32 and mixed precision, against Float64 on the
+    same (Float32) values."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    m = (n + 1) ** 3
+    mag = 4096.0 + rng.integers(0, 64, m) * 2.0 ** -11
+    v32 = torch.as_tensor((np.where(rng.random(m) < 0.5, -1.0, 1.0) * mag).astype(np.float32), device=dev)
+    g = cc.CartesianGrid((0.0, 0.0, 0.0), (n, n, n), (1.0, 1.0, 1.0))
+    caches = {}
+    for name, dt, prec in (("f64", torch.float64, "plain"), ("float32", torch.float32, "plain"),
+                           ("mixed", torch.float32, "mixed")):
+        c = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=dt, device=dev, precision=prec)
+        cc.update_cache(c, cc.NodalField(v32.to(dt)), g)
+        caches[name] = c
+    out = {"field": f"{n}^3 nodal field +-(4096 + k 2^-11), seed {seed}"}
+    for name in ("float32", "mixed"):
+        e = field_errors(caches[name], caches["f64"])
+        out[name] = {k: e[k] for k in ("volume_fraction", "face_fraction", "kind_mismatch", "ambiguous_mismatch")}
+    return out
 
 
 def traffic_per_update(n):

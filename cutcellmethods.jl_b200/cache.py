@@ -65,7 +65,16 @@ class NodalField:
         self.values = values
 
 
-def _prec(dtype):
+def _prec(dtype, precision="plain"):
+    """The library's precision code for columns of ``dtype``; ``precision="mixed"`` (Float32
+    columns only) adds the Float64 islands: edge roots of tiny denominators, the asymptotic
+    deciders, PLIC's plane-cube clips."""
+    if precision not in ("plain", "mixed"):
+        raise ValueError(f"unknown precision {precision!r}")
+    if precision == "mixed":
+        if dtype != torch.float32:
+            raise ValueError("mixed precision stores Float32 columns")
+        return _lib.CC_MIXED
     if dtype == torch.float64:
         return _lib.CC_F64
     if dtype == torch.float32:
@@ -198,9 +207,11 @@ class PLICCutCellCache(_CacheBase):
     method = _lib.CC_PLIC
 
 
-def allocate_cache(domain, method, dtype=torch.float64, device=None, table: bytes | None = None):
+def allocate_cache(domain, method, dtype=torch.float64, device=None, table: bytes | None = None,
+                   precision: str = "plain"):
     """Storage for ``method``'s cut cells over every cell of ``domain`` (a CartesianGrid, or a
-    QuadTree for marching squares), seeded as no body."""
+    QuadTree for marching squares), seeded as no body. ``precision="mixed"`` (with Float32)
+    evaluates in Float32 with Float64 islands."""
     from . import MarchingCubesCutCell, MarchingSquaresCutCell, PLICCutCell
     if device is None:
         device = torch.device("cuda", torch.cuda.current_device())
@@ -208,7 +219,7 @@ def allocate_cache(domain, method, dtype=torch.float64, device=None, table: byte
     if device.type != "cuda":
         raise ValueError("caches live on a CUDA device; there is no CPU backend")
     dev = device.index if device.index is not None else torch.cuda.current_device()
-    prec = _prec(dtype)
+    prec = _prec(dtype, precision)
     m = method if isinstance(method, type) else type(method)
     if isinstance(domain, QuadTree):
         if m is not MarchingSquaresCutCell:
@@ -218,6 +229,7 @@ def allocate_cache(domain, method, dtype=torch.float64, device=None, table: byte
         c.handle = _Handle(dev, _lib.CC_MARCHING_SQUARES, 2, prec, (n, 0, 0))
         c.tree_n = n
         c.n = None
+        c.precision = precision
         c.phi = torch.empty(n, 4, dtype=dtype, device=device)
         c.cells = CellColumns(n, 2, dtype, device)
         return update_cache(c, EmptyGeo(1.0), domain)
@@ -242,6 +254,7 @@ def allocate_cache(domain, method, dtype=torch.float64, device=None, table: byte
         raise ArgumentError(_lib.CC_BAD_ARG, f"unknown method {method}")
     c.n = g.n
     c.tree_n = None
+    c.precision = precision
     c.cells = CellColumns(g.ncell, g.dim, dtype, device)
     if isinstance(c, PLICCutCellCache):
         c.normals = torch.empty(g.ncell, g.dim, dtype=dtype, device=device)
@@ -322,16 +335,17 @@ def kinds(cache):
 _vol_handles = {}
 
 
-def calc_volume(geo, grid: CartesianGrid, dtype=torch.float64, device=None):
+def calc_volume(geo, grid: CartesianGrid, dtype=torch.float64, device=None, precision: str = "plain"):
     """The measure of {phi < 0} over ``grid`` from every cell's PLIC plane (src/volume.jl:29-40),
     accumulated on the device in compensated Float64."""
     if device is None:
         device = torch.device("cuda", torch.cuda.current_device())
     device = torch.device(device)
     dev = device.index if device.index is not None else torch.cuda.current_device()
-    key = (dev, _prec(dtype))
+    prec = _prec(dtype, precision)
+    key = (dev, prec)
     if key not in _vol_handles:
-        _vol_handles[key] = _Handle(dev, _lib.CC_PLIC, 3, _prec(dtype), (1, 1, 1))
+        _vol_handles[key] = _Handle(dev, _lib.CC_PLIC, 3, prec, (1, 1, 1))
     h = _vol_handles[key]
     tp = _TapeRef(as_tape(geo, grid.dim))
     out = C.c_double(0.0)

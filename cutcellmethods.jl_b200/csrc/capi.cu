@@ -230,7 +230,7 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   if (dim != 2 && dim != 3) return fail(CC_BAD_ARG, "dimension must be 2 or 3");
   if (method == CC_MARCHING_SQUARES && dim != 2) return fail(CC_BAD_ARG, "marching squares is 2D");
   if (method == CC_MARCHING_CUBES && dim != 3) return fail(CC_BAD_ARG, "marching cubes is 3D");
-  if (prec != CC_F32 && prec != CC_F64) return fail(CC_BAD_ARG, "unsupported precision");
+  if (prec != CC_F32 && prec != CC_F64 && prec != CC_MIXED) return fail(CC_BAD_ARG, "unsupported precision");
   const bool tree = method == CC_MARCHING_SQUARES && n[1] == 0;
   for (int a = 0; a < (tree ? 1 : dim); ++a)
     if (n[a] < 1) return fail(CC_BAD_ARG, "every axis needs at least one cell");
@@ -347,7 +347,8 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   } else {
     if (body && (st = upload_tape<float>(h, body, 3, s, &tape)) != CC_OK) return st;
     e = cci::launch_mc<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
-                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s);
+                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s, true,
+                              h->prec == CC_MIXED);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching cubes launch");
   return CC_OK;
@@ -381,7 +382,7 @@ static cc_status ms_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   } else {
     if (body && (st = upload_tape<float>(h, body, 2, s, &tape)) != CC_OK) return st;
     e = cci::launch_ms<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
-                              static_cast<float*>(phi_out), cols_of(cells), s);
+                              static_cast<float*>(phi_out), cols_of(cells), s, h->prec == CC_MIXED);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching squares launch");
   return CC_OK;
@@ -426,7 +427,7 @@ cc_status cc_ms_tree_update(cc_handle* h, const cc_tree* t, const cc_optape* bod
     if ((st = upload_tape<float>(h, body, 2, s, &tape)) != CC_OK) return st;
     const float x0[2] = {float(t->x0[0]), float(t->x0[1])};
     e = cci::launch_ms_tree<float>(x0, t->base_d, t->nleaves, t->level, t->coord, tape, static_cast<float*>(phi4),
-                                   cols_of(cells), s);
+                                   cols_of(cells), s, h->prec == CC_MIXED);
   }
   if (e != cudaSuccess) return cuda_fail(e, "tree launch");
   return CC_OK;
@@ -452,10 +453,11 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body, 
                                                   static_cast<double*>(intercepts), is_valid, s);
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
+    const bool mx = h->prec == CC_MIXED;
     e = g->dim == 3 ? cci::launch_plic<float, 3>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
-                                                 static_cast<float*>(intercepts), is_valid, s)
+                                                 static_cast<float*>(intercepts), is_valid, s, mx)
                     : cci::launch_plic<float, 2>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
-                                                 static_cast<float*>(intercepts), is_valid, s);
+                                                 static_cast<float*>(intercepts), is_valid, s, mx);
   }
   if (e != cudaSuccess) return cuda_fail(e, "PLIC launch");
   return CC_OK;
@@ -486,8 +488,9 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     const cci::DevGrid<float> dg2 = dev_grid<float>(g);
-    e = g->dim == 3 ? cci::launch_calc_volume<float, 3>(dg2, tape, partial, res, s)
-                    : cci::launch_calc_volume<float, 2>(dg2, tape, partial, res, s);
+    const bool mx = h->prec == CC_MIXED;
+    e = g->dim == 3 ? cci::launch_calc_volume<float, 3>(dg2, tape, partial, res, s, mx)
+                    : cci::launch_calc_volume<float, 2>(dg2, tape, partial, res, s, mx);
     float pf = dg2.d[0] * dg2.d[1];
     if (g->dim == 3) pf = pf * dg2.d[2];
     pd = pf;

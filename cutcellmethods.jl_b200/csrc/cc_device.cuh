@@ -467,12 +467,26 @@ template <class T> __device__ __forceinline__ T centroid_coord(T x0, T d, long l
   return x0 + T(double(i) + 0.5) * d;
 }
 
+// Mixed precision (CC_MIXED): Float32 storage and bulk arithmetic with FP64 islands. The
+// template flag MX selects them; it is only ever set with T = float.
+//  * the edge root phi_a / (phi_a - phi_b) in FP64 when the FP32 denominator is below 2^-100,
+//    where FP32 quotients of (near-)subnormal values lose bits;
+//  * the asymptotic deciders (test_face / test_interior): products of FP32 values are exact in
+//    FP64, so a decider's sign is the exact sign of its FP32 inputs' determinant;
+//  * the plane-cube clip of PLIC (gvf2 / gvf3) evaluated in FP64 and rounded once.
+constexpr float MIXED_TINY = 7.8886090522101181e-31f;  // 2^-100
+
 // _open_fraction, src/marching_squares/marching_squares.jl:192-198
-template <class T>
+template <class T, bool MX = false>
 __device__ __forceinline__ T open_fraction(T pa, T pb) {
   const bool fa = pa >= T(0), fb = pb >= T(0);
   if (fa && fb) return T(1);
   if (!fa && !fb) return T(0);
+  if constexpr (MX) {
+    const T den = fa ? pa - pb : pb - pa;
+    if (fabs(den) < T(MIXED_TINY))
+      return T(fa ? double(pa) / (double(pa) - double(pb)) : double(pb) / (double(pb) - double(pa)));
+  }
   return fa ? pa / (pa - pb) : pb / (pb - pa);
 }
 
@@ -537,6 +551,19 @@ __device__ __forceinline__ T gvf3(T n1, T n2, T n3, T a) {
     }
   }
   return flip ? T(1) - v : v;
+}
+
+// The plane-cube clips under a precision policy: with MX (T = float), evaluated in FP64 from the
+// FP32 arguments and rounded once.
+template <class T, bool MX>
+__device__ __forceinline__ T gvf2m(T n1, T n2, T a) {
+  if constexpr (MX) return T(gvf2<double>(double(n1), double(n2), double(a)));
+  else return gvf2<T>(n1, n2, a);
+}
+template <class T, bool MX>
+__device__ __forceinline__ T gvf3m(T n1, T n2, T n3, T a) {
+  if constexpr (MX) return T(gvf3<double>(double(n1), double(n2), double(n3), double(a)));
+  else return gvf3<T>(n1, n2, n3, a);
 }
 
 }  // namespace ccd

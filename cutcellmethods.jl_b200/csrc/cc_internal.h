@@ -51,7 +51,7 @@ struct Cols {
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s, bool with_cut = true);
+                      cudaStream_t s, bool with_cut = true, bool mixed = false);
 
 // The learned correction (learned.cu).
 int mlp_nparam();
@@ -70,25 +70,26 @@ cudaError_t launch_labels(const DevGrid<double>& g, const DevTape& tape, const f
                           const DevTable& tb, const unsigned* list, long long n, float* feats, float* labels,
                           float* plain, int64_t* index, cudaStream_t s);
 
+// `mixed` (Float32 only) selects the FP64 islands of mixed precision; see cc_device.cuh.
 template <class T>
 cudaError_t launch_ms(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
-                      const Cols& cols, cudaStream_t s);
+                      const Cols& cols, cudaStream_t s, bool mixed = false);
 
 template <class T>
 cudaError_t launch_ms_tree(const T x0[2], const double base_d[2], long long nleaves,
                            const int32_t* level, const int32_t* coord, const DevTape& tape,
-                           T* phi4, const Cols& cols, cudaStream_t s);
+                           T* phi4, const Cols& cols, cudaStream_t s, bool mixed = false);
 
 template <class T, int D>
 cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals,
-                        T* intercepts, uint8_t* valid, cudaStream_t s);
+                        T* intercepts, uint8_t* valid, cudaStream_t s, bool mixed = false);
 
 // calc_volume partial sums: nblocks (sum, compensation) pairs into `partial`, then a final
 // single-block pass into out[0..1]. `partial` holds 2 * calc_volume_blocks() doubles.
 int calc_volume_blocks();
 template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial,
-                               double* out, cudaStream_t s);
+                               double* out, cudaStream_t s, bool mixed = false);
 
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);

@@ -283,6 +283,7 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
   cc_status st = check_mc(h, g);
   if (st != CC_OK) return st;
   if (!mlp || !phi || !cells_ok(cells)) return fail(CC_BAD_ARG, "null argument");
+  if (h->prec == CC_MIXED) return fail(CC_BAD_ARG, "the learned correction runs on Float32 or Float64 caches");
   if (!(g->d[0] > 0.0)) return fail(CC_BAD_ARG, "bad grid");
   if ((st = cci::validate_body(body, 3)) != CC_OK) return st;
   Dev dg(h->device);

@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
   if (fast && tid == 0) bulk_wait<0>();  // all tensor stores complete before the CTA retires
 }
 
-template <class T, bool SAMPLE>
+template <class T, bool SAMPLE, bool MX>
 __global__ void __launch_bounds__(CUT_NT) mc_cut_kernel(const McArgs<T> A) {
   const long long n0 = A.g.n[0], n1 = A.g.n[1];
   const long long nx = n0 + 1, ny = n1 + 1;
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(CUT_NT) mc_cut_kernel(const McArgs<T> A) {
                       node_coord(A.g.x0[2], A.g.d[2], k)};
     const T l[3] = {node_coord(A.g.x0[0], A.g.d[0], i + 1) - org[0], node_coord(A.g.x0[1], A.g.d[1], j + 1) - org[1],
                     node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
-    mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
+    mc_cut_cell<T, MX>(ph, l, org, cs, A.tb, st, ci);
   }
 }
 
@@ -428,7 +428,7 @@ namespace cci {
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s, bool with_cut) {
+                      cudaStream_t s, bool with_cut, bool mixed) {
   using TL = Tile<T>;
   McArgs<T> a;
   a.g = g;
@@ -452,23 +452,27 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   const bool sample = phi_in == nullptr;
   const int sm = smem_bytes<T>(sample ? tape.bytes_len : 0);
   const int cut_blocks = 148 * 8;
+  // the FP64 islands of mixed precision exist for Float32 caches only
+  const bool mx = mixed && sizeof(T) == 4;
   if (sample) {
     e = cudaFuncSetAttribute(mc_fill_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     mc_fill_kernel<T, true><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
-    if (with_cut) mc_cut_kernel<T, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    if (with_cut && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
   } else {
     e = cudaFuncSetAttribute(mc_fill_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     mc_fill_kernel<T, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
-    if (with_cut) mc_cut_kernel<T, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    if (with_cut && mx) mc_cut_kernel<T, false, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, false, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
   }
   return cudaGetLastError();
 }
 
 template cudaError_t launch_mc<float>(const DevGrid<float>&, const DevTape&, const float*, float*,
-                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool);
+                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool);
 template cudaError_t launch_mc<double>(const DevGrid<double>&, const DevTape&, const double*, double*,
-                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool);
+                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool);
 
 }  // namespace cci

@@ -8,6 +8,7 @@
 // (:306-330) and the divergence-theorem sums.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include "cc_device.cuh"
 #include "cc_internal.h"
 
@@ -50,51 +51,59 @@ __device__ __forceinline__ T nudge(T v) {
   return fabs(v) < e ? e : v;
 }
 
-// _test_face, src/marching_cubes/marching_cubes.jl:401-406
-template <class T>
+// _test_face, src/marching_cubes/marching_cubes.jl:401-406. With MX the determinant and the
+// final product are evaluated in FP64 (R) from the FP32 corner values; the threshold stays eps(T).
+template <class T, bool MX = false>
 __device__ __forceinline__ bool test_face(const T* cb, int face) {
+  using R = typename std::conditional<MX, double, T>::type;
   const int f = (face < 0 ? -face : face) - 1;
-  const T A = cb[c_quads[f][0]], B = cb[c_quads[f][1]], C = cb[c_quads[f][2]], D = cb[c_quads[f][3]];
-  const T det = A * C - B * D;
-  if (fabs(det) < Eps<T>::v()) return face >= 0;
-  return (T(face) * A) * det >= T(0);
+  const R A = cb[c_quads[f][0]], B = cb[c_quads[f][1]], C = cb[c_quads[f][2]], D = cb[c_quads[f][3]];
+  const R det = A * C - B * D;
+  if (fabs(det) < R(Eps<T>::v())) return face >= 0;
+  return (R(face) * A) * det >= R(0);
 }
 // The same decider for a face code known at compile time (face_outside_connected, :421-422).
-template <class T, int FACE>
+template <class T, int FACE, bool MX = false>
 __device__ __forceinline__ bool test_face_c(const T* cb) {
+  using R = typename std::conditional<MX, double, T>::type;
   constexpr int q[6][4] = {{0, 4, 5, 1}, {1, 5, 6, 2}, {2, 6, 7, 3}, {3, 7, 4, 0}, {0, 3, 2, 1}, {4, 7, 6, 5}};
-  const T A = cb[q[FACE - 1][0]], B = cb[q[FACE - 1][1]], C = cb[q[FACE - 1][2]], D = cb[q[FACE - 1][3]];
-  const T det = A * C - B * D;
-  if (fabs(det) < Eps<T>::v()) return true;
-  return (T(FACE) * A) * det >= T(0);
+  const R A = cb[q[FACE - 1][0]], B = cb[q[FACE - 1][1]], C = cb[q[FACE - 1][2]], D = cb[q[FACE - 1][3]];
+  const R det = A * C - B * D;
+  if (fabs(det) < R(Eps<T>::v())) return true;
+  return (R(FACE) * A) * det >= R(0);
 }
 
-// _test_interior, :427-504
-template <class T>
-__device__ bool test_interior(int itype, int edge, const T* cb, int s) {
-  T At = T(0), Bt = T(0), Ct = T(0), Dt = T(0);
+// _test_interior, :427-504. With MX every step runs in FP64 (R) from the FP32 corner values; the
+// thresholds stay eps(T).
+template <class T, bool MX = false>
+__device__ bool test_interior(int itype, int edge, const T* cbt, int s) {
+  using R = typename std::conditional<MX, double, T>::type;
+  R cb[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) cb[k] = cbt[k];
+  R At = R(0), Bt = R(0), Ct = R(0), Dt = R(0);
   if (itype == CC_MC_INTERIOR_CASE4_10) {
-    const T a = (cb[4] - cb[0]) * (cb[6] - cb[2]) - (cb[7] - cb[3]) * (cb[5] - cb[1]);
-    const T b = ((cb[2] * (cb[4] - cb[0]) + cb[0] * (cb[6] - cb[2])) - cb[1] * (cb[7] - cb[3])) - cb[3] * (cb[5] - cb[1]);
-    const T t = -b / (T(2) * a);
-    if (t < T(0) || t > T(1)) return s > 0;
+    const R a = (cb[4] - cb[0]) * (cb[6] - cb[2]) - (cb[7] - cb[3]) * (cb[5] - cb[1]);
+    const R b = ((cb[2] * (cb[4] - cb[0]) + cb[0] * (cb[6] - cb[2])) - cb[1] * (cb[7] - cb[3])) - cb[3] * (cb[5] - cb[1]);
+    const R t = -b / (R(2) * a);
+    if (t < R(0) || t > R(1)) return s > 0;
     At = cb[0] + (cb[4] - cb[0]) * t;
     Bt = cb[3] + (cb[7] - cb[3]) * t;
     Ct = cb[2] + (cb[6] - cb[2]) * t;
     Dt = cb[1] + (cb[5] - cb[1]) * t;
   } else {
     const uint8_t* e = c_iedge[edge];
-    const T t = cb[e[0]] / (cb[e[0]] - cb[e[1]]);
+    const R t = cb[e[0]] / (cb[e[0]] - cb[e[1]]);
     Bt = cb[e[2]] + (cb[e[3]] - cb[e[2]]) * t;
     Ct = cb[e[4]] + (cb[e[5]] - cb[e[4]]) * t;
     Dt = cb[e[6]] + (cb[e[7]] - cb[e[6]]) * t;
   }
   int test = 0;
-  if (At >= T(0)) test += 1;
-  if (Bt >= T(0)) test += 2;
-  if (Ct >= T(0)) test += 4;
-  if (Dt >= T(0)) test += 8;
-  const T eps = Eps<T>::v();
+  if (At >= R(0)) test += 1;
+  if (Bt >= R(0)) test += 2;
+  if (Ct >= R(0)) test += 4;
+  if (Dt >= R(0)) test += 8;
+  const R eps = R(Eps<T>::v());
   if (test == 6 || test == 8 || test == 9 || test == 12 || (test >= 0 && test <= 4)) return s > 0;
   if (test == 5) return (At * Ct - Bt * Dt < eps) ? s > 0 : s < 0;
   if (test == 10) return (At * Ct - Bt * Dt >= eps) ? s > 0 : s < 0;
@@ -104,7 +113,7 @@ __device__ bool test_interior(int itype, int edge, const T* cb, int s) {
 // The open polygon of one cube face in its own (p, q) frame: cell_boundary_walk
 // (src/marching_squares/marching_squares.jl:240-251) then _face_polygon
 // (src/marching_cubes/moments.jl:111-139) with _chord_target (:91-98).
-template <class T>
+template <class T, bool MX = false>
 __device__ __forceinline__ void face_polygon(const T fn[4][2], const T fphi[4], bool connect, T& area2,
                                              T& m0, T& m1) {
   T sa[4][2], sb[4][2];
@@ -113,7 +122,7 @@ __device__ __forceinline__ void face_polygon(const T fn[4][2], const T fphi[4], 
   for (int k = 0; k < 4; ++k) {
     const int k1 = (k + 1) & 3;
     const T fa = fphi[k], fb = fphi[k1];
-    const T frac = open_fraction(fa, fb);
+    const T frac = open_fraction<T, MX>(fa, fb);
     present[k] = fa >= T(0) || fb >= T(0);
     if (fa >= T(0) && fb >= T(0)) {
       sa[k][0] = fn[k][0]; sa[k][1] = fn[k][1]; sb[k][0] = fn[k1][0]; sb[k][1] = fn[k1][1];
@@ -209,7 +218,7 @@ __device__ __forceinline__ void put_cell(const Stage<T>& st, long long lc, int k
 // raw corner values in MC_NODE_BITS order, `l` the cell's lattice edge lengths
 // (x_{i+1} - x_i per axis: every corner's cell-local coordinate is 0 or l exactly), `org` the
 // lower corner and `cs` the grid's cell size.
-template <class T>
+template <class T, bool MX = false>
 __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T org[3], const T cs[3],
                                          const DevTable tb, const Stage<T> st, long long lc) {
   T phi[8];
@@ -226,10 +235,10 @@ __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T o
   for (int p = 0; p < 8; ++p) lut |= (phi[p] >= T(0) ? 1 : 0) << p;
   const cc_mc_lut ent = tb.luts[lut];
   int o = 0;
-  for (int i = 0; i < ent.ntests; ++i) o |= (test_face(phi, ent.face[i]) ? 1 : 0) << i;
+  for (int i = 0; i < ent.ntests; ++i) o |= (test_face<T, MX>(phi, ent.face[i]) ? 1 : 0) << i;
   const cc_mc_outcome oc = tb.outs[ent.outcome_base + o];
   int tile = oc.tile_true;
-  if (oc.itype != CC_MC_INTERIOR_NONE && !test_interior(oc.itype, oc.edge, phi, oc.s)) tile = oc.tile_false;
+  if (oc.itype != CC_MC_INTERIOR_NONE && !test_interior<T, MX>(oc.itype, oc.edge, phi, oc.s)) tile = oc.tile_false;
   const cc_mc_tile tl = tb.tiles[tile];
 
   // the six face clips (cut_cell_faces / _cut_cell_face, moments.jl:150-257)
@@ -260,15 +269,15 @@ __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T o
     } else {
       bool connect;
       switch (dir) {
-        case 0: connect = test_face_c<T, face_test_code(0)>(phi); break;
-        case 1: connect = test_face_c<T, face_test_code(1)>(phi); break;
-        case 2: connect = test_face_c<T, face_test_code(2)>(phi); break;
-        case 3: connect = test_face_c<T, face_test_code(3)>(phi); break;
-        case 4: connect = test_face_c<T, face_test_code(4)>(phi); break;
-        default: connect = test_face_c<T, face_test_code(5)>(phi); break;
+        case 0: connect = test_face_c<T, face_test_code(0), MX>(phi); break;
+        case 1: connect = test_face_c<T, face_test_code(1), MX>(phi); break;
+        case 2: connect = test_face_c<T, face_test_code(2), MX>(phi); break;
+        case 3: connect = test_face_c<T, face_test_code(3), MX>(phi); break;
+        case 4: connect = test_face_c<T, face_test_code(4), MX>(phi); break;
+        default: connect = test_face_c<T, face_test_code(5), MX>(phi); break;
       }
       T area2, m0, m1;
-      face_polygon(fn, fphi, connect, area2, m0, m1);
+      face_polygon<T, MX>(fn, fphi, connect, area2, m0, m1);
       const T full = (T(1) * cs[p]) * cs[q];
       frac = (T(0.5) * area2) / full;
       if (area2 != T(0)) { const T den = T(3) * area2; c0 = m0 / den; c1 = m1 / den; }
@@ -288,7 +297,7 @@ __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T o
     const int a = edge_node(e, 0), b = edge_node(e, 1);
     const T fa = phi[a], fb = phi[b];
     if ((fa >= T(0)) != (fb >= T(0))) {
-      const T s = open_fraction(fa, fb);
+      const T s = open_fraction<T, MX>(fa, fb);
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
         const T pa = cbit(a, x) ? l[x] : T(0);

@@ -23,7 +23,7 @@ __host__ __device__ constexpr int dir_edge(int dir) { return dir == 0 ? 3 : dir 
 
 // cut_cell_moments (2D), src/marching_squares/moments.jl:66-164, from global corner
 // coordinates `nd` (MS_NODE_BITS order) and corner values `ph`; writes cell `ci`'s columns.
-template <class T>
+template <class T, bool MX>
 __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Cols& cols, long long ci) {
   const T o0 = nd[0][0], o1 = nd[0][1];
   const T ce0 = o0 + T(0.5) * cs[0], ce1 = o1 + T(0.5) * cs[1];
@@ -61,7 +61,7 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
   for (int k = 0; k < 4; ++k) {
     const int k1 = (k + 1) & 3;
     const T fa = ph[k], fb = ph[k1];
-    fr[k] = open_fraction(fa, fb);
+    fr[k] = open_fraction<T, MX>(fa, fb);
     pr[k] = fa >= T(0) || fb >= T(0);
     if (fa >= T(0) && fb >= T(0)) {
       sa[k][0] = nd[k][0]; sa[k][1] = nd[k][1]; sb[k][0] = nd[k1][0]; sb[k][1] = nd[k1][1];
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(NT) ms_sample_kernel(const DevGrid<T> g, const
   }
 }
 
-template <class T>
+template <class T, bool MX>
 __global__ void __launch_bounds__(NT) ms_cells_kernel(const DevGrid<T> g, const T* __restrict__ phi, const Cols cols) {
   const long long n0 = g.n[0], n1 = g.n[1], nx = n0 + 1, total = n0 * n1;
   const T cs[2] = {g.d[0], g.d[1]};
@@ -160,11 +160,11 @@ __global__ void __launch_bounds__(NT) ms_cells_kernel(const DevGrid<T> g, const 
     const T nd[4][2] = {{xa, ya}, {xb, ya}, {xb, yb}, {xa, yb}};
     const long long b = i + nx * j;
     const T ph[4] = {phi[b], phi[b + 1], phi[b + nx + 1], phi[b + nx]};
-    ms_cell<T>(nd, ph, cs, cols, ci);
+    ms_cell<T, MX>(nd, ph, cs, cols, ci);
   }
 }
 
-template <class T>
+template <class T, bool MX>
 __global__ void __launch_bounds__(NT) ms_tree_kernel(const T x00, const T x01, const double bd0, const double bd1,
                                                      long long nl, const int32_t* __restrict__ level,
                                                      const int32_t* __restrict__ coord, const DevTape tape, T* phi4,
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(NT) ms_tree_kernel(const T x00, const T x01, c
       ph[q] = tape_eval<T, 2, T>(t, nd[q]);
       phi4[4 * i + q] = ph[q];
     }
-    ms_cell<T>(nd, ph, h, cols, i);
+    ms_cell<T, MX>(nd, ph, h, cols, i);
   }
 }
 
@@ -202,32 +202,40 @@ namespace cci {
 
 template <class T>
 cudaError_t launch_ms(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
-                      const Cols& cols, cudaStream_t s) {
+                      const Cols& cols, cudaStream_t s, bool mixed) {
   const T* phi = phi_in;
   if (!phi_in) {
     const int sm = ((tape.bytes_len + 15) / 16) * 16;
     ms_sample_kernel<T><<<grid_blocks((g.n[0] + 1) * (g.n[1] + 1)), NT, sm, s>>>(g, tape, phi_out);
     phi = phi_out;
   }
-  ms_cells_kernel<T><<<grid_blocks(g.n[0] * g.n[1]), NT, 0, s>>>(g, phi, cols);
+  if (mixed && sizeof(T) == 4) ms_cells_kernel<T, true><<<grid_blocks(g.n[0] * g.n[1]), NT, 0, s>>>(g, phi, cols);
+  else ms_cells_kernel<T, false><<<grid_blocks(g.n[0] * g.n[1]), NT, 0, s>>>(g, phi, cols);
   return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_ms_tree(const T x0[2], const double base_d[2], long long nleaves, const int32_t* level,
-                           const int32_t* coord, const DevTape& tape, T* phi4, const Cols& cols, cudaStream_t s) {
+                           const int32_t* coord, const DevTape& tape, T* phi4, const Cols& cols, cudaStream_t s,
+                           bool mixed) {
   if (nleaves <= 0) return cudaSuccess;
   const int sm = ((tape.bytes_len + 15) / 16) * 16;
-  ms_tree_kernel<T><<<grid_blocks(nleaves), NT, sm, s>>>(x0[0], x0[1], base_d[0], base_d[1], nleaves, level,
-                                                         coord, tape, phi4, cols);
+  if (mixed && sizeof(T) == 4)
+    ms_tree_kernel<T, true><<<grid_blocks(nleaves), NT, sm, s>>>(x0[0], x0[1], base_d[0], base_d[1], nleaves, level,
+                                                                 coord, tape, phi4, cols);
+  else
+    ms_tree_kernel<T, false><<<grid_blocks(nleaves), NT, sm, s>>>(x0[0], x0[1], base_d[0], base_d[1], nleaves, level,
+                                                                  coord, tape, phi4, cols);
   return cudaGetLastError();
 }
 
-template cudaError_t launch_ms<float>(const DevGrid<float>&, const DevTape&, const float*, float*, const Cols&, cudaStream_t);
-template cudaError_t launch_ms<double>(const DevGrid<double>&, const DevTape&, const double*, double*, const Cols&, cudaStream_t);
+template cudaError_t launch_ms<float>(const DevGrid<float>&, const DevTape&, const float*, float*, const Cols&, cudaStream_t,
+                                      bool);
+template cudaError_t launch_ms<double>(const DevGrid<double>&, const DevTape&, const double*, double*, const Cols&,
+                                       cudaStream_t, bool);
 template cudaError_t launch_ms_tree<float>(const float*, const double*, long long, const int32_t*, const int32_t*,
-                                           const DevTape&, float*, const Cols&, cudaStream_t);
+                                           const DevTape&, float*, const Cols&, cudaStream_t, bool);
 template cudaError_t launch_ms_tree<double>(const double*, const double*, long long, const int32_t*, const int32_t*,
-                                            const DevTape&, double*, const Cols&, cudaStream_t);
+                                            const DevTape&, double*, const Cols&, cudaStream_t, bool);
 
 }  // namespace cci

@@ -28,8 +28,8 @@ struct PlaneFit {
   bool valid;
 };
 
-// cell_plane, src/plic/plic.jl:72-88
-template <class T, int D>
+// cell_plane, src/plic/plic.jl:72-88 (with MX the plane-cube clip runs in FP64)
+template <class T, int D, bool MX>
 __device__ __forceinline__ PlaneFit<T, D> cell_plane(const STape<T>& t, const DevGrid<T>& g, const long long idx[3]) {
   Dual<T, D> x[D];
 #pragma unroll
@@ -58,13 +58,13 @@ __device__ __forceinline__ PlaneFit<T, D> cell_plane(const STape<T>& t, const De
 #pragma unroll
   for (int q = 0; q < D; ++q) pl.n[q] = r.g[q];
   pl.a = a;
-  if constexpr (D == 2) pl.fraction = gvf2(r.g[0], r.g[1], a);
-  else pl.fraction = gvf3(r.g[0], r.g[1], r.g[D - 1], a);
+  if constexpr (D == 2) pl.fraction = gvf2m<T, MX>(r.g[0], r.g[1], a);
+  else pl.fraction = gvf3m<T, MX>(r.g[0], r.g[1], r.g[D - 1], a);
   pl.valid = true;
   return pl;
 }
 
-template <class T, int D>
+template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const DevTape tape, const Cols cols,
                                                       T* normals, T* intercepts, uint8_t* valid) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const 
   T* vf = static_cast<T*>(cols.vf);
   for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
     const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
-    const PlaneFit<T, D> pl = cell_plane<T, D>(t, g, idx);
+    const PlaneFit<T, D> pl = cell_plane<T, D, MX>(t, g, idx);
     const T frac = T(1) - pl.fraction;
 #pragma unroll
     for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const 
 }
 
 // _cell_wet + _face_area, src/plic/apertures.jl:73-125 (k is the 0-based direction)
-template <class T, int D>
+template <class T, int D, bool MX>
 __device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k) {
   const T s = (k & 1) ? T(1) : T(0);
   if constexpr (D == 2) {
@@ -95,7 +95,7 @@ __device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T
     const T len = cs[p];
     if (!valid) return frac < T(0.5) ? T(0) : len;
     const T base = n[c] * s - a;
-    return open_fraction(base, base + n[p]) * len;
+    return open_fraction<T, MX>(base, base + n[p]) * len;
   } else {
     const int c = k >> 1;
     const int p = c == 0 ? 1 : 0;
@@ -104,12 +104,12 @@ __device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T
     if (!valid) return frac < T(0.5) ? T(0) : U * V;
     const T base = n[c] * s - a;
     if (n[p] == T(0) && n[q] == T(0)) return base >= T(0) ? U * V : T(0);
-    const T solid = gvf2(n[p], n[q], -base);
+    const T solid = gvf2m<T, MX>(n[p], n[q], -base);
     return (U * V) * (T(1) - solid);
   }
 }
 
-template <class T, int D>
+template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const Cols cols, const T* __restrict__ normals,
                                                        const T* __restrict__ intercepts, const uint8_t* __restrict__ valid) {
   const long long n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
@@ -126,17 +126,17 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
       T full;
       if constexpr (D == 2) full = cs[1 - c];
       else full = (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
-      const T own = face_area<T, D>(normals + D * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, k);
+      const T own = face_area<T, D, MX>(normals + D * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, k);
       T r;
       if ((k & 1) == 0) {
         const bool has = idx[c] >= 1;
         const long long cj = has ? ci - stride : ci;
-        const T below = face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k + 1);
+        const T below = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k + 1);
         r = has ? (below / full + own / full) / T(2) : own / full;
       } else {
         const bool has = idx[c] <= n[c] - 2;
         const long long cj = has ? ci + stride : ci;
-        const T above = face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k - 1);
+        const T above = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k - 1);
         r = has ? (own / full + above / full) / T(2) : own / full;
       }
       ff[2 * D * ci + k] = r;
@@ -156,7 +156,7 @@ struct KSum {
 };
 
 // calc_volume, src/volume.jl:29-40: every cell's cell_plane solid fraction, summed.
-template <class T, int D>
+template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, const DevTape tape, double* partial) {
   extern __shared__ __align__(16) unsigned char smem[];
   const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, con
   KSum acc{0.0, 0.0};
   for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
     const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
-    acc.add(double(cell_plane<T, D>(t, g, idx).fraction));
+    acc.add(double(cell_plane<T, D, MX>(t, g, idx).fraction));
   }
   __shared__ double ss[NT], sc[NT];
   ss[threadIdx.x] = acc.s;
@@ -261,11 +261,16 @@ namespace cci {
 
 template <class T, int D>
 cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals, T* intercepts,
-                        uint8_t* valid, cudaStream_t s) {
+                        uint8_t* valid, cudaStream_t s, bool mixed) {
   const long long total = g.n[0] * g.n[1] * (D == 3 ? g.n[2] : 1);
   const int sm = ((tape.bytes_len + 15) / 16) * 16;
-  plic_fit_kernel<T, D><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
-  plic_face_kernel<T, D><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+  if (mixed && sizeof(T) == 4) {
+    plic_fit_kernel<T, D, true><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
+    plic_face_kernel<T, D, true><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+  } else {
+    plic_fit_kernel<T, D, false><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
+    plic_face_kernel<T, D, false><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+  }
   return cudaGetLastError();
 }
 
@@ -273,9 +278,10 @@ int calc_volume_blocks() { return VOL_BLOCKS; }
 
 template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial, double* out,
-                               cudaStream_t s) {
+                               cudaStream_t s, bool mixed) {
   const int sm = ((tape.bytes_len + 15) / 16) * 16;
-  calc_volume_kernel<T, D><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+  if (mixed && sizeof(T) == 4) calc_volume_kernel<T, D, true><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+  else calc_volume_kernel<T, D, false><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
   calc_volume_final<<<1, 32, 0, s>>>(partial, VOL_BLOCKS, out);
   return cudaGetLastError();
 }
@@ -294,8 +300,9 @@ cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* am
 
 #define INST(T, D)                                                                                      \
   template cudaError_t launch_plic<T, D>(const DevGrid<T>&, const DevTape&, const Cols&, T*, T*, uint8_t*, \
-                                         cudaStream_t);                                                 \
-  template cudaError_t launch_calc_volume<T, D>(const DevGrid<T>&, const DevTape&, double*, double*, cudaStream_t);
+                                         cudaStream_t, bool);                                           \
+  template cudaError_t launch_calc_volume<T, D>(const DevGrid<T>&, const DevTape&, double*, double*, cudaStream_t, \
+                                                bool);
 INST(float, 2)
 INST(float, 3)
 INST(double, 2)

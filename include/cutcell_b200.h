@@ -60,9 +60,12 @@ typedef enum {
   CC_BAD_FILE = 11
 } cc_status;
 
-/* Precision of a cache: the element type T of its columns. CC_MIXED stores
- * Float32 columns and evaluates in Float32 with Float64 islands (edge roots of
- * nearly equal corner values, the asymptotic face decider). */
+/* Precision of a cache: the element type T of its columns. CC_MIXED stores Float32 columns and
+ * evaluates in Float32 with Float64 islands: the edge root phi_a / (phi_a - phi_b) when the
+ * Float32 denominator is below 2^-100; the marching-cubes asymptotic face and interior deciders
+ * (exact signs: products of Float32 values are exact in Float64); PLIC's plane-cube clips
+ * (gvf2 / gvf3). calc_volume and the report reduce in compensated Float64 in every precision.
+ * The learned correction does not take CC_MIXED handles. */
 typedef enum { CC_F32 = 0, CC_F64 = 1, CC_MIXED = 2 } cc_prec;
 
 /* Methods (the reference's stateless method tags). */

@@ -337,13 +337,41 @@ static const int MS_DIRECTION_EDGE0[4] = {3, 1, 0, 2};
 inline int ms_next(int k) { return (k + 1) & 3; }
 inline int ms_prev(int k) { return (k + 3) & 3; }
 
+// Mixed precision (prec 2 at the C entry points): Float32 data and arithmetic with Float64
+// islands -- the edge root when the Float32 denominator is below 2^-100, the asymptotic deciders,
+// the PLIC plane-cube clips. A process-wide flag, set for the duration of one entry-point call.
+inline bool& mixed_flag() {
+  static bool m = false;
+  return m;
+}
+struct MixedScope {
+  bool old;
+  explicit MixedScope(bool m) : old(mixed_flag()) { mixed_flag() = m; }
+  ~MixedScope() { mixed_flag() = old; }
+};
+template <class T> inline bool mixed_on() { return std::is_same<T, float>::value && mixed_flag(); }
+constexpr float MIXED_TINY = 7.8886090522101181e-31f;  // 2^-100
+
 // _open_fraction, marching_squares.jl:192-198
 template <class T>
 inline T open_fraction(T pa, T pb) {
   const bool fa = pa >= T(0), fb = pb >= T(0);
   if (fa && fb) return T(1);
   if (!fa && !fb) return T(0);
+  if (mixed_on<T>()) {
+    const T den = fa ? pa - pb : pb - pa;
+    if (std::fabs(den) < T(MIXED_TINY))
+      return T(fa ? double(pa) / (double(pa) - double(pb)) : double(pb) / (double(pb) - double(pa)));
+  }
   return fa ? pa / (pa - pb) : pb / (pb - pa);
+}
+
+// The plane-cube clips; under mixed precision evaluated in Float64 and rounded once.
+template <class T> inline T gvf2p(T n1, T n2, T a) {
+  return mixed_on<T>() ? T(gvf2<double>(n1, n2, a)) : gvf2<T>(n1, n2, a);
+}
+template <class T> inline T gvf3p(T n1, T n2, T n3, T a) {
+  return mixed_on<T>() ? T(gvf3<double>(n1, n2, n3, a)) : gvf3<T>(n1, n2, n3, a);
 }
 
 // _open_segment, marching_squares.jl:208-217
@@ -551,14 +579,19 @@ template <class T> inline T nudge(T v) {
   return std::fabs(v) < e ? e : v;
 }
 
-// _test_face, marching_cubes.jl:401-406
+// _test_face, marching_cubes.jl:401-406, evaluated in R (T, or Float64 under mixed precision)
+// with the threshold eps(T).
+template <class T, class R>
+inline bool test_face_r(const T* cb, int face) {
+  const int* q = MC_TEST_FACE_QUADS1[std::abs(face) - 1];
+  const R A = cb[q[0] - 1], B = cb[q[1] - 1], C = cb[q[2] - 1], D = cb[q[3] - 1];
+  const R det = A * C - B * D;
+  if (std::fabs(det) < R(std::numeric_limits<T>::epsilon())) return face >= 0;
+  return (R(face) * A) * det >= R(0);
+}
 template <class T>
 inline bool test_face(const T* cb, int face) {
-  const int* q = MC_TEST_FACE_QUADS1[std::abs(face) - 1];
-  const T A = cb[q[0] - 1], B = cb[q[1] - 1], C = cb[q[2] - 1], D = cb[q[3] - 1];
-  const T det = A * C - B * D;
-  if (std::fabs(det) < std::numeric_limits<T>::epsilon()) return face >= 0;
-  return (T(face) * A) * det >= T(0);
+  return mixed_on<T>() ? test_face_r<T, double>(cb, face) : test_face_r<T, T>(cb, face);
 }
 
 // _test_interior, marching_cubes.jl:427-504. Reference edges 0..11 as
@@ -569,36 +602,40 @@ static const int MC_INTERIOR_EDGE1[12][8] = {
     {4, 1, 3, 2, 7, 6, 8, 5}, {5, 6, 8, 7, 4, 3, 1, 2}, {6, 7, 5, 8, 1, 4, 2, 3},
     {7, 8, 6, 5, 2, 1, 3, 4}, {8, 5, 7, 6, 3, 2, 4, 1}, {1, 5, 4, 8, 3, 7, 2, 6},
     {2, 6, 1, 5, 4, 8, 3, 7}, {3, 7, 2, 6, 1, 5, 4, 8}, {4, 8, 3, 7, 2, 6, 1, 5}};
-template <class T>
-inline bool test_interior(int itype, int edge, const T* cb, int s) {
-  T At = T(0), Bt = T(0), Ct = T(0), Dt = T(0);
-  auto c = [&](int i) { return cb[i - 1]; };
+template <class T, class R>
+inline bool test_interior_r(int itype, int edge, const T* cb, int s) {
+  R At = R(0), Bt = R(0), Ct = R(0), Dt = R(0);
+  auto c = [&](int i) { return R(cb[i - 1]); };
   if (itype == CC_MC_INTERIOR_CASE4_10) {
-    const T a = (c(5) - c(1)) * (c(7) - c(3)) - (c(8) - c(4)) * (c(6) - c(2));
-    const T b = ((c(3) * (c(5) - c(1)) + c(1) * (c(7) - c(3))) - c(2) * (c(8) - c(4))) - c(4) * (c(6) - c(2));
-    const T t = -b / (T(2) * a);
-    if (t < T(0) || t > T(1)) return s > 0;
+    const R a = (c(5) - c(1)) * (c(7) - c(3)) - (c(8) - c(4)) * (c(6) - c(2));
+    const R b = ((c(3) * (c(5) - c(1)) + c(1) * (c(7) - c(3))) - c(2) * (c(8) - c(4))) - c(4) * (c(6) - c(2));
+    const R t = -b / (R(2) * a);
+    if (t < R(0) || t > R(1)) return s > 0;
     At = c(1) + (c(5) - c(1)) * t;
     Bt = c(4) + (c(8) - c(4)) * t;
     Ct = c(3) + (c(7) - c(3)) * t;
     Dt = c(2) + (c(6) - c(2)) * t;
   } else {
     const int* e = MC_INTERIOR_EDGE1[edge];
-    const T t = c(e[0]) / (c(e[0]) - c(e[1]));
+    const R t = c(e[0]) / (c(e[0]) - c(e[1]));
     Bt = c(e[2]) + (c(e[3]) - c(e[2])) * t;
     Ct = c(e[4]) + (c(e[5]) - c(e[4])) * t;
     Dt = c(e[6]) + (c(e[7]) - c(e[6])) * t;
   }
   int test = 0;
-  if (At >= T(0)) test += 1;
-  if (Bt >= T(0)) test += 2;
-  if (Ct >= T(0)) test += 4;
-  if (Dt >= T(0)) test += 8;
-  const T eps = std::numeric_limits<T>::epsilon();
+  if (At >= R(0)) test += 1;
+  if (Bt >= R(0)) test += 2;
+  if (Ct >= R(0)) test += 4;
+  if (Dt >= R(0)) test += 8;
+  const R eps = R(std::numeric_limits<T>::epsilon());
   if (test == 6 || test == 8 || test == 9 || test == 12 || (test >= 0 && test <= 4)) return s > 0;
   if (test == 5) return (At * Ct - Bt * Dt < eps) ? s > 0 : s < 0;
   if (test == 10) return (At * Ct - Bt * Dt >= eps) ? s > 0 : s < 0;
   return s < 0;
+}
+template <class T>
+inline bool test_interior(int itype, int edge, const T* cb, int s) {
+  return mixed_on<T>() ? test_interior_r<T, double>(itype, edge, cb, s) : test_interior_r<T, T>(itype, edge, cb, s);
 }
 
 struct McTable {
@@ -949,7 +986,7 @@ inline Plane<T, D> cell_plane(const Tape<T>& tp, const T* x0, const T* d, const 
   }
   for (int q = 0; q < D; ++q) pl.n[q] = r.g[q];
   pl.a = a;
-  pl.fraction = D == 2 ? gvf2(r.g[0], r.g[1], a) : gvf3(r.g[0], r.g[1], r.g[D - 1], a);
+  pl.fraction = D == 2 ? gvf2p(r.g[0], r.g[1], a) : gvf3p(r.g[0], r.g[1], r.g[D - 1], a);
   pl.valid = true;
   return pl;
 }
@@ -973,7 +1010,7 @@ inline T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k /*0-b
     if (!valid) return frac < T(0.5) ? T(0) : U * V;
     const T base = n[c] * s - a;
     if (n[p] == T(0) && n[q] == T(0)) return base >= T(0) ? U * V : T(0);
-    const T solid = gvf2(n[p], n[q], -base);
+    const T solid = gvf2p(n[p], n[q], -base);
     return (U * V) * (T(1) - solid);
   }
 }
@@ -1045,7 +1082,8 @@ T calc_volume(const cc_grid& g, const Tape<T>& tp) {
 }  // namespace oc
 
 // ======================================================================================
-// C entry points for the test harness (ctypes). prec: 0 = Float32, 1 = Float64.
+// C entry points for the test harness (ctypes). prec: 0 = Float32, 1 = Float64, 2 = mixed
+// (Float32 data with the Float64 islands).
 extern "C" {
 
 int oc_set_threads(int n) {
@@ -1054,6 +1092,7 @@ int oc_set_threads(int n) {
 }
 
 int oc_sample_nodes(int prec, const cc_grid* g, const cc_optape* t, void* phi) {
+  oc::MixedScope mixed(prec == 2);
   if (g->dim == 3) {
     if (prec == 1) oc::sample_nodes<double, 3>(*g, oc::make_tape<double>(t), (double*)phi);
     else oc::sample_nodes<float, 3>(*g, oc::make_tape<float>(t), (float*)phi);
@@ -1066,6 +1105,7 @@ int oc_sample_nodes(int prec, const cc_grid* g, const cc_optape* t, void* phi) {
 
 int oc_mc_cells_from_phi(int prec, const cc_grid* g, const uint8_t* table, const void* phi,
                          const cc_cells* c) {
+  oc::MixedScope mixed(prec == 2);
   oc::McTable tb;
   if (!tb.parse(table)) return CC_BAD_TABLE;
   if (prec == 1) oc::mc_cells<double>(*g, tb, (const double*)phi, *c);
@@ -1075,17 +1115,20 @@ int oc_mc_cells_from_phi(int prec, const cc_grid* g, const uint8_t* table, const
 
 int oc_mc_update(int prec, const cc_grid* g, const cc_optape* t, const uint8_t* table, void* phi,
                  const cc_cells* c) {
+  oc::MixedScope mixed(prec == 2);
   oc_sample_nodes(prec, g, t, phi);
   return oc_mc_cells_from_phi(prec, g, table, phi, c);
 }
 
 int oc_ms_cells_from_phi(int prec, const cc_grid* g, const void* phi, const cc_cells* c) {
+  oc::MixedScope mixed(prec == 2);
   if (prec == 1) oc::ms_cells<double>(*g, (const double*)phi, *c);
   else oc::ms_cells<float>(*g, (const float*)phi, *c);
   return 0;
 }
 
 int oc_ms_update(int prec, const cc_grid* g, const cc_optape* t, void* phi, const cc_cells* c) {
+  oc::MixedScope mixed(prec == 2);
   oc_sample_nodes(prec, g, t, phi);
   return oc_ms_cells_from_phi(prec, g, phi, c);
 }
@@ -1093,6 +1136,7 @@ int oc_ms_update(int prec, const cc_grid* g, const cc_optape* t, void* phi, cons
 int oc_ms_tree_update(int prec, const double* x0, const double* base_d, int64_t nleaves,
                       const int32_t* level, const int32_t* coord, const cc_optape* t, void* phi4,
                       const cc_cells* c) {
+  oc::MixedScope mixed(prec == 2);
   if (prec == 1) oc::ms_tree<double>(x0, base_d, nleaves, level, coord, oc::make_tape<double>(t), (double*)phi4, *c);
   else oc::ms_tree<float>(x0, base_d, nleaves, level, coord, oc::make_tape<float>(t), (float*)phi4, *c);
   return 0;
@@ -1100,6 +1144,7 @@ int oc_ms_tree_update(int prec, const double* x0, const double* base_d, int64_t 
 
 int oc_plic_update(int prec, const cc_grid* g, const cc_optape* t, const cc_cells* c, void* normals,
                    void* intercepts, uint8_t* is_valid) {
+  oc::MixedScope mixed(prec == 2);
   if (g->dim == 3) {
     if (prec == 1) oc::plic_update<double, 3>(*g, oc::make_tape<double>(t), *c, (double*)normals, (double*)intercepts, is_valid);
     else oc::plic_update<float, 3>(*g, oc::make_tape<float>(t), *c, (float*)normals, (float*)intercepts, is_valid);
@@ -1111,6 +1156,7 @@ int oc_plic_update(int prec, const cc_grid* g, const cc_optape* t, const cc_cell
 }
 
 double oc_calc_volume(int prec, const cc_grid* g, const cc_optape* t) {
+  oc::MixedScope mixed(prec == 2);
   if (g->dim == 3) {
     if (prec == 1) return oc::calc_volume<double, 3>(*g, oc::make_tape<double>(t));
     return double(oc::calc_volume<float, 3>(*g, oc::make_tape<float>(t)));
@@ -1121,6 +1167,7 @@ double oc_calc_volume(int prec, const cc_grid* g, const cc_optape* t) {
 
 // Every cell's cell_plane solid fraction, widened to double (the calc_volume integrand).
 int oc_plic_fractions(int prec, const cc_grid* g, const cc_optape* t, double* out) {
+  oc::MixedScope mixed(prec == 2);
   const int64_t n[3] = {g->n[0], g->n[1], g->dim == 3 ? g->n[2] : 1};
   const int64_t ncell = n[0] * n[1] * n[2];
   auto run = [&](auto zero, auto dimc) {
