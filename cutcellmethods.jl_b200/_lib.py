@@ -17,6 +17,11 @@ CC_F32, CC_F64, CC_MIXED = 0, 1, 2
 CC_MARCHING_SQUARES, CC_MARCHING_CUBES, CC_PLIC = 0, 1, 2
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("threads", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("chunk", C.c_int32), ("use_graph", C.c_int32)]
+
+
 class Grid(C.Structure):
     _fields_ = [("dim", C.c_int32), ("pad_", C.c_int32), ("x0", C.c_double * 3),
                 ("d", C.c_double * 3), ("n", C.c_int64 * 3)]
@@ -68,6 +73,16 @@ EXPORTS = {
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "cc_mc_update_learned": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_float, C.c_void_p, C.c_void_p],
+    "cc_batch_create": [C.c_int32, C.c_int32, C.c_void_p],
+    "cc_batch_destroy": [C.c_void_p],
+    "cc_batch_add_ms_grid": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_batch_add_ms_tree": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_batch_set_body": [C.c_void_p, C.c_int32, C.c_void_p],
+    "cc_batch_set_config": [C.c_void_p, C.c_void_p],
+    "cc_batch_get_config": [C.c_void_p, C.c_void_p],
+    "cc_batch_info": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_batch_run": [C.c_void_p, C.c_void_p],
+    "cc_batch_autotune": [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_version": [],
     "cc_last_error": [],
 }

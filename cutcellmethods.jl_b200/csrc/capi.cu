@@ -103,19 +103,19 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 namespace {
 
-// Pack a validated tape for the device -- each primitive's parameter block moved to a 4-element
-// boundary (read there with vector loads), each smooth-min k copied beside the blocks, everything
-// narrowed to T -- and upload it into the handle's buffer, ordered on stream s.
+}  // namespace
+
+namespace cci {
+
+// Pack a validated tape for the device into `out` (capacity tape_pack_capacity()): the ops,
+// padded to 16 bytes, then each primitive's parameter block moved to a 4-element boundary (read
+// there with vector loads), each smooth-min k copied beside the blocks, everything narrowed to T.
+// Returns the packed size in bytes; *n_params receives the packed parameter count.
 template <class T>
-cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, cci::DevTape* out) {
-  if (h->tape_pending) {
-    const cudaError_t e = cudaEventSynchronize(h->tape_copied);
-    if (e != cudaSuccess) return cuda_fail(e, "tape staging");
-    h->tape_pending = false;
-  }
+size_t pack_tape(const cc_optape* t, int dim, unsigned char* out, int* n_params) {
   const size_t ops_bytes = ((t->n_ops * sizeof(cc_op) + 15) / 16) * 16;
-  cc_op* ops = reinterpret_cast<cc_op*>(h->tape_host);
-  T* p = reinterpret_cast<T*>(h->tape_host + ops_bytes);
+  cc_op* ops = reinterpret_cast<cc_op*>(out);
+  T* p = reinterpret_cast<T*>(out + ops_bytes);
   int np = 0;
   for (int i = 0; i < t->n_ops; ++i) {
     cc_op op = t->ops[i];
@@ -136,8 +136,28 @@ cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s,
     }
     ops[i] = op;
   }
-  for (size_t b = t->n_ops * sizeof(cc_op); b < ops_bytes; ++b) h->tape_host[b] = 0;
-  const size_t bytes = ops_bytes + np * sizeof(T);
+  for (size_t b = t->n_ops * sizeof(cc_op); b < ops_bytes; ++b) out[b] = 0;
+  *n_params = np;
+  return ops_bytes + np * sizeof(T);
+}
+template size_t pack_tape<float>(const cc_optape*, int, unsigned char*, int*);
+template size_t pack_tape<double>(const cc_optape*, int, unsigned char*, int*);
+size_t tape_pack_capacity() { return TAPE_CAP; }
+
+}  // namespace cci
+
+namespace {
+
+// Pack a validated tape and upload it into the handle's buffer, ordered on stream s.
+template <class T>
+cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, cci::DevTape* out) {
+  if (h->tape_pending) {
+    const cudaError_t e = cudaEventSynchronize(h->tape_copied);
+    if (e != cudaSuccess) return cuda_fail(e, "tape staging");
+    h->tape_pending = false;
+  }
+  int np = 0;
+  const size_t bytes = cci::pack_tape<T>(t, dim, h->tape_host, &np);
   cudaError_t e = cudaMemcpyAsync(h->tape_dev, h->tape_host, bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_fail(e, "tape upload");
   e = cudaEventRecord(h->tape_copied, s);

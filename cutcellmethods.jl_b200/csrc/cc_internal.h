@@ -91,6 +91,11 @@ template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial,
                                double* out, cudaStream_t s, bool mixed = false);
 
+// Op-tape packing (capi.cu): pack a validated host tape for the device (see pack_tape).
+template <class T>
+size_t pack_tape(const cc_optape* t, int dim, unsigned char* out, int* n_params);
+size_t tape_pack_capacity();
+
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);
 

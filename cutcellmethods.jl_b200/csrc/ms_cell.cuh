@@ -1,0 +1,133 @@
+// ms_cell.cuh -- the per-cell marching-squares construction, shared by the grid, tree and
+// batched kernels: cut_cell_moments (2D), src/marching_squares/moments.jl:66-164, with
+// cell_boundary_walk (src/marching_squares/marching_squares.jl:240-251) and cell_gap_segments
+// (:291-317).
+#pragma once
+#include <cstdint>
+#include "cc_device.cuh"
+#include "cc_internal.h"
+
+namespace ccms {
+
+using namespace ccd;
+using cci::Cols;
+
+// MS_DIRECTION_EDGE (0-based), src/marching_squares/marching_squares.jl:81-82
+__host__ __device__ constexpr int dir_edge(int dir) { return dir == 0 ? 3 : dir == 1 ? 1 : dir == 2 ? 0 : 2; }
+
+// cut_cell_moments (2D), src/marching_squares/moments.jl:66-164, from global corner
+// coordinates `nd` (MS_NODE_BITS order) and corner values `ph`; writes cell `ci`'s columns.
+template <class T, bool MX>
+__device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Cols& cols, long long ci) {
+  const T o0 = nd[0][0], o1 = nd[0][1];
+  const T ce0 = o0 + T(0.5) * cs[0], ce1 = o1 + T(0.5) * cs[1];
+  const T vol_cell = cs[0] * cs[1];
+  int nout = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) nout += ph[k] >= T(0) ? 1 : 0;
+  T* vf = static_cast<T*>(cols.vf);
+  T* c = static_cast<T*>(cols.c);
+  T* ff = static_cast<T*>(cols.ff);
+  T* fcl = static_cast<T*>(cols.fcl);
+  T* ic = static_cast<T*>(cols.ic);
+  T fc[4];
+  if (nout == 4 || nout == 0) {
+    const bool out = nout == 4;
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+      const int k = dir_edge(dir), k1 = (k + 1) & 3;
+      const int p = dir < 2 ? 1 : 0;
+      fc[dir] = T(0.5) * (nd[k][p] + nd[k1][p]) - nd[0][p];
+    }
+    cols.kind[ci] = out ? 1 : 0;
+    cols.amb[ci] = 0;
+    vf[ci] = out ? T(1) : T(0);
+    c[2 * ci] = ce0; c[2 * ci + 1] = ce1;
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) { ff[4 * ci + dir] = out ? T(1) : T(0); fcl[4 * ci + dir] = fc[dir]; }
+    ic[2 * ci] = ce0; ic[2 * ci + 1] = ce1;
+    return;
+  }
+  // cell_boundary_walk, marching_squares.jl:240-251
+  T fr[4], sa[4][2], sb[4][2];
+  bool pr[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int k1 = (k + 1) & 3;
+    const T fa = ph[k], fb = ph[k1];
+    fr[k] = open_fraction<T, MX>(fa, fb);
+    pr[k] = fa >= T(0) || fb >= T(0);
+    if (fa >= T(0) && fb >= T(0)) {
+      sa[k][0] = nd[k][0]; sa[k][1] = nd[k][1]; sb[k][0] = nd[k1][0]; sb[k][1] = nd[k1][1];
+    } else if (fa >= T(0)) {
+      sa[k][0] = nd[k][0]; sa[k][1] = nd[k][1];
+      sb[k][0] = nd[k][0] + fr[k] * (nd[k1][0] - nd[k][0]);
+      sb[k][1] = nd[k][1] + fr[k] * (nd[k1][1] - nd[k][1]);
+    } else {
+      sa[k][0] = nd[k1][0] + fr[k] * (nd[k][0] - nd[k1][0]);
+      sa[k][1] = nd[k1][1] + fr[k] * (nd[k][1] - nd[k1][1]);
+      sb[k][0] = nd[k1][0]; sb[k][1] = nd[k1][1];
+    }
+  }
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir) {
+    const int k = dir_edge(dir), k1 = (k + 1) & 3;
+    const int p = dir < 2 ? 1 : 0;
+    const T x = pr[k] ? T(0.5) * (sa[k][p] + sb[k][p]) : T(0.5) * (nd[k][p] + nd[k1][p]);
+    fc[dir] = x - nd[0][p];
+    ff[4 * ci + dir] = fr[k];
+    fcl[4 * ci + dir] = fc[dir];
+  }
+  T area2 = T(0), m0 = T(0), m1 = T(0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!pr[k]) continue;
+    const T la0 = sa[k][0] - o0, la1 = sa[k][1] - o1, lb0 = sb[k][0] - o0, lb1 = sb[k][1] - o1;
+    const T cr = la0 * lb1 - la1 * lb0;
+    area2 = area2 + cr;
+    m0 = m0 + (la0 + lb0) * cr;
+    m1 = m1 + (la1 + lb1) * cr;
+  }
+  // cell_gap_segments, marching_squares.jl:291-317 (with _next_present, :255-264)
+  int nint = 0;
+  T ilen = T(0), im0 = T(0), im1 = T(0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!pr[k]) continue;
+    int j = (k + 1) & 3;
+    if (!pr[j]) { j = (j + 1) & 3; if (!pr[j]) { j = (j + 1) & 3; if (!pr[j]) j = k; } }
+    const T a0 = sb[k][0], a1 = sb[k][1];
+    const T b0 = j == 0 ? sa[0][0] : j == 1 ? sa[1][0] : j == 2 ? sa[2][0] : sa[3][0];
+    const T b1 = j == 0 ? sa[0][1] : j == 1 ? sa[1][1] : j == 2 ? sa[2][1] : sa[3][1];
+    if (a0 != b0 || a1 != b1) {
+      ++nint;
+      if (nint <= 2) {
+        const T la0 = a0 - o0, la1 = a1 - o1, lb0 = b0 - o0, lb1 = b1 - o1;
+        const T cr = la0 * lb1 - la1 * lb0;
+        area2 = area2 + cr;
+        m0 = m0 + (la0 + lb0) * cr;
+        m1 = m1 + (la1 + lb1) * cr;
+        const T v0 = b0 - a0, v1 = b1 - a1;
+        const T len = sqrt(v0 * v0 + v1 * v1);
+        ilen = ilen + len;
+        const T hl = T(0.5) * len;
+        im0 = im0 + hl * (a0 + b0);
+        im1 = im1 + hl * (a1 + b1);
+      }
+    }
+  }
+  const T area = T(0.5) * area2;
+  cols.kind[ci] = 2;
+  cols.amb[ci] = nint > 1 ? 1 : 0;
+  vf[ci] = area / vol_cell;
+  if (area2 != T(0)) {
+    const T den = T(3) * area2;
+    c[2 * ci] = o0 + m0 / den; c[2 * ci + 1] = o1 + m1 / den;
+  } else {
+    c[2 * ci] = ce0; c[2 * ci + 1] = ce1;
+  }
+  if (ilen > T(0)) { ic[2 * ci] = im0 / ilen; ic[2 * ci + 1] = im1 / ilen; }
+  else { ic[2 * ci] = ce0; ic[2 * ci + 1] = ce1; }
+}
+
+}  // namespace ccms

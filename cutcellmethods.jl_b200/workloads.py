@@ -55,3 +55,26 @@ def mc_bytes_per_update(n: int, elem: int) -> int:
     cells = n ** 3
     nodes = (n + 1) ** 3
     return cells * (2 + 25 * elem) + nodes * elem
+
+
+def moving_circle_updates(k: int = 256, seed: int = 0, n_min: int = 64, n_max: int = 1024):
+    """K updates of a translating circle (radius 0.3, velocity (0.4, 0.1), dt = 1e-3, centre
+    (-0.05, -0.0125) at t = 0) over [-1,1]^2, update i on its own n_i x n_i grid with n_i drawn
+    uniformly from [n_min, n_max]: a list of (grid, body, n_i)."""
+    from .geometry import Circle
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_min, n_max + 1, k)
+    out = []
+    for i in range(k):
+        t = i * 1e-3
+        c = (-0.05 + 0.4 * t, -0.0125 + 0.1 * t)
+        n = int(ns[i])
+        g = CartesianGrid((-1.0, -1.0), (n, n), (2.0 / n, 2.0 / n))
+        out.append((g, Circle(c, 0.3), n))
+    return out
+
+
+def star_body(amp, ph):
+    """The star curve r(theta) = 0.5 + sum_k a_k cos(k theta + phi_k), k = 2..6, as a body."""
+    from .geometry import Star
+    return Star((0.0, 0.0), 0.5, tuple(float(a) for a in amp), tuple(float(p) for p in ph))

@@ -257,6 +257,42 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
                     const void* volume_fraction, int64_t counts[5],
                     double* min_volume_fraction, void* stream);
 
+/* ---- batched marching squares -----------------------------------------------------------
+ * Many MarchingSquaresCutCell updates (update_cache! on a CartesianGrid,
+ * src/marching_squares/cache.jl:49-78, or on an AdaptiveMesh{2}'s leaves, :115-137), each with
+ * its own body and columns, in ONE persistent launch over a work list of grid tiles and leaf
+ * chunks, replayed from a CUDA graph. No counterpart entry point in the reference, which runs one
+ * update per call. Each item's results are bit-identical to cc_ms_update / cc_ms_tree_update on
+ * the same inputs, whatever the launch shape. The batch stores the items' device pointers; they
+ * must stay valid while the batch is run. */
+typedef struct cc_batch cc_batch;
+typedef struct {
+  int32_t tile_x, tile_y; /* grid tile in cells (1..256 each, at most 4096 cells) */
+  int32_t threads;        /* per CTA: a multiple of 32 in 32..256; also the leaves per tree chunk */
+  int32_t ctas_per_sm;    /* persistent CTAs per SM (148 SMs) */
+  int32_t chunk;          /* tiles taken per atomic pop */
+  int32_t use_graph;      /* replay a captured CUDA graph (1) or launch directly (0) */
+} cc_batch_config;
+cc_status cc_batch_create(int32_t device, int32_t prec, cc_batch** out);
+cc_status cc_batch_destroy(cc_batch* b);
+/* Add an update; *item (if not NULL) receives its index. The body must be a 2D op-tape. */
+cc_status cc_batch_add_ms_grid(cc_batch* b, const cc_grid* g, const cc_optape* body, void* phi,
+                               const cc_cells* cells, int32_t* item);
+cc_status cc_batch_add_ms_tree(cc_batch* b, const cc_tree* t, const cc_optape* body, void* phi4,
+                               const cc_cells* cells, int32_t* item);
+/* Move an item's body: the same op structure with new parameters (CC_BAD_TAPE otherwise). Waits
+ * for the batch's previous run; the next run uses the new parameters. */
+cc_status cc_batch_set_body(cc_batch* b, int32_t item, const cc_optape* body);
+cc_status cc_batch_set_config(cc_batch* b, const cc_batch_config* cfg);
+cc_status cc_batch_get_config(const cc_batch* b, cc_batch_config* cfg);
+/* Items, and the work list's tiles for the current configuration (-1 before the first run). */
+cc_status cc_batch_info(const cc_batch* b, int64_t* n_items, int64_t* total_tiles);
+/* Run every update, ordered after the work already on `stream` and before what follows it. */
+cc_status cc_batch_run(cc_batch* b, void* stream);
+/* Time every candidate launch shape (tiles 32x4..128x2, 128/256 threads, 2/4/8 CTAs per SM,
+ * chunks 1/4) on the batch as it stands, `reps` timed runs each, and keep the fastest. */
+cc_status cc_batch_autotune(cc_batch* b, int32_t reps, cc_batch_config* best, float* best_ms, void* stream);
+
 /* ---- learned volume-fraction correction ----------------------------------------------------
  * An MLP 8 -> 64 -> 64 -> 1 (GELU hidden layers, sigmoid output p; tensor-core GEMMs on BF16
  * operands with FP32 accumulate) that corrects marching cubes' fluid volume fraction of a cut
