@@ -23,6 +23,11 @@ larger than the 126 MB L2, so no flush is needed between steps).
   (CUDA events). Equal error: plain marching cubes' convergence order p is measured between n/2
   and n on the same body; plain reaches the learned error at n * (L1_plain / L1_learned)^(1/p)
   cells per axis, which costs (that / n)^3 plain updates at n.
+* ``batch``: the batched marching-squares workloads -- 256 updates of a translating circle
+  (radius 0.3, velocity (0.4, 0.1), dt 1e-3), update i on its own n_i x n_i grid of [-1,1]^2,
+  n_i ~ U{64..1024}, Float32 and Float64; and a quadtree refined from level 4 to 12 toward a star
+  curve -- as per-update launches against one autotuned, graph-captured batched launch (CUDA
+  events, the same caches).
 * ``cpu_baseline`` / ``--impl reference``: the oracle (a C++ restatement of the reference's CPU
   path, all host threads) on a bounded slab of the same workload -- the reference itself is Julia
   and cannot run here.
@@ -233,6 +238,7 @@ def run_ours(args, rank, world, dist):
     precision["degenerate_deciders"] = degenerate_decider_errors(cc, dev)
 
     learned = None if args.no_learned else learned_block(args, dev, cc)
+    batched = None if args.no_batch else batch_block(args, dev, cc)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
 
@@ -257,6 +263,7 @@ def run_ours(args, rank, world, dist):
                       "roofline_frac": bytes_per / (statistics.mean(perm) * 1e-3) / 1e9 / peak},
             "precision": precision,
             "learned": learned,
+            "batch": batched,
             "report": rep}
     if not args.no_cpu and world == 1:
         v, threads, sample = cpu_port_rate(n, 0)
@@ -335,6 +342,68 @@ def traffic_per_update(n):
     return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
 
 
+def batch_block(args, dev, cc, k=256):
+    """Batched updates against per-update launches (the moving-circle and quadtree workloads)."""
+    import importlib
+    import torch
+    Bm = importlib.import_module("cutcell_b200.batch")
+    W = cc.workloads
+    s = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 2)):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / reps
+
+    out = {}
+    for dtype, name in ((torch.float32, "f32"), (torch.float64, "f64")):
+        ups = W.moving_circle_updates(k, seed=0)
+        tapes = [cc.flatten(body, 2) for _, body, _ in ups]
+        caches = [cc.allocate_cache(g, cc.MarchingSquaresCutCell(), dtype=dtype, device=dev) for g, _, _ in ups]
+        cells = sum(g.ncell for g, _, _ in ups)
+        nodes = sum(g.nnode for g, _, _ in ups)
+        elem = 4 if dtype == torch.float32 else 8
+        algo = cells * (2 + 9 * elem) + nodes * elem
+
+        def per_update():
+            for c, (g, _, _), t in zip(caches, ups, tapes):
+                cc.update_cache(c, t, g, sync=False)
+        ms_single = timed(per_update, 3)
+        b = Bm.Batch(dtype=dtype, device=dev)
+        for c, (g, _, _), t in zip(caches, ups, tapes):
+            b.add(c, t, g)
+        cfg, tune_ms = b.autotune(reps=2)
+        ms_graph = timed(lambda: b.run(sync=False), 5)
+        b.configure(use_graph=0)
+        ms_direct = timed(lambda: b.run(sync=False), 5)
+        out[name] = {"updates": k, "cells": cells, "grids": "n x n, n ~ U{64..1024}, over [-1,1]^2",
+                     "ms_per_update_launches": ms_single, "ms_batched_graph": ms_graph, "ms_batched_direct": ms_direct,
+                     "speedup": ms_single / ms_graph, "cells_per_s_batched": cells / (ms_graph * 1e-3),
+                     "roofline_frac": algo / (ms_graph * 1e-3) / 1e9 / measured_peak()[0],
+                     "algorithmic_bytes": algo, "autotuned": cfg}
+        del b, caches
+        torch.cuda.empty_cache()
+    tree, amp, ph = cc.star_curve_tree(0, 4, 12)
+    body = cc.flatten(W.star_body(amp, ph), 2)
+    tc = cc.allocate_cache(tree, cc.MarchingSquaresCutCell(), dtype=torch.float32, device=dev)
+    ms_tree = timed(lambda: cc.update_cache(tc, body, tree, sync=False), 5)
+    bt = Bm.Batch(dtype=torch.float32, device=dev)
+    bt.add(tc, body, tree)
+    cfg, _ = bt.autotune(reps=3)
+    ms_tree_b = timed(lambda: bt.run(sync=False), 10)
+    out["quadtree"] = {"leaves": tree.nleaves, "levels": "4..12 toward a star curve (seed 0)",
+                       "ms_single_update": ms_tree, "ms_batched_graph": ms_tree_b,
+                       "leaves_per_s_batched": tree.nleaves / (ms_tree_b * 1e-3), "autotuned": cfg}
+    return out
+
+
 def learned_block(args, dev, cc):
     """Accuracy and cost of the learned correction against plain marching cubes (see the module
     docstring)."""
@@ -396,6 +465,7 @@ def main():
     ap.add_argument("--prec", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
