@@ -73,6 +73,10 @@ EXPORTS = {
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "cc_mc_update_learned": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_float, C.c_void_p, C.c_void_p],
+    "cc_mc_mesh": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_mc_mesh_cell_indices": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                C.c_void_p],
     "cc_batch_create": [C.c_int32, C.c_int32, C.c_void_p],
     "cc_batch_destroy": [C.c_void_p],
     "cc_batch_add_ms_grid": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],

@@ -294,6 +294,8 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->rep_scratch) cudaFree(h->rep_scratch);
   if (h->cut_list) cudaFree(h->cut_list);
   if (h->cut_count) cudaFree(h->cut_count);
+  if (h->mesh_vbase) cudaFree(h->mesh_vbase);
+  if (h->mesh_scan) cudaFree(h->mesh_scan);
   delete h;
   return CC_OK;
 }

@@ -126,5 +126,9 @@ struct cc_handle {
   unsigned* cut_count = nullptr;
   double* vol_scratch = nullptr;  // calc_volume partials + result
   unsigned long long* rep_scratch = nullptr;  // report counters + min
+  unsigned* mesh_vbase = nullptr;  // generate_mesh: first vertex of each node's cut edges
+  size_t mesh_vbase_n = 0;
+  unsigned long long* mesh_scan = nullptr;  // generate_mesh: per-block counts and offsets
+  size_t mesh_scan_n = 0;
 };
 

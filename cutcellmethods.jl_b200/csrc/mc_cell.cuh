@@ -214,6 +214,22 @@ __device__ __forceinline__ void put_cell(const Stage<T>& st, long long lc, int k
   st.ic[3 * lc] = ic[0]; st.ic[3 * lc + 1] = ic[1]; st.ic[3 * lc + 2] = ic[2];
 }
 
+// cell_triangles over the table (src/marching_cubes/marching_cubes.jl:538-651): the tile of a cube
+// with nudged corner values `phi` (MC_NODE_BITS order).
+template <class T, bool MX = false>
+__device__ __forceinline__ int mc_tile(const T phi[8], const DevTable& tb) {
+  int lut = 0;
+#pragma unroll
+  for (int p = 0; p < 8; ++p) lut |= (phi[p] >= T(0) ? 1 : 0) << p;
+  const cc_mc_lut ent = tb.luts[lut];
+  int o = 0;
+  for (int i = 0; i < ent.ntests; ++i) o |= (test_face<T, MX>(phi, ent.face[i]) ? 1 : 0) << i;
+  const cc_mc_outcome oc = tb.outs[ent.outcome_base + o];
+  int tile = oc.tile_true;
+  if (oc.itype != CC_MC_INTERIOR_NONE && !test_interior<T, MX>(oc.itype, oc.edge, phi, oc.s)) tile = oc.tile_false;
+  return tile;
+}
+
 // cut_cell_moments (3D) for a cut cell, src/marching_cubes/moments.jl:275-346. `phr` are the
 // raw corner values in MC_NODE_BITS order, `l` the cell's lattice edge lengths
 // (x_{i+1} - x_i per axis: every corner's cell-local coordinate is 0 or l exactly), `org` the
@@ -229,17 +245,7 @@ __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T o
   for (int a = 0; a < 3; ++a) centre[a] = org[a] + T(0.5) * cs[a];
   const T vol_cell = (cs[0] * cs[1]) * cs[2];
 
-  // cell_triangles over the table (src/marching_cubes/marching_cubes.jl:538-651)
-  int lut = 0;
-#pragma unroll
-  for (int p = 0; p < 8; ++p) lut |= (phi[p] >= T(0) ? 1 : 0) << p;
-  const cc_mc_lut ent = tb.luts[lut];
-  int o = 0;
-  for (int i = 0; i < ent.ntests; ++i) o |= (test_face<T, MX>(phi, ent.face[i]) ? 1 : 0) << i;
-  const cc_mc_outcome oc = tb.outs[ent.outcome_base + o];
-  int tile = oc.tile_true;
-  if (oc.itype != CC_MC_INTERIOR_NONE && !test_interior<T, MX>(oc.itype, oc.edge, phi, oc.s)) tile = oc.tile_false;
-  const cc_mc_tile tl = tb.tiles[tile];
+  const cc_mc_tile tl = tb.tiles[mc_tile<T, MX>(phi, tb)];
 
   // the six face clips (cut_cell_faces / _cut_cell_face, moments.jl:150-257)
   T ff[6], fcl[12];
@@ -372,7 +378,10 @@ __device__ __noinline__ void mc_cut_cell(const T phr[8], const T l[3], const T o
   } else {
     ic[0] = centre[0]; ic[1] = centre[1]; ic[2] = centre[2];
   }
-  const int lc_case = ent.lcase;
+  int lut = 0;
+#pragma unroll
+  for (int p = 0; p < 8; ++p) lut |= (phi[p] >= T(0) ? 1 : 0) << p;
+  const int lc_case = tb.luts[lut].lcase;
   const bool amb_case = lc_case == 5 || lc_case == 7 || lc_case == 8 || lc_case == 11 || lc_case == 13 || lc_case == 14;
   put_cell<T>(st, lc, 2, (amb_face || amb_case) ? 1 : 0, volume / vol_cell, c, ff, fcl, ic);
 }

@@ -1,0 +1,441 @@
+// mesh.cu -- generate_mesh for a marching-cubes cache on the device
+// (src/marching_cubes/surface.jl:82-112, where the reference marches cache.phi serially on the host).
+//
+// The surface is the one the cache's cut cells integrate: every cut cell's triangles are the
+// tile its moments used (the same table, the same face and interior deciders), and a vertex on
+// a grid edge is that edge's crossing as the cells place it, anchored on the outside node:
+// x_out + s (x_in - x_out), s = phi_out / (phi_out - phi_in), nudged corner values. Every cell
+// around an edge computes the same vertex, so the vertex is stored once and shared: the mesh is
+// watertight and wound so each triangle's normal points out of the body. A tile's code 13 is
+// the cell's interior vertex, the mean of its crossings.
+//
+// The numbering is deterministic: first the edge vertices, each owned by its edge's lower node,
+// nodes in linear order (x fastest) and each node's x, y, z edges in that order; then the
+// interior vertices, cells in linear order; triangles by cell in linear order, each cell's in
+// tile order. Two passes of three kernels each count per block, scan the block totals and emit
+// through in-block scans. The edge pass keeps each node's first vertex, so a cell's triangles can
+// name the vertices of edges other nodes own.
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/cutcell_b200.h"
+#include "cc_device.cuh"
+#include "cc_internal.h"
+#include "mc_cell.cuh"
+
+namespace {
+
+using namespace ccd;
+using namespace ccmc;
+using cci::DevGrid;
+using cci::DevTable;
+
+constexpr int MB = 256;          // threads per block
+constexpr int IPT = 16;          // items per thread
+constexpr int BLK = MB * IPT;    // nodes or cells per block
+
+template <class T>
+__device__ __forceinline__ bool outside(T v) { return nudge(v) >= T(0); }
+
+// Bit a set: node (i,j,k)'s edge to the next node along axis a crosses the surface.
+template <class T>
+__device__ __forceinline__ unsigned node_edges(const T* __restrict__ phi, long long i, long long j, long long k,
+                                               const long long n[3]) {
+  const long long nx = n[0] + 1, ny = n[1] + 1;
+  const long long v = i + nx * (j + ny * k);
+  const bool o = outside(phi[v]);
+  unsigned m = 0;
+  if (i < n[0] && outside(phi[v + 1]) != o) m |= 1u;
+  if (j < n[1] && outside(phi[v + nx]) != o) m |= 2u;
+  if (k < n[2] && outside(phi[v + nx * ny]) != o) m |= 4u;
+  return m;
+}
+
+// The crossing on node v's edge along axis a (world coordinates), as the cells place it.
+template <class T>
+__device__ __forceinline__ void edge_vertex(const T* __restrict__ phi, const DevGrid<T>& g, long long i, long long j,
+                                            long long k, int a, T out[3]) {
+  const long long nx = g.n[0] + 1, ny = g.n[1] + 1;
+  const long long v = i + nx * (j + ny * k);
+  const long long w = v + (a == 0 ? 1 : a == 1 ? nx : nx * ny);
+  const T fa = nudge(phi[v]), fb = nudge(phi[w]);
+  const long long idx[3] = {i, j, k};
+  T xa[3], xb[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    xa[q] = node_coord(g.x0[q], g.d[q], idx[q]);
+    xb[q] = node_coord(g.x0[q], g.d[q], idx[q] + (q == a ? 1 : 0));
+  }
+  const T s = open_fraction(fa, fb);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) out[q] = fa >= T(0) ? xa[q] + s * (xb[q] - xa[q]) : xb[q] + s * (xa[q] - xb[q]);
+}
+
+// Exclusive scan of one value per thread over the block; returns the prefix, *total the sum.
+__device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long* total) {
+  __shared__ unsigned long long warp_sum[MB / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long v = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) warp_sum[w] = v;
+  __syncthreads();
+  unsigned long long base = 0, all = 0;
+  for (int q = 0; q < MB / 32; ++q) {
+    if (q < w) base += warp_sum[q];
+    all += warp_sum[q];
+  }
+  __syncthreads();
+  *total = all;
+  return base + v - x;
+}
+
+// ---- the edge vertices ----------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(MB) node_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                        unsigned long long* bsum) {
+  const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
+  const long long v0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  unsigned long long c = 0;
+  for (int q = 0; q < IPT; ++q) {
+    const long long v = v0 + q;
+    if (v < nn) c += __popc(node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n));
+  }
+  unsigned long long total;
+  block_scan(c, &total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(MB) node_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                       const unsigned long long* __restrict__ boff,
+                                                       unsigned* __restrict__ vbase, T* __restrict__ verts) {
+  const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
+  const long long v0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  unsigned m[IPT];
+  unsigned long long c = 0;
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    const long long v = v0 + q;
+    m[q] = v < nn ? node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n) : 0u;
+    c += __popc(m[q]);
+  }
+  unsigned long long total;
+  unsigned long long id = boff[blockIdx.x] + block_scan(c, &total);
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    const long long v = v0 + q;
+    if (v >= nn) break;
+    vbase[v] = unsigned(id);
+    if (verts) {
+      const long long i = v % nx, j = (v / nx) % ny, k = v / (nx * ny);
+      for (int a = 0; a < 3; ++a) {
+        if (!(m[q] >> a & 1u)) continue;
+        T p[3];
+        edge_vertex(phi, g, i, j, k, a, p);
+        verts[3 * id] = p[0]; verts[3 * id + 1] = p[1]; verts[3 * id + 2] = p[2];
+        ++id;
+      }
+    } else {
+      id += __popc(m[q]);
+    }
+  }
+}
+
+// ---- the cells: triangles and interior vertices ----------------------------------------------
+template <class T>
+__device__ __forceinline__ void corners(const T* __restrict__ phi, const long long n[3], long long i, long long j,
+                                        long long k, T ph[8]) {
+  const long long nx = n[0] + 1, ny = n[1] + 1;
+  const long long b0 = i + nx * (j + ny * k), bz = nx * ny;
+  const T r[8] = {phi[b0], phi[b0 + 1], phi[b0 + nx + 1], phi[b0 + nx],
+                  phi[b0 + bz], phi[b0 + bz + 1], phi[b0 + bz + nx + 1], phi[b0 + bz + nx]};
+#pragma unroll
+  for (int c = 0; c < 8; ++c) ph[c] = nudge(r[c]);
+}
+
+// A cell's triangle count and whether its tile uses the interior vertex (code 13); -1 tile if
+// the cell is not cut.
+template <class T, bool MX>
+__device__ __forceinline__ int cell_tile(const T ph[8], const DevTable& tb, int& ntris, int& interior) {
+  int nout = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) nout += ph[c] >= T(0) ? 1 : 0;
+  ntris = 0;
+  interior = 0;
+  if (nout == 0 || nout == 8) return -1;
+  const int tile = mc_tile<T, MX>(ph, tb);
+  const cc_mc_tile tl = tb.tiles[tile];
+  ntris = tl.ntris;
+  const uint8_t* codes = tb.codes + tl.code_off;
+  for (int q = 0; q < 3 * tl.ntris; ++q) interior |= codes[q] == 13 ? 1 : 0;
+  return tile;
+}
+
+template <class T, bool MX>
+__global__ void __launch_bounds__(MB) cell_count_kernel(const T* __restrict__ phi, const DevGrid<T> g, const DevTable tb,
+                                                        unsigned long long* bsum) {
+  const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
+  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  unsigned long long t = 0, in = 0;
+  for (int q = 0; q < IPT; ++q) {
+    const long long c = c0 + q;
+    if (c >= nc) break;
+    T ph[8];
+    corners(phi, g.n, c % n0, (c / n0) % n1, c / (n0 * n1), ph);
+    int nt, it;
+    cell_tile<T, MX>(ph, tb, nt, it);
+    t += nt;
+    in += it;
+  }
+  unsigned long long tt, ti;
+  block_scan(t, &tt);
+  block_scan(in, &ti);
+  if (threadIdx.x == 0) {
+    bsum[2 * blockIdx.x] = tt;
+    bsum[2 * blockIdx.x + 1] = ti;
+  }
+}
+
+template <class T, bool MX>
+__global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g, const DevTable tb,
+                                                       const unsigned long long* __restrict__ boff,
+                                                       const unsigned* __restrict__ vbase, unsigned long long n_edge_verts,
+                                                       T* __restrict__ verts, int32_t* __restrict__ tris,
+                                                       int64_t* __restrict__ tri_cells) {
+  const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
+  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  unsigned long long t = 0, in = 0;
+  for (int q = 0; q < IPT; ++q) {
+    const long long c = c0 + q;
+    if (c >= nc) break;
+    T ph[8];
+    corners(phi, g.n, c % n0, (c / n0) % n1, c / (n0 * n1), ph);
+    int nt, it;
+    cell_tile<T, MX>(ph, tb, nt, it);
+    t += nt;
+    in += it;
+  }
+  unsigned long long tt, ti;
+  unsigned long long tri_id = boff[2 * blockIdx.x] + block_scan(t, &tt);
+  unsigned long long int_id = n_edge_verts + boff[2 * blockIdx.x + 1] + block_scan(in, &ti);
+  for (int q = 0; q < IPT; ++q) {
+    const long long c = c0 + q;
+    if (c >= nc) break;
+    const long long i = c % n0, j = (c / n0) % n1, k = c / (n0 * n1);
+    T ph[8];
+    corners(phi, g.n, i, j, k, ph);
+    int nt, it;
+    const int tile = cell_tile<T, MX>(ph, tb, nt, it);
+    if (tile < 0) continue;
+    // the vertex of each of the cell's twelve edges (code e + 1), from its lower node's numbering
+    unsigned vid[12];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) {
+      const int ca = edge_node(e, 0), cb = edge_node(e, 1);
+      const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
+      const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
+      const long long li = i + cbit(lo, 0), lj = j + cbit(lo, 1), lk = k + cbit(lo, 2);
+      const unsigned m = node_edges(phi, li, lj, lk, g.n);
+      const long long v = li + (g.n[0] + 1) * (lj + (g.n[1] + 1) * lk);
+      vid[e] = vbase[v] + __popc(m & ((1u << a) - 1u));
+    }
+    unsigned centre = 0;
+    if (it) {
+      centre = unsigned(int_id++);
+      T acc[3] = {T(0), T(0), T(0)};
+      int ncr = 0;
+      for (int e = 0; e < 12; ++e) {
+        const int ca = edge_node(e, 0), cb = edge_node(e, 1);
+        if ((ph[ca] >= T(0)) == (ph[cb] >= T(0))) continue;
+        const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
+        const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
+        T p[3];
+        edge_vertex(phi, g, i + cbit(lo, 0), j + cbit(lo, 1), k + cbit(lo, 2), a, p);
+        acc[0] = acc[0] + p[0]; acc[1] = acc[1] + p[1]; acc[2] = acc[2] + p[2];
+        ++ncr;
+      }
+      if (verts) {
+        verts[3 * (long long)centre] = acc[0] / T(ncr);
+        verts[3 * (long long)centre + 1] = acc[1] / T(ncr);
+        verts[3 * (long long)centre + 2] = acc[2] / T(ncr);
+      }
+    }
+    const cc_mc_tile tl = tb.tiles[tile];
+    const uint8_t* codes = tb.codes + tl.code_off;
+    for (int r = 0; r < tl.ntris; ++r, ++tri_id) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int code = codes[3 * r + q];
+        tris[3 * tri_id + q] = int32_t(code == 13 ? centre : vid[code - 1]);
+      }
+      if (tri_cells) tri_cells[tri_id] = c;
+    }
+  }
+}
+
+// Exclusive scan of `n` per-block counts (stride values apart, `lanes` interleaved series) in one
+// CTA, in place; totals[l] receives series l's sum.
+__global__ void scan_blocks_kernel(unsigned long long* a, long long n, int lanes, unsigned long long* totals) {
+  __shared__ unsigned long long carry[4];
+  if (threadIdx.x < 4) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int l = 0; l < lanes; ++l) {
+    for (long long base = 0; base < n; base += MB) {
+      const long long q = base + threadIdx.x;
+      const unsigned long long x = q < n ? a[q * lanes + l] : 0ull;
+      unsigned long long total;
+      const unsigned long long pre = block_scan(x, &total);
+      if (q < n) a[q * lanes + l] = carry[l] + pre;
+      __syncthreads();
+      if (threadIdx.x == 0) carry[l] += total;
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x < lanes) totals[threadIdx.x] = carry[threadIdx.x];
+}
+
+cc_status fail(cc_status s, const std::string& m) {
+  cci::set_last_error(m);
+  return s;
+}
+cc_status cuda_fail(cudaError_t e, const char* where) {
+  cci::set_last_error(std::string(where) + ": " + cudaGetErrorString(e));
+  return CC_CUDA_ERR;
+}
+
+template <class T>
+DevGrid<T> grid_of(const cc_grid* g) {
+  DevGrid<T> d;
+  for (int a = 0; a < 3; ++a) {
+    d.x0[a] = T(g->x0[a]);
+    d.d[a] = T(g->d[a]);
+    d.n[a] = g->n[a];
+  }
+  return d;
+}
+
+template <class T, bool MX>
+cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int64_t vcap, int32_t* tris, int64_t tcap,
+                   int64_t* tri_cells, int64_t* nv, int64_t* nt, cudaStream_t s) {
+  const DevGrid<T> g = grid_of<T>(gg);
+  const long long nn = (g.n[0] + 1) * (g.n[1] + 1) * (g.n[2] + 1);
+  const long long nc = g.n[0] * g.n[1] * g.n[2];
+  const long long nbn = (nn + BLK - 1) / BLK, nbc = (nc + BLK - 1) / BLK;
+  if (nn > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 nodes");
+  cudaError_t e = cudaSuccess;
+  if (size_t(nn) > h->mesh_vbase_n) {
+    if (h->mesh_vbase) cudaFree(h->mesh_vbase);
+    h->mesh_vbase = nullptr;
+    h->mesh_vbase_n = 0;
+    if ((e = cudaMalloc(&h->mesh_vbase, size_t(nn) * sizeof(unsigned))) != cudaSuccess)
+      return cuda_fail(e, "generate_mesh scratch");
+    h->mesh_vbase_n = size_t(nn);
+  }
+  const size_t scan_n = size_t(nbn + 2 * nbc + 8);
+  if (scan_n > h->mesh_scan_n) {
+    if (h->mesh_scan) cudaFree(h->mesh_scan);
+    h->mesh_scan = nullptr;
+    h->mesh_scan_n = 0;
+    if ((e = cudaMalloc(&h->mesh_scan, scan_n * sizeof(unsigned long long))) != cudaSuccess)
+      return cuda_fail(e, "generate_mesh scratch");
+    h->mesh_scan_n = scan_n;
+  }
+  unsigned long long* nb = h->mesh_scan;              // node blocks
+  unsigned long long* cb = nb + nbn;                  // cell blocks (tris, interior) interleaved
+  unsigned long long* tot = cb + 2 * nbc;             // edge vertices, tris, interior vertices
+  node_count_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb);
+  scan_blocks_kernel<<<1, MB, 0, s>>>(nb, nbn, 1, tot);
+  cell_count_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb);
+  scan_blocks_kernel<<<1, MB, 0, s>>>(cb, nbc, 2, tot + 1);
+  unsigned long long t[3];
+  if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(t, tot, sizeof t, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "generate_mesh count");
+  const long long n_vert = (long long)(t[0] + t[2]), n_tri = (long long)t[1];
+  if (nv) *nv = n_vert;
+  if (nt) *nt = n_tri;
+  if (!verts && !tris) return CC_OK;  // counting only
+  if (!verts || !tris || vcap < n_vert || tcap < n_tri)
+    return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
+  if (n_vert > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 vertices");
+  node_emit_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, h->mesh_vbase, verts);
+  cell_emit_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, h->mesh_vbase, t[0], verts, tris, tri_cells);
+  if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "generate_mesh emit");
+  return CC_OK;
+}
+
+// cell_indices (src/marching_cubes/surface.jl:128-143): the cell of each triangle, from its
+// vertices' centroid (summed and divided in the mesh's precision) floored against the grid in
+// Float64, clamped to the grid.
+template <class T>
+__global__ void cell_index_kernel(const cc_grid g, const T* __restrict__ verts, const int32_t* __restrict__ tris,
+                                  long long nt, int64_t* __restrict__ out) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt; t += (long long)gridDim.x * blockDim.x) {
+    const long long va = tris[3 * t], vb = tris[3 * t + 1], vc = tris[3 * t + 2];
+    long long idx[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const T cT = ((verts[3 * va + a] + verts[3 * vb + a]) + verts[3 * vc + a]) / T(3);
+      const double c = double(cT);
+      long long q = (long long)floor((c - g.x0[a]) / g.d[a]);
+      q = q < 0 ? 0 : (q > g.n[a] - 1 ? g.n[a] - 1 : q);
+      idx[a] = q;
+    }
+    out[t] = idx[0] + g.n[0] * (idx[1] + g.n[1] * idx[2]);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+cc_status cc_mc_mesh(cc_handle* h, const cc_grid* g, const void* phi, void* vertices, int64_t vertex_capacity,
+                     int32_t* triangles, int64_t triangle_capacity, int64_t* triangle_cells, int64_t* n_vertices,
+                     int64_t* n_triangles, void* stream) {
+  if (!h || !g || !phi) return fail(CC_BAD_ARG, "null argument");
+  if (h->method != CC_MARCHING_CUBES) return fail(CC_BAD_ARG, "handle was created for another method");
+  if (g->dim != 3) return fail(CC_DIM_MISMATCH, "grid dimension differs from the cache's");
+  for (int a = 0; a < 3; ++a)
+    if (g->n[a] != h->n[a]) return fail(CC_DIM_MISMATCH, "grid size differs from the cache's");
+  if (!h->table_dev) return fail(CC_NO_TABLE, "no marching-cubes tiling table set on the handle");
+  int old = -1;
+  cudaGetDevice(&old);
+  if (old != h->device) cudaSetDevice(h->device);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cc_status st;
+  if (h->prec == CC_F64)
+    st = run_mesh<double, false>(h, g, static_cast<const double*>(phi), static_cast<double*>(vertices), vertex_capacity,
+                                 triangles, triangle_capacity, triangle_cells, n_vertices, n_triangles, s);
+  else if (h->prec == CC_MIXED)
+    st = run_mesh<float, true>(h, g, static_cast<const float*>(phi), static_cast<float*>(vertices), vertex_capacity,
+                               triangles, triangle_capacity, triangle_cells, n_vertices, n_triangles, s);
+  else
+    st = run_mesh<float, false>(h, g, static_cast<const float*>(phi), static_cast<float*>(vertices), vertex_capacity,
+                                triangles, triangle_capacity, triangle_cells, n_vertices, n_triangles, s);
+  if (old >= 0 && old != h->device) cudaSetDevice(old);
+  return st;
+}
+
+cc_status cc_mc_mesh_cell_indices(cc_handle* h, const cc_grid* g, const void* vertices, const int32_t* triangles,
+                                  int64_t n_triangles, int64_t* cells, void* stream) {
+  if (!h || !g || (n_triangles > 0 && (!vertices || !triangles || !cells)) || n_triangles < 0)
+    return fail(CC_BAD_ARG, "null argument");
+  if (g->dim != 3) return fail(CC_DIM_MISMATCH, "a 3D grid");
+  if (n_triangles == 0) return CC_OK;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int blocks = int(n_triangles / 256 + 1 < 148 * 16 ? n_triangles / 256 + 1 : 148 * 16);
+  if (h->prec == CC_F64)
+    cell_index_kernel<double><<<blocks, 256, 0, s>>>(*g, static_cast<const double*>(vertices), triangles, n_triangles, cells);
+  else
+    cell_index_kernel<float><<<blocks, 256, 0, s>>>(*g, static_cast<const float*>(vertices), triangles, n_triangles, cells);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? CC_OK : cuda_fail(e, "cell_indices");
+}
+
+}  // extern "C"

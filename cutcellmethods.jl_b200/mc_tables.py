@@ -16,7 +16,8 @@ kernels read:
 * ``project_table()`` builds a project-designed tiling in that format: on every cut face the
   chords are paired exactly as the face clip pairs them (``face_outside_connected`` on a saddle,
   src/marching_cubes/marching_cubes.jl:421-422), so the chords close into loops, and each loop is
-  fanned into triangles wound out of the body. It is watertight with the face clips by
+  fanned into triangles wound out of the body, from an apex that leaves no triangle flat in a cube
+  face (so the marched surface is manifold). It is watertight with the face clips by
   construction, so volumes are exact for planar interfaces; it is NOT MarchingCubes.jl's tiling, so
   non-planar cut cells' volume and centroids differ from the reference's (the real tables are
   encoded into the same format by the Julia shim, julia/CutCellB200.jl).
@@ -195,13 +196,34 @@ def _loops(lut, connect):
     return loops
 
 
-def _fan(loops, rot=0):
+def _edge_faces(code):
+    """The two cube faces (directions 0..5) containing edge ``code`` (1-based)."""
+    a, b = MC_EDGE_NODES[code - 1]
+    return {d for d in range(6) if (a - 1) in face_nodes(d) and (b - 1) in face_nodes(d)}
+
+
+def _flat(tri):
+    """Whether a triangle of edge codes lies in one cube face (its three edges share a face)."""
+    return bool(_edge_faces(tri[0]) & _edge_faces(tri[1]) & _edge_faces(tri[2]))
+
+
+def _fan(loops, alt=0):
+    """Fan each loop into triangles from the first apex (rotation) that puts no triangle flat in a
+    cube face -- a flat triangle would meet its mirror from the neighbouring cell and make the
+    surface non-manifold -- or, with ``alt``, from the next such apex (a second, different fan).
+    A loop with no such apex is fanned from the cell's interior vertex (code 13)."""
     tris = []
     for lp in loops:
-        r = rot % len(lp)
-        lp = lp[r:] + lp[:r]
-        for i in range(1, len(lp) - 1):
-            tris.append((lp[0], lp[i], lp[i + 1]))
+        good = []
+        for r in range(len(lp)):
+            q = lp[r:] + lp[:r]
+            fan = [(q[0], q[i], q[i + 1]) for i in range(1, len(q) - 1)]
+            if not any(_flat(t) for t in fan):
+                good.append(fan)
+        if good:
+            tris += good[alt % len(good)]
+        else:
+            tris += [(13, lp[i], lp[(i + 1) % len(lp)]) for i in range(len(lp))]
     return tris
 
 
@@ -232,7 +254,7 @@ def _build(probe: bool):
                 itype = 1 if lc in (5, 11) else 2
                 edge = crossed[o % len(crossed)] if crossed else 0
                 s = 1 if (o & 1) == 0 else -1
-                outcomes.append((itype, edge, s, t_true, tile_id(_fan(loops, 1))))
+                outcomes.append((itype, edge, s, t_true, tile_id(_fan(loops, alt=1))))
             else:
                 outcomes.append((0, 0, 0, t_true, t_true))
         luts.append((lc, len(dirs), faces, base))

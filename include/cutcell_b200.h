@@ -257,6 +257,25 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
                     const void* volume_fraction, int64_t counts[5],
                     double* min_volume_fraction, void* stream);
 
+/* generate_mesh for a marching-cubes cache (src/marching_cubes/surface.jl:82-112), on the device:
+ * the surface its cut cells integrate -- each cut cell's triangles the tile its moments used, a
+ * vertex on a grid edge that edge's crossing as the cells place it (anchored on the outside node),
+ * shared by every cell around the edge, code 13 the cell's interior vertex (the mean of its
+ * crossings). Watertight inside the grid, open at its bounds, wound so each triangle's normal
+ * points out of the body. `phi` is the cache's nodal field. vertices T[n_vertices][3],
+ * triangles int32[n_triangles][3] (0-based vertex indices), triangle_cells int64[n_triangles]
+ * (the cell of each triangle; may be NULL). Order: edge vertices by lower node (linear, x fastest)
+ * then axis x, y, z; then interior vertices by cell; triangles by cell, each cell's in tile order.
+ * Call with vertices = triangles = NULL to count; then with arrays of at least the counted
+ * sizes. Blocking. Scratch: 4 bytes per node, kept on the handle. */
+cc_status cc_mc_mesh(cc_handle* h, const cc_grid* g, const void* phi, void* vertices, int64_t vertex_capacity,
+                     int32_t* triangles, int64_t triangle_capacity, int64_t* triangle_cells,
+                     int64_t* n_vertices, int64_t* n_triangles, void* stream);
+/* cell_indices (src/marching_cubes/surface.jl:128-143): each triangle's cell, 0-based linear index,
+ * from its centroid floored against the grid (in Float64), clamped to the grid. Blocking. */
+cc_status cc_mc_mesh_cell_indices(cc_handle* h, const cc_grid* g, const void* vertices, const int32_t* triangles,
+                                  int64_t n_triangles, int64_t* cells, void* stream);
+
 /* ---- batched marching squares -----------------------------------------------------------
  * Many MarchingSquaresCutCell updates (update_cache! on a CartesianGrid,
  * src/marching_squares/cache.jl:49-78, or on an AdaptiveMesh{2}'s leaves, :115-137), each with

@@ -908,6 +908,125 @@ void mc_cells(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells&
   });
 }
 
+// generate_mesh (src/marching_cubes/surface.jl:82-112) restated for the project's device mesh:
+// every cut cell's triangles are its tile's, each edge vertex the crossing anchored on the
+// outside node in world coordinates, shared; code 13 the mean of the cell's crossings. Numbered
+// serially: edge vertices by lower node (linear order) then axis, interior vertices by cell,
+// triangles by cell.
+template <class T>
+struct Mesh {
+  std::vector<T> verts;
+  std::vector<int32_t> tris;
+  std::vector<int64_t> cells;
+};
+
+template <class T>
+inline T nudged_at(const T* phi, int64_t v) { return nudge(phi[v]); }
+
+template <class T>
+void edge_vertex(const T x0[3], const T d[3], const T* phi, const int64_t n[3], int64_t i, int64_t j, int64_t k,
+                 int a, T out[3]) {
+  const int64_t nx = n[0] + 1, ny = n[1] + 1;
+  const int64_t v = i + nx * (j + ny * k);
+  const int64_t w = v + (a == 0 ? 1 : a == 1 ? nx : nx * ny);
+  const T fa = nudge(phi[v]), fb = nudge(phi[w]);
+  const int64_t idx[3] = {i, j, k};
+  T xa[3], xb[3];
+  for (int q = 0; q < 3; ++q) {
+    xa[q] = node_coord(x0[q], d[q], idx[q]);
+    xb[q] = node_coord(x0[q], d[q], idx[q] + (q == a ? 1 : 0));
+  }
+  const T s = open_fraction(fa, fb);
+  for (int q = 0; q < 3; ++q) out[q] = fa >= T(0) ? xa[q] + s * (xb[q] - xa[q]) : xb[q] + s * (xa[q] - xb[q]);
+}
+
+template <class T>
+Mesh<T> mc_mesh(const cc_grid& g, const McTable& tb, const T* phi) {
+  const int64_t n[3] = {g.n[0], g.n[1], g.n[2]};
+  const int64_t nx = n[0] + 1, ny = n[1] + 1, nz = n[2] + 1;
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
+  const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  Mesh<T> m;
+  std::vector<uint32_t> vbase(size_t(nx * ny * nz));
+  auto out = [&](int64_t v) { return nudge(phi[v]) >= T(0); };
+  auto edges = [&](int64_t i, int64_t j, int64_t k) {
+    const int64_t v = i + nx * (j + ny * k);
+    unsigned msk = 0;
+    if (i < n[0] && out(v + 1) != out(v)) msk |= 1u;
+    if (j < n[1] && out(v + nx) != out(v)) msk |= 2u;
+    if (k < n[2] && out(v + nx * ny) != out(v)) msk |= 4u;
+    return msk;
+  };
+  uint32_t id = 0;
+  for (int64_t k = 0; k < nz; ++k)
+    for (int64_t j = 0; j < ny; ++j)
+      for (int64_t i = 0; i < nx; ++i) {
+        const unsigned msk = edges(i, j, k);
+        vbase[size_t(i + nx * (j + ny * k))] = id;
+        for (int a = 0; a < 3; ++a) {
+          if (!(msk >> a & 1u)) continue;
+          T p[3];
+          edge_vertex(x0, d, phi, n, i, j, k, a, p);
+          m.verts.insert(m.verts.end(), p, p + 3);
+          ++id;
+        }
+      }
+  std::vector<T> interior;
+  for (int64_t k = 0; k < n[2]; ++k)
+    for (int64_t j = 0; j < n[1]; ++j)
+      for (int64_t i = 0; i < n[0]; ++i) {
+        T ph[8];
+        int nout = 0;
+        for (int q = 0; q < 8; ++q) {
+          ph[q] = nudge(phi[(i + MC_BITS[q][0]) + nx * ((j + MC_BITS[q][1]) + ny * (k + MC_BITS[q][2]))]);
+          nout += ph[q] >= T(0) ? 1 : 0;
+        }
+        if (nout == 0 || nout == 8) continue;
+        const uint8_t* codes;
+        int lcase;
+        const int nt = cell_triangles(tb, ph, &codes, &lcase);
+        uint32_t vid[12];
+        T acc[3] = {T(0), T(0), T(0)};
+        int ncr = 0;
+        for (int e = 0; e < 12; ++e) {
+          const int ca = MC_EDGE_NODES1[e][0] - 1, cb = MC_EDGE_NODES1[e][1] - 1;
+          const int a = MC_BITS[ca][0] != MC_BITS[cb][0] ? 0 : (MC_BITS[ca][1] != MC_BITS[cb][1] ? 1 : 2);
+          const int lo = MC_BITS[ca][a] < MC_BITS[cb][a] ? ca : cb;
+          const int64_t li = i + MC_BITS[lo][0], lj = j + MC_BITS[lo][1], lk = k + MC_BITS[lo][2];
+          const unsigned msk = edges(li, lj, lk);
+          vid[e] = vbase[size_t(li + nx * (lj + ny * lk))] + uint32_t(__builtin_popcount(msk & ((1u << a) - 1u)));
+          if ((ph[ca] >= T(0)) != (ph[cb] >= T(0))) {
+            T p[3];
+            edge_vertex(x0, d, phi, n, li, lj, lk, a, p);
+            acc[0] = acc[0] + p[0]; acc[1] = acc[1] + p[1]; acc[2] = acc[2] + p[2];
+            ++ncr;
+          }
+        }
+        bool uses13 = false;
+        for (int q = 0; q < 3 * nt; ++q) uses13 = uses13 || codes[q] == 13;
+        uint32_t centre = 0;
+        if (uses13) {
+          centre = uint32_t(interior.size() / 3);
+          interior.push_back(acc[0] / T(ncr));
+          interior.push_back(acc[1] / T(ncr));
+          interior.push_back(acc[2] / T(ncr));
+        }
+        for (int r = 0; r < nt; ++r) {
+          for (int q = 0; q < 3; ++q) {
+            const int code = codes[3 * r + q];
+            // an interior vertex is numbered after all edge vertices: a placeholder until then
+            m.tris.push_back(code == 13 ? -1 - int32_t(centre) : int32_t(vid[code - 1]));
+          }
+          m.cells.push_back(i + n[0] * (j + n[1] * k));
+        }
+      }
+  const int32_t ne = int32_t(m.verts.size() / 3);
+  for (auto& t : m.tris)
+    if (t < 0) t = ne + (-1 - t);
+  m.verts.insert(m.verts.end(), interior.begin(), interior.end());
+  return m;
+}
+
 static const int MS_BITS[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
 
 template <class T>
@@ -1118,6 +1237,25 @@ int oc_mc_update(int prec, const cc_grid* g, const cc_optape* t, const uint8_t* 
   oc::MixedScope mixed(prec == 2);
   oc_sample_nodes(prec, g, t, phi);
   return oc_mc_cells_from_phi(prec, g, table, phi, c);
+}
+
+// generate_mesh: counts into *nv / *nt; arrays written when non-null (capacities checked).
+int oc_mc_mesh(int prec, const cc_grid* g, const uint8_t* table, const void* phi, void* verts, int64_t vcap,
+               int32_t* tris, int64_t tcap, int64_t* cells, int64_t* nv, int64_t* nt) {
+  oc::MixedScope mixed(prec == 2);
+  oc::McTable tb;
+  if (!tb.parse(table)) return CC_BAD_TABLE;
+  auto run = [&](auto m) {
+    using TT = typename std::decay<decltype(m.verts[0])>::type;
+    *nv = int64_t(m.verts.size() / 3);
+    *nt = int64_t(m.tris.size() / 3);
+    if (verts && *nv <= vcap) std::memcpy(verts, m.verts.data(), m.verts.size() * sizeof(TT));
+    if (tris && *nt <= tcap) std::memcpy(tris, m.tris.data(), m.tris.size() * sizeof(int32_t));
+    if (cells && *nt <= tcap) std::memcpy(cells, m.cells.data(), m.cells.size() * sizeof(int64_t));
+    return 0;
+  };
+  if (prec == 1) return run(oc::mc_mesh<double>(*g, tb, (const double*)phi));
+  return run(oc::mc_mesh<float>(*g, tb, (const float*)phi));
 }
 
 int oc_ms_cells_from_phi(int prec, const cc_grid* g, const void* phi, const cc_cells* c) {

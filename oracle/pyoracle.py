@@ -57,6 +57,8 @@ def lib():
         L.oc_eval_tape.restype = C.c_double
         L.oc_ms_tree_update.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_mc_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -131,6 +133,24 @@ def mc_cells_from_phi(g, phi, table: bytes, prec):
                                     C.byref(cells_struct(cols)))
     assert rc == 0
     return cols
+
+
+def mc_mesh(g, phi, table: bytes, prec):
+    """The marching-cubes surface of the nodal field phi: (vertices [nv, 3], triangles [nt, 3] int32,
+    cell of each triangle [nt] int64)."""
+    phi = np.ascontiguousarray(phi, dtype_of(prec))
+    tb = np.frombuffer(table, np.uint8).copy()
+    nv, nt = C.c_int64(0), C.c_int64(0)
+    gs = grid_struct(g)
+    rc = lib().oc_mc_mesh(prec, C.byref(gs), _ptr(tb), _ptr(phi), None, 0, None, 0, None, C.byref(nv), C.byref(nt))
+    assert rc == 0
+    v = np.zeros((nv.value, 3), dtype_of(prec))
+    t = np.zeros((nt.value, 3), np.int32)
+    c = np.zeros(nt.value, np.int64)
+    rc = lib().oc_mc_mesh(prec, C.byref(gs), _ptr(tb), _ptr(phi), _ptr(v), nv.value, _ptr(t), nt.value, _ptr(c),
+                          C.byref(nv), C.byref(nt))
+    assert rc == 0
+    return v, t, c
 
 
 def mc_update(g, tape, table: bytes, prec):

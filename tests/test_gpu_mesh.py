@@ -1,0 +1,66 @@
+"""generate_mesh on the B200 through the C ABI: the marching-cubes surface of a cache's phi, bit for
+bit the oracle's (vertices, triangles, the cell of each triangle), and cell_indices."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import cc, po, XorShift, bits
+
+pytestmark = pytest.mark.gpu
+S = __import__("cutcell_b200.surface", fromlist=["surface"])
+TABLE = cc.mc_tables.project_table()
+DT = {0: torch.float32, 1: torch.float64, 2: torch.float32}
+
+
+def cache_for(g, geo, prec):
+    c = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=DT[prec], precision="mixed" if prec == 2 else "plain")
+    return cc.update_cache(c, geo, g)
+
+
+def check_against_oracle(cache, g, prec):
+    m = S.generate_mesh(cache, g)
+    v, t, owner = po.mc_mesh(g, cache.phi.cpu().numpy(), TABLE, prec)
+    assert m.nodes.shape[0] == v.shape[0] > 0 and m.elements.shape[0] == t.shape[0]
+    assert np.array_equal(bits(m.nodes.cpu().numpy()), bits(v))
+    assert np.array_equal(m.elements.cpu().numpy(), t)
+    assert np.array_equal(m.cells.cpu().numpy(), owner)
+    return m
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_mesh_bitwise(prec):
+    for body, g in ((cc.Sphere((0.01, 0.02, -0.03), 1.0), cc.grid3(40)), (cc.workloads.csg_body(0), cc.workloads.csg_grid(64)),
+                    (cc.workloads.smooth_blob(4), cc.CartesianGrid((0.02, -0.01, 0.0), (48, 37, 29), (0.021, 0.028, 0.035)))):
+        check_against_oracle(cache_for(g, body, prec), g, prec)
+
+
+def test_mesh_of_a_nodal_field_and_cell_indices():
+    n = 35
+    g = cc.CartesianGrid((0.0, 0.0, 0.0), (n, n, n), (1.0, 1.0, 1.0))
+    rng = XorShift(31337)
+    vals = np.array([rng.randn() for _ in range((n + 1) ** 3)])
+    cache = cc.allocate_cache(g, cc.MarchingCubesCutCell())
+    cc.update_cache(cache, cc.NodalField(torch.as_tensor(vals)), g)
+    m = check_against_oracle(cache, g, 1)
+    # every triangle's cell is a cut cell, and every cut cell has triangles
+    kinds = cache.cells.kind.cpu().numpy()
+    assert np.array_equal(np.unique(m.cells.cpu().numpy()), np.flatnonzero(kinds == 2))
+    # cell_indices floors each centroid: the emitting cell, except triangles flush in a shared face
+    ci = S.cell_indices(m, g, cache).cpu().numpy()
+    own = m.cells.cpu().numpy()
+    v = m.nodes.cpu().numpy()[m.elements.cpu().numpy()]
+    flush = np.zeros(len(ci), bool)
+    for a in range(3):
+        flush |= np.all(np.abs(v[:, :, a] - np.round(v[:, :, a])) == 0, axis=1)
+    assert np.all((ci == own) | flush)
+    assert (ci == own).mean() > 0.99
+
+
+def test_mesh_edge_cases():
+    g = cc.grid3(16)
+    empty = cache_for(g, cc.Sphere((5.0, 5.0, 5.0), 0.5), 1)
+    with pytest.warns(UserWarning):
+        m = S.generate_mesh(empty, g)
+    assert m.nodes.shape[0] == 0 and m.elements.shape[0] == 0
+    with pytest.raises(cc.DimensionMismatch):
+        S.generate_mesh(empty, cc.grid3(17))
