@@ -28,6 +28,8 @@ larger than the 126 MB L2, so no flush is needed between steps).
   n_i ~ U{64..1024}, Float32 and Float64; and a quadtree refined from level 4 to 12 toward a star
   curve -- as per-update launches against one autotuned, graph-captured batched launch (CUDA
   events, the same caches).
+* ``mesh``: generate_mesh (count and emit) of the Float32 CSG cache on the device, and the oracle's
+  serial march of a bounded slab of the same field.
 * ``cpu_baseline`` / ``--impl reference``: the oracle (a C++ restatement of the reference's CPU
   path, all host threads) on a bounded slab of the same workload -- the reference itself is Julia
   and cannot run here.
@@ -239,6 +241,7 @@ def run_ours(args, rank, world, dist):
 
     learned = None if args.no_learned else learned_block(args, dev, cc)
     batched = None if args.no_batch else batch_block(args, dev, cc)
+    mesh = mesh_block(args, dev, cc)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
 
@@ -264,6 +267,7 @@ def run_ours(args, rank, world, dist):
             "precision": precision,
             "learned": learned,
             "batch": batched,
+            "mesh": mesh,
             "report": rep}
     if not args.no_cpu and world == 1:
         v, threads, sample = cpu_port_rate(n, 0)
@@ -340,6 +344,46 @@ def traffic_per_update(n):
         return None
     s = n / 256.0
     return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
+
+
+def mesh_block(args, dev, cc):
+    """generate_mesh of the Float32 CSG cache at n^3 on the device, against the oracle's serial
+    march of a bounded slab of the same field."""
+    import importlib
+    import numpy as np
+    import torch
+    S = importlib.import_module("cutcell_b200.surface")
+    n = args.n
+    g = cc.workloads.csg_grid(n)
+    cache = cc.update_cache(cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32, device=dev),
+                            cc.workloads.csg_body(0), g)
+    for _ in range(max(args.warmup, 2)):
+        m = S.generate_mesh(cache, g)
+    torch.cuda.synchronize(dev)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m = S.generate_mesh(cache, g)
+    torch.cuda.synchronize(dev)
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    out = {"grid": f"{n}^3 CSG body, Float32", "ms": ms, "vertices": int(m.nodes.shape[0]),
+           "triangles": int(m.elements.shape[0]), "cells_per_s": n ** 3 / (ms * 1e-3)}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        slab = 8
+        k0 = n // 2 - slab // 2
+        nx = n + 1
+        phi = cache.phi.reshape(n + 1, nx, nx)[k0:k0 + slab + 1].cpu().numpy().reshape(-1)
+        sub = cc.CartesianGrid((g.x0[0], g.x0[1], g.x0[2] + k0 * g.d[2]), (n, n, slab), g.d)
+        table = cc.mc_tables.project_table()
+        t0 = time.perf_counter()
+        po.mc_mesh(sub, phi, table, 0)
+        dt = time.perf_counter() - t0
+        out["cpu_oracle_serial"] = {"cells_per_s": n * n * slab / dt, "sample": f"oracle mc_mesh of a {n}x{n}x{slab} slab"}
+    del cache, m
+    torch.cuda.empty_cache()
+    return out
 
 
 def batch_block(args, dev, cc, k=256):
