@@ -28,6 +28,9 @@ larger than the 126 MB L2, so no flush is needed between steps).
   n_i ~ U{64..1024}, Float32 and Float64; and a quadtree refined from level 4 to 12 toward a star
   curve -- as per-update launches against one autotuned, graph-captured batched launch (CUDA
   events, the same caches).
+* ``plic``: PLICCutCell over [0,1]^3 at the same n, a union of 64 seeded spheres: update times
+  in Float32, Float64 and mixed precision, the resolved face fractions' single-valuedness, the
+  errors against Float64, and calc_volume against a 10^8-point Monte Carlo estimate.
 * ``mesh``: generate_mesh (count and emit) of the Float32 CSG cache on the device, and the oracle's
   serial march of a bounded slab of the same field.
 * ``cpu_baseline`` / ``--impl reference``: the oracle (a C++ restatement of the reference's CPU
@@ -242,6 +245,7 @@ def run_ours(args, rank, world, dist):
     learned = None if args.no_learned else learned_block(args, dev, cc)
     batched = None if args.no_batch else batch_block(args, dev, cc)
     mesh = mesh_block(args, dev, cc)
+    plic = None if args.no_plic else plic_block(args, dev, cc)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
 
@@ -268,6 +272,7 @@ def run_ours(args, rank, world, dist):
             "learned": learned,
             "batch": batched,
             "mesh": mesh,
+            "plic": plic,
             "report": rep}
     if not args.no_cpu and world == 1:
         v, threads, sample = cpu_port_rate(n, 0)
@@ -344,6 +349,76 @@ def traffic_per_update(n):
         return None
     s = n / 256.0
     return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
+
+
+def plic_block(args, dev, cc):
+    """PLIC over [0,1]^3 at n^3, a union of 64 seeded spheres: update times (Float32, Float64,
+    mixed), the resolved face fractions' single-valuedness, every precision's error against
+    Float64, and calc_volume against a 10^8-point Monte Carlo estimate."""
+    import math
+    import torch
+    n = args.n
+    g = cc.workloads.unit_grid(n)
+    body = cc.workloads.sphere_cloud(0, 64)
+    tape = cc.flatten(body, 3)
+    s = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / reps
+
+    def faces_single_valued(c):
+        ff = c.cells.face_fraction.reshape(n, n, n, 6)
+        bad = 0
+        for ax, dim in ((0, 2), (1, 1), (2, 0)):  # x, y, z (the tensor is [z, y, x, dir])
+            lo = ff.narrow(dim, 1, n - 1)[..., 2 * ax]
+            hi = ff.narrow(dim, 0, n - 1)[..., 2 * ax + 1]
+            bad += int((lo.view(torch.int32 if ff.dtype == torch.float32 else torch.int64) !=
+                        hi.view(torch.int32 if ff.dtype == torch.float32 else torch.int64)).sum().item())
+        return bad
+
+    out = {"grid": f"[0,1]^3 at {n}^3", "body": "union of 64 spheres, centres U[0.1,0.9]^3, radii U[0.02,0.08], seed 0"}
+    ref = cc.allocate_cache(g, cc.PLICCutCell(), dtype=torch.float64, device=dev)
+    ms64 = timed(lambda: cc.update_cache(ref, tape, g, sync=False), args.steps)
+    out["f64"] = {"ms": ms64, "cells_per_s": n ** 3 / (ms64 * 1e-3), "shared_face_mismatches": faces_single_valued(ref)}
+    for name, prec in (("f32", "plain"), ("mixed", "mixed")):
+        c = cc.allocate_cache(g, cc.PLICCutCell(), dtype=torch.float32, device=dev, precision=prec)
+        ms = timed(lambda: cc.update_cache(c, tape, g, sync=False), args.steps)
+        vf = (c.cells.volume_fraction.double() - ref.cells.volume_fraction).abs()
+        fd = (c.cells.face_fraction.double() - ref.cells.face_fraction).abs()
+        out[name] = {"ms": ms, "cells_per_s": n ** 3 / (ms * 1e-3),
+                     "roofline_frac": n ** 3 * 46 / (ms * 1e-3) / 1e9 / measured_peak()[0],
+                     "shared_face_mismatches": faces_single_valued(c),
+                     "is_valid_differs_from_f64": int((c.is_valid != ref.is_valid).sum().item()),
+                     "kind_differs_from_f64": int((c.cells.kind != ref.cells.kind).sum().item()),
+                     "vf_err_vs_f64": {"max": vf.max().item(), "mean": vf.mean().item()},
+                     "face_fraction_err_vs_f64": {"max": fd.max().item(), "mean": fd.mean().item()}}
+        del c, vf, fd
+        torch.cuda.empty_cache()
+    del ref
+    torch.cuda.empty_cache()
+    vols = {}
+    for name, dt, prec in (("f64", torch.float64, "plain"), ("f32", torch.float32, "plain"),
+                           ("mixed", torch.float32, "mixed")):
+        t0 = time.perf_counter()
+        vols[name] = cc.calc_volume(tape, g, dtype=dt, precision=prec)
+        vols[name + "_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    mc, inside = cc.monte_carlo_volume(body, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 100_000_000, 0)
+    mc_ms = (time.perf_counter() - t0) * 1e3
+    sigma = math.sqrt(mc * (1 - mc) / 1e8)
+    out["calc_volume"] = dict(vols, monte_carlo={"points": 100_000_000, "seed": 0, "volume": mc, "std_error": sigma,
+                                                 "ms": mc_ms},
+                              f64_minus_mc_in_sigmas=(vols["f64"] - mc) / sigma)
+    return out
 
 
 def mesh_block(args, dev, cc):
@@ -510,6 +585,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-plic", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -31,7 +31,7 @@ def __getattr__(name):
     if name in ("allocate_cache", "update_cache", "MarchingCubesCutCellCache",
                 "MarchingSquaresCutCellCache", "PLICCutCellCache", "calc_volume",
                 "cut_cell_report", "face_fractions", "volume_fractions", "kinds", "CCError",
-                "DimensionMismatch", "ArgumentError", "NodalField", "CellColumns"):
+                "DimensionMismatch", "ArgumentError", "NodalField", "CellColumns", "monte_carlo_volume"):
         from . import cache
         return getattr(cache, name)
     raise AttributeError(name)

@@ -73,6 +73,8 @@ EXPORTS = {
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "cc_mc_update_learned": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_float, C.c_void_p, C.c_void_p],
+    "cc_monte_carlo_volume": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p,
+                              C.c_void_p, C.c_void_p],
     "cc_mc_mesh": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_mc_mesh_cell_indices": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,

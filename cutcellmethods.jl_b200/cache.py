@@ -354,6 +354,26 @@ def calc_volume(geo, grid: CartesianGrid, dtype=torch.float64, device=None, prec
     return out.value
 
 
+def monte_carlo_volume(geo, lo, hi, n_points: int, seed: int = 0, device=None):
+    """(volume, points inside): the Monte Carlo measure of {phi < 0} in the box lo..hi from
+    n_points seeded points, on the device in Float64 (an independent check of calc_volume)."""
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    device = torch.device(device)
+    dev = device.index if device.index is not None else torch.cuda.current_device()
+    key = (dev, _lib.CC_F64)
+    if key not in _vol_handles:
+        _vol_handles[key] = _Handle(dev, _lib.CC_PLIC, 3, _lib.CC_F64, (1, 1, 1))
+    h = _vol_handles[key]
+    tp = _TapeRef(as_tape(geo, 3))
+    l = (C.c_double * 3)(*lo)
+    u = (C.c_double * 3)(*hi)
+    inside, vol = C.c_int64(0), C.c_double(0.0)
+    _check(h.lib.cc_monte_carlo_volume(h.h, C.byref(tp.s), l, u, n_points, seed, C.byref(inside), C.byref(vol),
+                                       _stream(device)))
+    return vol.value, inside.value
+
+
 def cut_cell_report(cache):
     """Counts by kind, ambiguous, and the smallest non-zero cut volume fraction
     (src/cut_cell.jl:302-319), reduced on the device."""

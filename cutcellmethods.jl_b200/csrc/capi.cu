@@ -140,6 +140,18 @@ size_t pack_tape(const cc_optape* t, int dim, unsigned char* out, int* n_params)
   *n_params = np;
   return ops_bytes + np * sizeof(T);
 }
+// 1 for a union (PUSH then MIN) of spheres, 2 for a smooth union (PUSH then SMIN), else 0.
+int tape_prunable(const cc_optape* t) {
+  if (t->n_ops < 2 || t->ops[0].combine != CC_COMB_PUSH) return 0;
+  const int mode = t->ops[1].combine;
+  if (mode != CC_COMB_MIN && mode != CC_COMB_SMIN) return 0;
+  for (int i = 0; i < t->n_ops; ++i) {
+    if (t->ops[i].opcode != CC_OP_SPHERE) return 0;
+    if (i > 0 && t->ops[i].combine != mode) return 0;
+  }
+  return mode == CC_COMB_MIN ? 1 : 2;
+}
+
 template size_t pack_tape<float>(const cc_optape*, int, unsigned char*, int*);
 template size_t pack_tape<double>(const cc_optape*, int, unsigned char*, int*);
 size_t tape_pack_capacity() { return TAPE_CAP; }
@@ -167,6 +179,7 @@ cc_status upload_tape(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s,
   out->n_ops = t->n_ops;
   out->n_params = np;
   out->bytes_len = int(bytes);
+  out->prunable = cci::tape_prunable(t);
   return CC_OK;
 }
 
@@ -523,6 +536,29 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "calc_volume");
   *out = sum * pd;
+  return CC_OK;
+}
+
+cc_status cc_monte_carlo_volume(cc_handle* h, const cc_optape* body, const double lo[3], const double hi[3],
+                                int64_t n_points, uint64_t seed, int64_t* inside, double* volume, void* stream) {
+  if (!h || !lo || !hi || !inside || n_points < 0) return fail(CC_BAD_ARG, "null argument");
+  for (int a = 0; a < 3; ++a)
+    if (!(hi[a] > lo[a])) return fail(CC_BAD_ARG, "empty box");
+  cc_status st = validate_tape(body, 3);
+  if (st != CC_OK) return st;
+  DeviceGuard dg(h->device);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cci::DevTape tape{nullptr, 0, 0, 0};
+  if ((st = upload_tape<double>(h, body, 3, s, &tape)) != CC_OK) return st;
+  unsigned long long* cnt = h->rep_scratch;  // the report's counter slots, free between calls
+  cudaError_t e = cci::launch_monte_carlo(tape, lo, hi, n_points, seed, cnt, s);
+  unsigned long long c = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&c, cnt, sizeof c, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "cc_monte_carlo_volume");
+  *inside = (int64_t)c;
+  if (volume)
+    *volume = n_points > 0 ? double(c) / double(n_points) * ((hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2])) : 0.0;
   return CC_OK;
 }
 

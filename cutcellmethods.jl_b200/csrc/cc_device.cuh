@@ -461,6 +461,71 @@ __device__ __forceinline__ STape<T> load_tape(const unsigned char* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------------------------
+// Pruning a union of spheres to a region. For a tape that is a union (mode 1: PUSH then MIN) or
+// smooth union (mode 2: PUSH then SMIN) of spheres, and a box containing every point a CTA will
+// evaluate, the ops that cannot change any of those values are dropped:
+//  * union: sphere i is dropped when its smallest value over the box exceeds the largest value of
+//    some other sphere there -- it is then strictly above the minimum everywhere, never selected,
+//    and the minimum (value and gradient) is bit-identical without it;
+//  * smooth union: sphere i (i > 0) is dropped when its smallest value exceeds, by its smoothing k,
+//    the largest value over the box of every earlier sphere's minimum -- then the smooth-min step
+//    sees |top - v| >= k, h = 0, and returns the running value unchanged, bit for bit.
+// The bounds carry a margin of 16 eps(T) times the magnitudes involved, so T's rounding of the
+// evaluation can not cross them. All threads call this; it returns the kept op count and writes
+// the kept ops (the first one's combine made PUSH) to `out`. `ls`, `us`: n_ops doubles each.
+template <class T, int D>
+__device__ int prune_union(const STape<T>& t, int mode, const double lo[D], const double hi[D], double* ls, double* us,
+                           cc_op* out, int* count) {
+  const int n = t.n_ops;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const T* p = t.p + t.ops[i].poff;
+    double dmin2 = 0.0, dmax2 = 0.0, mag = fabs(double(p[D])) + 1.0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double c = p[a];
+      const double below = lo[a] - c, above = c - hi[a];
+      const double dn = below > 0.0 ? below : (above > 0.0 ? above : 0.0);
+      const double dx = fabs(lo[a] - c) > fabs(hi[a] - c) ? fabs(lo[a] - c) : fabs(hi[a] - c);
+      dmin2 += dn * dn;
+      dmax2 += dx * dx;
+      mag += fabs(c) + (fabs(lo[a]) > fabs(hi[a]) ? fabs(lo[a]) : fabs(hi[a]));
+    }
+    const double r = p[D];
+    const double margin = 16.0 * double(Eps<T>::v()) * (mag + sqrt(dmax2));
+    ls[i] = sqrt(dmin2) - r - margin;
+    us[i] = sqrt(dmax2) - r + margin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int m = 0;
+    if (mode == 1) {
+      int jm = 0;
+      for (int j = 1; j < n; ++j) if (us[j] < us[jm]) jm = j;
+      double u2 = 1.0e300;
+      for (int j = 0; j < n; ++j) if (j != jm && us[j] < u2) u2 = us[j];
+      for (int i = 0; i < n; ++i) {
+        if (ls[i] > (i == jm ? u2 : us[jm])) continue;
+        cc_op op = t.ops[i];
+        if (m == 0) op.combine = CC_COMB_PUSH;
+        out[m++] = op;
+      }
+    } else {
+      double prefix = us[0];
+      out[m++] = t.ops[0];
+      for (int i = 1; i < n; ++i) {
+        const double k = t.p[t.ops[i].kparam];
+        const double kmargin = 16.0 * double(Eps<T>::v()) * (fabs(k) + fabs(prefix) + fabs(ls[i]) + 1.0);
+        if (!(ls[i] >= prefix + k + kmargin)) out[m++] = t.ops[i];
+        if (us[i] < prefix) prefix = us[i];
+      }
+    }
+    *count = m;
+  }
+  __syncthreads();
+  return *count;
+}
+
+// ---------------------------------------------------------------------------------------------
 // CartesianMeshes stand-ins: node and centroid coordinates, the plane-cube clip.
 template <class T> __device__ __forceinline__ T node_coord(T x0, T d, long long i) { return x0 + T(i) * d; }
 template <class T> __device__ __forceinline__ T centroid_coord(T x0, T d, long long i) {

@@ -31,6 +31,7 @@ struct DevTape {
   int n_ops;
   int n_params;
   int bytes_len;
+  int prunable = 0;  // 1: a union (MIN) of spheres, 2: a smooth union (SMIN) of spheres; see prune_union
 };
 
 struct Cols {
@@ -87,6 +88,9 @@ cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& co
 // calc_volume partial sums: nblocks (sum, compensation) pairs into `partial`, then a final
 // single-block pass into out[0..1]. `partial` holds 2 * calc_volume_blocks() doubles.
 int calc_volume_blocks();
+// Monte Carlo count of points of the box lo..hi where the body is negative (see plic.cu).
+cudaError_t launch_monte_carlo(const DevTape& tape, const double lo[3], const double hi[3], long long npts,
+                               unsigned long long seed, unsigned long long* out, cudaStream_t s);
 template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial,
                                double* out, cudaStream_t s, bool mixed = false);
@@ -95,6 +99,7 @@ cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double*
 template <class T>
 size_t pack_tape(const cc_optape* t, int dim, unsigned char* out, int* n_params);
 size_t tape_pack_capacity();
+int tape_prunable(const cc_optape* t);
 
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);

@@ -64,25 +64,76 @@ __device__ __forceinline__ PlaneFit<T, D> cell_plane(const STape<T>& t, const De
   return pl;
 }
 
+// The cell tiles the centroid kernels work in: NT cells, 32 along x (coalesced stores), and the
+// tape pruned to the box of each tile's centroids when the body is a union of spheres.
+template <int D> struct PTile;
+template <> struct PTile<3> { static constexpr int X = 32, Y = 4, Z = 2; };
+template <> struct PTile<2> { static constexpr int X = 32, Y = 8, Z = 1; };
+
+// Shared-memory layout of a centroid kernel: the tape, then the pruned ops and the bounds.
+struct CentroidSmem {
+  int ops_off, ls_off, us_off, bytes;
+  __host__ __device__ static CentroidSmem of(const DevTape& tape) {
+    CentroidSmem c;
+    c.ops_off = ((tape.bytes_len + 15) / 16) * 16;
+    c.ls_off = c.ops_off + ((tape.n_ops * int(sizeof(cc_op)) + 15) / 16) * 16;
+    c.us_off = c.ls_off + tape.n_ops * 8;
+    c.bytes = c.us_off + tape.n_ops * 8;
+    return c;
+  }
+};
+
+// The tape a tile's cells are evaluated with: pruned to the tile's centroid box if it can be.
+template <class T, int D>
+__device__ __forceinline__ STape<T> tile_tape(const STape<T>& t, const DevTape& tape, const DevGrid<T>& g,
+                                              const long long i0[3], unsigned char* smem, int* count) {
+  if (!tape.prunable) return t;
+  const CentroidSmem L = CentroidSmem::of(tape);
+  const int ext[3] = {PTile<D>::X, PTile<D>::Y, PTile<D>::Z};
+  double lo[D], hi[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const long long last = i0[a] + ext[a] - 1 < g.n[a] - 1 ? i0[a] + ext[a] - 1 : g.n[a] - 1;
+    lo[a] = double(g.x0[a]) + (double(i0[a]) + 0.5) * double(g.d[a]);
+    hi[a] = double(g.x0[a]) + (double(last) + 0.5) * double(g.d[a]);
+  }
+  cc_op* ops = reinterpret_cast<cc_op*>(smem + L.ops_off);
+  const int m = prune_union<T, D>(t, tape.prunable, lo, hi, reinterpret_cast<double*>(smem + L.ls_off),
+                                  reinterpret_cast<double*>(smem + L.us_off), ops, count);
+  STape<T> u = t;
+  u.ops = ops;
+  u.n_ops = m;
+  return u;
+}
+
 template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const DevTape tape, const Cols cols,
                                                       T* normals, T* intercepts, uint8_t* valid) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_count;
   const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
   __syncthreads();
+  using P = PTile<D>;
   const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
-  const long long total = n0 * n1 * n2;
+  const long long tx = (n0 + P::X - 1) / P::X, ty = (n1 + P::Y - 1) / P::Y, tz = (n2 + P::Z - 1) / P::Z;
   T* vf = static_cast<T*>(cols.vf);
-  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
-    const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
-    const PlaneFit<T, D> pl = cell_plane<T, D, MX>(t, g, idx);
-    const T frac = T(1) - pl.fraction;
+  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
+    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+    const STape<T> u = tile_tape<T, D>(t, tape, g, i0, smem, &s_count);
+    const int q = threadIdx.x;
+    const long long idx[3] = {i0[0] + q % P::X, i0[1] + (q / P::X) % P::Y, i0[2] + q / (P::X * P::Y)};
+    if (idx[0] < n0 && idx[1] < n1 && idx[2] < n2) {
+      const long long ci = idx[0] + n0 * (idx[1] + n1 * idx[2]);
+      const PlaneFit<T, D> pl = cell_plane<T, D, MX>(u, g, idx);
+      const T frac = T(1) - pl.fraction;
 #pragma unroll
-    for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
-    intercepts[ci] = pl.a;
-    valid[ci] = pl.valid ? 1 : 0;
-    vf[ci] = frac;
-    cols.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+      for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
+      intercepts[ci] = pl.a;
+      valid[ci] = pl.valid ? 1 : 0;
+      vf[ci] = frac;
+      cols.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+    }
+    __syncthreads();  // the next tile's pruning overwrites the ops this one read
   }
 }
 
@@ -159,14 +210,20 @@ struct KSum {
 template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, const DevTape tape, double* partial) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_count;
   const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
   __syncthreads();
+  using P = PTile<D>;
   const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
-  const long long total = n0 * n1 * n2;
+  const long long tx = (n0 + P::X - 1) / P::X, ty = (n1 + P::Y - 1) / P::Y, tz = (n2 + P::Z - 1) / P::Z;
   KSum acc{0.0, 0.0};
-  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
-    const long long idx[3] = {ci % n0, (ci / n0) % n1, ci / (n0 * n1)};
-    acc.add(double(cell_plane<T, D, MX>(t, g, idx).fraction));
+  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
+    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+    const STape<T> u = tile_tape<T, D>(t, tape, g, i0, smem, &s_count);
+    const int q = threadIdx.x;
+    const long long idx[3] = {i0[0] + q % P::X, i0[1] + (q / P::X) % P::Y, i0[2] + q / (P::X * P::Y)};
+    if (idx[0] < n0 && idx[1] < n1 && idx[2] < n2) acc.add(double(cell_plane<T, D, MX>(u, g, idx).fraction));
+    __syncthreads();
   }
   __shared__ double ss[NT], sc[NT];
   ss[threadIdx.x] = acc.s;
@@ -255,15 +312,71 @@ int blocks_for(long long work, int per_sm) {
   return int(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+// Monte Carlo volume of {phi < 0} in the box lo..hi: point p's coordinates are three
+// successive splitmix64 outputs of (seed, 3p + a), 53 random bits each, mapped to [lo, hi);
+// the body is evaluated in Float64. Counts accumulate per thread, then per CTA, then into
+// out[0] with one atomic add per CTA.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(NT) monte_carlo_kernel(const DevTape tape, double lo0, double lo1, double lo2,
+                                                         double hi0, double hi1, double hi2, long long npts,
+                                                         unsigned long long seed, unsigned long long* out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const STape<double> t = load_tape<double>(tape.bytes, tape.n_ops, tape.n_params, smem);
+  __syncthreads();
+  const double lo[3] = {lo0, lo1, lo2}, span[3] = {hi0 - lo0, hi1 - lo1, hi2 - lo2};
+  unsigned long long inside = 0;
+  for (long long p = blockIdx.x * (long long)NT + threadIdx.x; p < npts; p += (long long)gridDim.x * NT) {
+    double x[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const unsigned long long r = splitmix64(seed ^ (unsigned long long)(3 * p + a));
+      x[a] = lo[a] + double(r >> 11) * 0x1.0p-53 * span[a];
+    }
+    inside += tape_eval<double, 3, double>(t, x) < 0.0 ? 1 : 0;
+  }
+  __shared__ unsigned long long part[NT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) inside += __shfl_xor_sync(0xffffffffu, inside, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x / 32] = inside;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int w = 0; w < NT / 32; ++w) s += part[w];
+    atomicAdd(out, s);
+  }
+}
+
 }  // namespace
 
 namespace cci {
+
+cudaError_t launch_monte_carlo(const DevTape& tape, const double lo[3], const double hi[3], long long npts,
+                               unsigned long long seed, unsigned long long* out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || npts <= 0) return e;
+  const int sm = ((tape.bytes_len + 15) / 16) * 16;
+  monte_carlo_kernel<<<blocks_for(npts, 16), NT, sm, s>>>(tape, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], npts, seed,
+                                                          out);
+  return cudaGetLastError();
+}
 
 template <class T, int D>
 cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals, T* intercepts,
                         uint8_t* valid, cudaStream_t s, bool mixed) {
   const long long total = g.n[0] * g.n[1] * (D == 3 ? g.n[2] : 1);
-  const int sm = ((tape.bytes_len + 15) / 16) * 16;
+  const int sm = CentroidSmem::of(tape).bytes;
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(plic_fit_kernel<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(plic_fit_kernel<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+  }
   if (mixed && sizeof(T) == 4) {
     plic_fit_kernel<T, D, true><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
     plic_face_kernel<T, D, true><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
@@ -279,7 +392,13 @@ int calc_volume_blocks() { return VOL_BLOCKS; }
 template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial, double* out,
                                cudaStream_t s, bool mixed) {
-  const int sm = ((tape.bytes_len + 15) / 16) * 16;
+  const int sm = CentroidSmem::of(tape).bytes;
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(calc_volume_kernel<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(calc_volume_kernel<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+  }
   if (mixed && sizeof(T) == 4) calc_volume_kernel<T, D, true><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
   else calc_volume_kernel<T, D, false><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
   calc_volume_final<<<1, 32, 0, s>>>(partial, VOL_BLOCKS, out);

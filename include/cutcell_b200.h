@@ -251,6 +251,14 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body,
 cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, double* out,
                          void* stream);
 
+/* Monte Carlo measure of {phi < 0} inside the box lo..hi (3D): n_points seeded points, point p's
+ * coordinates three successive splitmix64 outputs of (seed XOR (3p + axis)) as 53-bit fractions of
+ * the box; the body is evaluated in Float64. An independent check of calc_volume; no counterpart
+ * in the reference. Blocking; *inside counts the points inside, *volume (if not NULL) is
+ * inside / n_points times the box volume. */
+cc_status cc_monte_carlo_volume(cc_handle* h, const cc_optape* body, const double lo[3], const double hi[3],
+                                int64_t n_points, uint64_t seed, int64_t* inside, double* volume, void* stream);
+
 /* cut_cell_report (src/cut_cell.jl:302-319) over a cache's columns.
  * Blocking. counts = {n, cut, inside, outside, ambiguous}. */
 cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8_t* ambiguous,

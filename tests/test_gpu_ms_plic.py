@@ -98,3 +98,32 @@ def test_calc_volume_compensated():
         pd = float(T(g.d[0]) * T(g.d[1]) * T(g.d[2]))
         exact = math.fsum(frac.tolist()) * pd
         assert abs(v - exact) <= 1e-12 * abs(exact) + (1e-6 if prec == 0 else 0.0) * abs(exact)
+
+
+def _splitmix64(z):
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def test_monte_carlo_volume():
+    body = cc.workloads.sphere_cloud(0, 64)
+    n, seed = 200_000, 12345
+    vol, inside = cc.monte_carlo_volume(body, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), n, seed)
+    # the same points and the same union of spheres, restated in numpy
+    p = np.arange(n, dtype=np.uint64)
+    x = np.stack([(_splitmix64(np.uint64(seed) ^ (np.uint64(3) * p + np.uint64(a))) >> np.uint64(11)).astype(np.float64)
+                  * 2.0 ** -53 for a in range(3)], axis=1)
+    d = np.full(n, np.inf)
+    for s in body.children:
+        c = np.array(s.center)
+        dd = x - c
+        d = np.minimum(d, np.sqrt((dd[:, 0] * dd[:, 0] + dd[:, 1] * dd[:, 1]) + dd[:, 2] * dd[:, 2]) - s.radius)
+    assert inside == int((d < 0).sum())
+    assert vol == inside / n
+    # against calc_volume's plane reconstruction at 256^3, within the Monte Carlo error
+    big, _ = cc.monte_carlo_volume(body, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 10_000_000, 7)
+    cv = cc.calc_volume(body, cc.workloads.unit_grid(256))
+    sigma = math.sqrt(big * (1 - big) / 1e7)
+    assert abs(cv - big) < 4 * sigma + 2e-5
