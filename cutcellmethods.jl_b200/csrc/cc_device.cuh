@@ -496,6 +496,85 @@ __device__ int prune_union(const STape<T>& t, int mode, const double lo[D], cons
     us[i] = sqrt(dmax2) - r + margin;
   }
   __syncthreads();
+  if (n <= int(blockDim.x) && blockDim.x <= 1024) {
+    // one op per thread: block reductions and scans, then an order-preserving compaction
+    __shared__ double s_val[32];
+    __shared__ int s_idx[32];
+    __shared__ int s_cnt[32];
+    const int i = threadIdx.x, lane = i & 31, w = i >> 5, nw = (blockDim.x + 31) >> 5;
+    const double u = i < n ? us[i] : 1.0e300;
+    bool keep = false;
+    if (mode == 1) {
+      // the smallest upper bound, its op, and the smallest of the others
+      double v = u;
+      int vi = i;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
+        if (ov < v || (ov == v && oi < vi)) { v = ov; vi = oi; }
+      }
+      if (lane == 0) { s_val[w] = v; s_idx[w] = vi; }
+      __syncthreads();
+      double mn = s_val[0];
+      int jm = s_idx[0];
+      for (int q = 1; q < nw; ++q)
+        if (s_val[q] < mn || (s_val[q] == mn && s_idx[q] < jm)) { mn = s_val[q]; jm = s_idx[q]; }
+      __syncthreads();
+      double v2 = i == jm ? 1.0e300 : u;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
+        v2 = ov < v2 ? ov : v2;
+      }
+      if (lane == 0) s_val[w] = v2;
+      __syncthreads();
+      double mn2 = s_val[0];
+      for (int q = 1; q < nw; ++q) mn2 = s_val[q] < mn2 ? s_val[q] : mn2;
+      keep = i < n && !(ls[i] > (i == jm ? mn2 : mn));
+    } else {
+      // the exclusive prefix minimum of the upper bounds
+      double v = u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double ov = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = ov < v ? ov : v;
+      }
+      if (lane == 31) s_val[w] = v;
+      __syncthreads();
+      double before = 1.0e300;  // the minimum over the earlier warps
+      for (int q = 0; q < w; ++q) before = s_val[q] < before ? s_val[q] : before;
+      double up = __shfl_up_sync(0xffffffffu, v, 1);
+      if (lane == 0) up = 1.0e300;
+      const double prefix = up < before ? up : before;  // min over ops 0..i-1
+      if (i < n) {
+        if (i == 0) keep = true;
+        else {
+          const double k = t.p[t.ops[i].kparam];
+          const double kmargin = 16.0 * double(Eps<T>::v()) * (fabs(k) + fabs(prefix) + fabs(ls[i]) + 1.0);
+          keep = !(ls[i] >= prefix + k + kmargin);
+        }
+      }
+      __syncthreads();
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_cnt[w] = __popc(b);
+    __syncthreads();
+    int pos = __popc(b & ((1u << lane) - 1u));
+    int total = 0;
+    for (int q = 0; q < nw; ++q) {
+      if (q < w) pos += s_cnt[q];
+      total += s_cnt[q];
+    }
+    if (keep) {
+      cc_op op = t.ops[i];
+      if (pos == 0) op.combine = CC_COMB_PUSH;
+      out[pos] = op;
+    }
+    if (i == 0) *count = total;
+    __syncthreads();
+    return *count;
+  }
   if (threadIdx.x == 0) {
     int m = 0;
     if (mode == 1) {

@@ -160,38 +160,83 @@ __device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T
   }
 }
 
+// The resolved faces (src/plic/cache.jl:118-162) of one tile: every cell's one-sided areas
+// (_face_area, apertures.jl:73-125) computed once into shared memory, with the faces the
+// neighbouring cells outside the tile show it; each shared face is then resolved from its two
+// one-sided areas, (left / full + right / full) / 2, the same expression in the same order from
+// either side, so the face is single-valued bit for bit. Boundary faces are one-sided.
 template <class T, int D, bool MX>
 __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const Cols cols, const T* __restrict__ normals,
                                                        const T* __restrict__ intercepts, const uint8_t* __restrict__ valid) {
+  using P = PTile<D>;
+  constexpr int NF = 2 * D;
+  constexpr int EXT[3] = {P::X, P::Y, P::Z};
+  constexpr int E0 = P::Y * P::Z, E1 = P::X * P::Z, E2 = P::X * P::Y;  // halo face sizes per axis
+  constexpr int HB[3] = {0, 2 * E0, 2 * E0 + 2 * E1};                  // halo base per axis
+  constexpr int NH = D == 3 ? 2 * (E0 + E1 + E2) : 2 * (E0 + E1);
+  __shared__ T own[NT * NF];
+  __shared__ T halo[NH];
   const long long n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
-  const long long total = n[0] * n[1] * n[2];
   const T* vf = static_cast<const T*>(cols.vf);
   T* ff = static_cast<T*>(cols.ff);
   const T cs[3] = {g.d[0], g.d[1], D == 3 ? g.d[2] : T(1)};
-  for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
-    const long long idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+  const long long tx = (n[0] + P::X - 1) / P::X, ty = (n[1] + P::Y - 1) / P::Y, tz = (n[2] + P::Z - 1) / P::Z;
+  auto area = [&](long long cj, int k) {
+    return face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k);
+  };
+  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
+    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+    const int q = threadIdx.x;
+    const int lq[3] = {q % P::X, (q / P::X) % P::Y, q / (P::X * P::Y)};
+    const long long idx[3] = {i0[0] + lq[0], i0[1] + lq[1], i0[2] + lq[2]};
+    const bool in = idx[0] < n[0] && idx[1] < n[1] && idx[2] < n[2];
+    const long long ci = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+    if (in) {
 #pragma unroll
-    for (int k = 0; k < 2 * D; ++k) {
-      const int c = k >> 1;
-      const long long stride = c == 0 ? 1 : (c == 1 ? n[0] : n[0] * n[1]);
-      T full;
-      if constexpr (D == 2) full = cs[1 - c];
-      else full = (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
-      const T own = face_area<T, D, MX>(normals + D * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, k);
-      T r;
-      if ((k & 1) == 0) {
-        const bool has = idx[c] >= 1;
-        const long long cj = has ? ci - stride : ci;
-        const T below = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k + 1);
-        r = has ? (below / full + own / full) / T(2) : own / full;
-      } else {
-        const bool has = idx[c] <= n[c] - 2;
-        const long long cj = has ? ci + stride : ci;
-        const T above = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k - 1);
-        r = has ? (own / full + above / full) / T(2) : own / full;
-      }
-      ff[2 * D * ci + k] = r;
+      for (int k = 0; k < NF; ++k) own[q * NF + k] = area(ci, k);
     }
+    // the halo: for each axis and side, the cell beyond the tile shows its face toward the tile
+    for (int h = threadIdx.x; h < NH; h += NT) {
+      int ax = 0;
+      if (D == 3 && h >= HB[2]) ax = 2;
+      else if (h >= HB[1]) ax = 1;
+      const int E = ax == 0 ? E0 : (ax == 1 ? E1 : E2);
+      const int side = (h - HB[ax]) / E, pos = (h - HB[ax]) % E;
+      const int o1 = ax == 0 ? 1 : 0, o2 = ax == 2 ? 1 : 2;  // the other two axes, increasing
+      long long nb[3];
+      nb[ax] = side == 0 ? i0[ax] - 1 : i0[ax] + EXT[ax];
+      nb[o1] = i0[o1] + pos % EXT[o1];
+      nb[o2] = i0[o2] + pos / EXT[o1];
+      if (nb[ax] >= 0 && nb[ax] < n[ax] && nb[o1] < n[o1] && nb[o2] < n[o2])
+        halo[h] = area(nb[0] + n[0] * (nb[1] + n[1] * nb[2]), side == 0 ? 2 * ax + 1 : 2 * ax);
+    }
+    __syncthreads();
+    if (in) {
+#pragma unroll
+      for (int k = 0; k < NF; ++k) {
+        const int c = k >> 1;
+        const int o1 = c == 0 ? 1 : 0, o2 = c == 2 ? 1 : 2;
+        T full;
+        if constexpr (D == 2) full = cs[1 - c];
+        else full = (T(1) * cs[o1]) * cs[o2];
+        const int lstride = c == 0 ? 1 : (c == 1 ? P::X : P::X * P::Y);
+        const int hpos = lq[o1] + EXT[o1] * (D == 3 ? lq[o2] : 0);
+        const T mine = own[q * NF + k];
+        T r;
+        if ((k & 1) == 0) {
+          const bool has = idx[c] >= 1;
+          const T below = lq[c] > 0 ? own[(q - lstride) * NF + k + 1] : halo[HB[c] + hpos];
+          r = has ? (below / full + mine / full) / T(2) : mine / full;
+        } else {
+          const bool has = idx[c] <= n[c] - 2;
+          const int Ec = c == 0 ? E0 : (c == 1 ? E1 : E2);
+          const T above = lq[c] < EXT[c] - 1 ? own[(q + lstride) * NF + k - 1] : halo[HB[c] + Ec + hpos];
+          r = has ? (mine / full + above / full) / T(2) : mine / full;
+        }
+        ff[2 * D * ci + k] = r;
+      }
+    }
+    __syncthreads();  // the next tile reuses own and halo
   }
 }
 
