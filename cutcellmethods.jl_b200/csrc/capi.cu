@@ -242,6 +242,19 @@ bool isotropic(const cc_grid* g) {
 
 namespace cci {
 cc_status validate_body(const cc_optape* t, int dim) { return validate_tape(t, dim); }
+
+void* prune_scratch(cc_handle* h, size_t bytes) {
+  if (bytes <= h->prune_bytes) return h->prune;
+  if (h->prune) cudaFree(h->prune);
+  h->prune = nullptr;
+  h->prune_bytes = 0;
+  if (cudaMalloc(&h->prune, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  h->prune_bytes = bytes;
+  return h->prune;
+}
 cc_status upload_body_f64(cc_handle* h, const cc_optape* t, int dim, cudaStream_t s, DevTape* out) {
   return upload_tape<double>(h, t, dim, s, out);
 }
@@ -309,6 +322,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->cut_count) cudaFree(h->cut_count);
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
   if (h->mesh_scan) cudaFree(h->mesh_scan);
+  if (h->prune) cudaFree(h->prune);
   delete h;
   return CC_OK;
 }
@@ -377,13 +391,18 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   cudaError_t e;
   if (h->prec == CC_F64) {
     if (body && (st = upload_tape<double>(h, body, 3, s, &tape)) != CC_OK) return st;
+    const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
+    void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dev_grid<double>(g), tape, static_cast<const double*>(phi_in),
-                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s);
+                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s,
+                               true, false, ps, ps ? pb : 0);
   } else {
     if (body && (st = upload_tape<float>(h, body, 3, s, &tape)) != CC_OK) return st;
+    const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
+    void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
                               static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s, true,
-                              h->prec == CC_MIXED);
+                              h->prec == CC_MIXED, ps, ps ? pb : 0);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching cubes launch");
   return CC_OK;

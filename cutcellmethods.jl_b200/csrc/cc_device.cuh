@@ -604,6 +604,20 @@ __device__ int prune_union(const STape<T>& t, int mode, const double lo[D], cons
   return *count;
 }
 
+// Shared-memory places of prune_union's output and scratch, after a tape loaded at `base`.
+struct PruneSmem {
+  int ops, ls, us, end;
+  template <class DT>
+  __host__ __device__ static PruneSmem of(const DT& tape, int base) {
+    PruneSmem p;
+    p.ops = base + ((tape.bytes_len + 15) / 16) * 16;
+    p.ls = p.ops + ((tape.n_ops * int(sizeof(cc_op)) + 15) / 16) * 16;
+    p.us = p.ls + tape.n_ops * 8;
+    p.end = p.us + tape.n_ops * 8;
+    return p;
+  }
+};
+
 // ---------------------------------------------------------------------------------------------
 // CartesianMeshes stand-ins: node and centroid coordinates, the plane-cube clip.
 template <class T> __device__ __forceinline__ T node_coord(T x0, T d, long long i) { return x0 + T(i) * d; }

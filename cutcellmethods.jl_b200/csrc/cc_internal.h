@@ -52,7 +52,12 @@ struct Cols {
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s, bool with_cut = true, bool mixed = false);
+                      cudaStream_t s, bool with_cut = true, bool mixed = false, void* prune_scratch = nullptr,
+                      size_t prune_bytes = 0);
+// Scratch launch_mc needs to prune a union-of-spheres tape per fill CTA (n_ops ops per CTA).
+size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool f64);
+// The handle's pruning scratch, grown to at least `bytes` (null on failure).
+void* prune_scratch(cc_handle* h, size_t bytes);
 
 // The learned correction (learned.cu).
 int mlp_nparam();
@@ -135,5 +140,7 @@ struct cc_handle {
   size_t mesh_vbase_n = 0;
   unsigned long long* mesh_scan = nullptr;  // generate_mesh: per-block counts and offsets
   size_t mesh_scan_n = 0;
+  void* prune = nullptr;  // marching cubes: per fill CTA pruned op lists of a union of spheres
+  size_t prune_bytes = 0;
 };
 

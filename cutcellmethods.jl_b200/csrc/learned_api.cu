@@ -296,8 +296,10 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     cci::DevTape tape{nullptr, 0, 0, 0};
     if ((st = cci::upload_body_f64(h, body, 3, s, &tape)) != CC_OK) return st;
     const cci::DevGrid<double> dg2 = grid_of<double>(g);
+    const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
+    void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dg2, tape, nullptr, static_cast<double*>(phi), cols_of(cells), h->tb, h->cut_list,
-                               h->cut_count, s, false);
+                               h->cut_count, s, false, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<double>(dg2, static_cast<const double*>(phi), cols_of(cells), h->tb, h->cut_list,
                                              h->cut_count, m->P, bound, m->fallback, m->err, s);
@@ -305,8 +307,10 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     cci::DevTape tape{nullptr, 0, 0, 0};
     if ((st = cci::upload_body_f32(h, body, 3, s, &tape)) != CC_OK) return st;
     const cci::DevGrid<float> dg2 = grid_of<float>(g);
+    const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
+    void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dg2, tape, nullptr, static_cast<float*>(phi), cols_of(cells), h->tb, h->cut_list,
-                              h->cut_count, s, false);
+                              h->cut_count, s, false, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<float>(dg2, static_cast<const float*>(phi), cols_of(cells), h->tb, h->cut_list,
                                             h->cut_count, m->P, bound, m->fallback, m->err, s);

@@ -58,6 +58,9 @@ struct McArgs {
   unsigned* cut_count;
   int n_itiles, n_jtiles;
   int use_tma;  // output columns leave through TMA tensor stores (maps below are valid)
+  // a union of spheres: each CTA's kept ops (stride tape.n_ops) and their count, or null
+  const cc_op* pruned_ops;
+  const int* pruned_count;
 };
 
 // One TMA tensor map per output column: kind, ambiguous, volume_fraction (n0 x n1 x n2), centroid
@@ -136,7 +139,38 @@ __device__ __forceinline__ Stage<T> stage_at(unsigned char* base) {
   return st;
 }
 
-template <class T, bool SAMPLE>
+// For a union of spheres: each fill CTA's pencil (cells i0.., j0.., k0..k1) gets the tape pruned to
+// the box of its nodes (prune_union), written to out[cta * n_ops ..] with its count.
+template <class T>
+__global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, cc_op* __restrict__ out,
+                                                            int* __restrict__ count) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_count;
+  using TL = Tile<T>;
+  const STape<T> t = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem);
+  __syncthreads();
+  const PruneSmem ps = PruneSmem::of(A.tape, 0);
+  int b = blockIdx.x;
+  const int it = b % A.n_itiles; b /= A.n_itiles;
+  const int jt = b % A.n_jtiles; b /= A.n_jtiles;
+  const long long n0 = A.g.n[0], n1 = A.g.n[1], n2 = A.g.n[2];
+  const long long i0 = (long long)it * TL::TX, j0 = (long long)jt * TL::TY, k0 = (long long)b * KZ;
+  const long long i1 = i0 + TL::TX < n0 ? i0 + TL::TX : n0, j1 = j0 + TL::TY < n1 ? j0 + TL::TY : n1;
+  const long long k1 = k0 + KZ < n2 ? k0 + KZ : n2;
+  const double lo[3] = {double(A.g.x0[0]) + double(i0) * double(A.g.d[0]),
+                        double(A.g.x0[1]) + double(j0) * double(A.g.d[1]),
+                        double(A.g.x0[2]) + double(k0) * double(A.g.d[2])};
+  const double hi[3] = {double(A.g.x0[0]) + double(i1) * double(A.g.d[0]),
+                        double(A.g.x0[1]) + double(j1) * double(A.g.d[1]),
+                        double(A.g.x0[2]) + double(k1) * double(A.g.d[2])};
+  cc_op* kept = reinterpret_cast<cc_op*>(smem + ps.ops);
+  const int m = prune_union<T, 3>(t, A.tape.prunable, lo, hi, reinterpret_cast<double*>(smem + ps.ls),
+                                  reinterpret_cast<double*>(smem + ps.us), kept, &s_count);
+  for (int q = threadIdx.x; q < m; q += blockDim.x) out[(long long)blockIdx.x * A.tape.n_ops + q] = kept[q];
+  if (threadIdx.x == 0) count[blockIdx.x] = m;
+}
+
+template <class T, bool SAMPLE, bool PRUNED>
 __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
                                                                             const __grid_constant__ ColumnMaps maps) {
   using TL = Tile<T>;
@@ -155,7 +189,16 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
   const long long k1 = (k0 + KZ < n2) ? k0 + KZ : n2;
 
   STape<T> tape;
-  if (SAMPLE) tape = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem + L::tape);
+  if (SAMPLE) {
+    tape = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem + L::tape);
+    if (PRUNED) {  // this pencil's kept ops over the loaded ones (same places, fewer)
+      const int m = A.pruned_count[blockIdx.x];
+      cc_op* ops = reinterpret_cast<cc_op*>(smem + L::tape);
+      __syncthreads();
+      for (int q = tid; q < m; q += NT) ops[q] = A.pruned_ops[(long long)blockIdx.x * A.tape.n_ops + q];
+      tape.n_ops = m;
+    }
+  }
   T* const ring = reinterpret_cast<T*>(smem + L::slab0);
   constexpr int RS = L::slab_bytes / int(sizeof(T));  // ring slot stride, elements
   if (SAMPLE) __syncthreads();
@@ -425,10 +468,16 @@ bool make_column_maps(const DevGrid<T>& g, const Cols& cols, ColumnMaps* maps) {
 
 namespace cci {
 
+size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool f64) {
+  const long long tx = f64 ? Tile<double>::TX : Tile<float>::TX, ty = Tile<float>::TY;
+  const long long blocks = ((n0 + tx - 1) / tx) * ((n1 + ty - 1) / ty) * ((n2 + KZ - 1) / KZ);
+  return size_t(((blocks * 4 + 15) / 16) * 16 + blocks * (long long)n_ops * (long long)sizeof(cc_op));
+}
+
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s, bool with_cut, bool mixed) {
+                      cudaStream_t s, bool with_cut, bool mixed, void* prune_scratch, size_t prune_bytes) {
   using TL = Tile<T>;
   McArgs<T> a;
   a.g = g;
@@ -450,20 +499,40 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   cudaError_t e = cudaMemsetAsync(cut_count, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   const bool sample = phi_in == nullptr;
+  a.pruned_ops = nullptr;
+  a.pruned_count = nullptr;
+  if (sample && tape.prunable && prune_scratch && prune_bytes >= mc_prune_bytes(g.n[0], g.n[1], g.n[2], tape.n_ops, sizeof(T) == 8)) {
+    int* cnt = static_cast<int*>(prune_scratch);
+    cc_op* ops = reinterpret_cast<cc_op*>(static_cast<unsigned char*>(prune_scratch) + ((blocks * 4 + 15) / 16) * 16);
+    const int psm = PruneSmem::of(tape, 0).end;
+    if (psm > 48 * 1024) {
+      e = cudaFuncSetAttribute(prune_pencils_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
+      if (e != cudaSuccess) return e;
+    }
+    prune_pencils_kernel<T><<<unsigned(blocks), 256, psm, s>>>(a, ops, cnt);
+    a.pruned_ops = ops;
+    a.pruned_count = cnt;
+  }
   const int sm = smem_bytes<T>(sample ? tape.bytes_len : 0);
   const int cut_blocks = 148 * 8;
   // the FP64 islands of mixed precision exist for Float32 caches only
   const bool mx = mixed && sizeof(T) == 4;
-  if (sample) {
-    e = cudaFuncSetAttribute(mc_fill_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (sample && a.pruned_ops) {
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
-    mc_fill_kernel<T, true><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    mc_fill_kernel<T, true, true><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    if (with_cut && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+  } else if (sample) {
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_fill_kernel<T, true, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
     if (with_cut && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
     else if (with_cut) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
   } else {
-    e = cudaFuncSetAttribute(mc_fill_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
-    mc_fill_kernel<T, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    mc_fill_kernel<T, false, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
     if (with_cut && mx) mc_cut_kernel<T, false, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
     else if (with_cut) mc_cut_kernel<T, false, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
   }
@@ -471,8 +540,10 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
 }
 
 template cudaError_t launch_mc<float>(const DevGrid<float>&, const DevTape&, const float*, float*,
-                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool);
+                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool,
+                                      void*, size_t);
 template cudaError_t launch_mc<double>(const DevGrid<double>&, const DevTape&, const double*, double*,
-                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool);
+                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool,
+                                       void*, size_t);
 
 }  // namespace cci
