@@ -79,6 +79,9 @@ EXPORTS = {
                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_mc_mesh_cell_indices": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                 C.c_void_p],
+    "cc_ms_mesh_grid": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_ms_mesh_tree": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cc_ms_mesh_fetch": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_batch_create": [C.c_int32, C.c_int32, C.c_void_p],
     "cc_batch_destroy": [C.c_void_p],
     "cc_batch_add_ms_grid": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],

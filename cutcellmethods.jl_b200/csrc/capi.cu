@@ -323,6 +323,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
   if (h->mesh_scan) cudaFree(h->mesh_scan);
   if (h->prune) cudaFree(h->prune);
+  cci::free_ms_mesh(h);
   delete h;
   return CC_OK;
 }

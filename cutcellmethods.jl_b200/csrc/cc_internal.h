@@ -106,6 +106,9 @@ size_t pack_tape(const cc_optape* t, int dim, unsigned char* out, int* n_params)
 size_t tape_pack_capacity();
 int tape_prunable(const cc_optape* t);
 
+// Release the contour a marching-squares handle holds (ms_mesh.cu).
+void free_ms_mesh(cc_handle* h);
+
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);
 
@@ -142,5 +145,6 @@ struct cc_handle {
   size_t mesh_scan_n = 0;
   void* prune = nullptr;  // marching cubes: per fill CTA pruned op lists of a union of spheres
   size_t prune_bytes = 0;
+  void* ms_mesh = nullptr;  // marching squares: the last contour built (ms_mesh.cu)
 };
 

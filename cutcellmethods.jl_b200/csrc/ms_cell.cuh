@@ -130,4 +130,50 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
   else { ic[2 * ci] = ce0; ic[2 * ci + 1] = ce1; }
 }
 
+// cell_interface (src/marching_squares/marching_squares.jl:343-351): the cell's n <= 2 contour
+// segments, the s-th from a[s] to b[s], oriented out of the body -- the walk of
+// cell_boundary_walk and the gaps of cell_gap_segments exactly as ms_cell builds them, endpoints
+// swapped.
+template <class T, bool MX>
+__device__ __forceinline__ int ms_interface(const T nd[4][2], const T ph[4], T a[2][2], T b[2][2]) {
+  T sa[4][2], sb[4][2];
+  bool pr[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int k1 = (k + 1) & 3;
+    const T fa = ph[k], fb = ph[k1];
+    const T fr = open_fraction<T, MX>(fa, fb);
+    pr[k] = fa >= T(0) || fb >= T(0);
+    if (fa >= T(0) && fb >= T(0)) {
+      sa[k][0] = nd[k][0]; sa[k][1] = nd[k][1]; sb[k][0] = nd[k1][0]; sb[k][1] = nd[k1][1];
+    } else if (fa >= T(0)) {
+      sa[k][0] = nd[k][0]; sa[k][1] = nd[k][1];
+      sb[k][0] = nd[k][0] + fr * (nd[k1][0] - nd[k][0]);
+      sb[k][1] = nd[k][1] + fr * (nd[k1][1] - nd[k][1]);
+    } else {
+      sa[k][0] = nd[k1][0] + fr * (nd[k][0] - nd[k1][0]);
+      sa[k][1] = nd[k1][1] + fr * (nd[k][1] - nd[k1][1]);
+      sb[k][0] = nd[k1][0]; sb[k][1] = nd[k1][1];
+    }
+  }
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!pr[k]) continue;
+    int j = (k + 1) & 3;
+    if (!pr[j]) { j = (j + 1) & 3; if (!pr[j]) { j = (j + 1) & 3; if (!pr[j]) j = k; } }
+    const T a0 = sb[k][0], a1 = sb[k][1];
+    const T b0 = j == 0 ? sa[0][0] : j == 1 ? sa[1][0] : j == 2 ? sa[2][0] : sa[3][0];
+    const T b1 = j == 0 ? sa[0][1] : j == 1 ? sa[1][1] : j == 2 ? sa[2][1] : sa[3][1];
+    if (a0 != b0 || a1 != b1) {
+      if (n < 2) {  // the public orientation: from the gap's end to its start
+        a[n][0] = b0; a[n][1] = b1;
+        b[n][0] = a0; b[n][1] = a1;
+      }
+      ++n;
+    }
+  }
+  return n < 2 ? n : 2;
+}
+
 }  // namespace ccms

@@ -284,6 +284,21 @@ cc_status cc_mc_mesh(cc_handle* h, const cc_grid* g, const void* phi, void* vert
 cc_status cc_mc_mesh_cell_indices(cc_handle* h, const cc_grid* g, const void* vertices, const int32_t* triangles,
                                   int64_t n_triangles, int64_t* cells, void* stream);
 
+/* generate_mesh for a marching-squares cache (src/marching_squares/surface.jl:70-111), on the device:
+ * the contour of the cache's phi -- a grid's nodal block, or a tree's per-leaf corners -- as the
+ * cells' cell_interface segments (oriented out of the body) in cell (leaf) order, vertices welded
+ * by exact coordinate equality and numbered by first occurrence (segment order, start before end),
+ * the numbering of the reference's serial weld. The contour is built into the handle (blocking);
+ * *n_vertices and *n_segments receive its size. cc_ms_mesh_fetch then copies it out: vertices
+ * T[n_vertices][2], segments int32[n_segments][2] (0-based), cells int64[n_segments] (each
+ * segment's cell or leaf; any pointer may be NULL). No device fault on any input: every hash probe
+ * is bounded. */
+cc_status cc_ms_mesh_grid(cc_handle* h, const cc_grid* g, const void* phi, int64_t* n_vertices, int64_t* n_segments,
+                          void* stream);
+cc_status cc_ms_mesh_tree(cc_handle* h, const cc_tree* t, const void* phi4, int64_t* n_vertices, int64_t* n_segments,
+                          void* stream);
+cc_status cc_ms_mesh_fetch(cc_handle* h, void* vertices, int32_t* segments, int64_t* cells, void* stream);
+
 /* ---- batched marching squares -----------------------------------------------------------
  * Many MarchingSquaresCutCell updates (update_cache! on a CartesianGrid,
  * src/marching_squares/cache.jl:49-78, or on an AdaptiveMesh{2}'s leaves, :115-137), each with

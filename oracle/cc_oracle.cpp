@@ -29,6 +29,8 @@
 #include <cstring>
 #include <limits>
 #include <vector>
+#include <map>
+#include <utility>
 #include <algorithm>
 #include <thread>
 #include <atomic>
@@ -1050,6 +1052,79 @@ void ms_cells(const cc_grid& g, const T* phi, const cc_cells& c) {
   });
 }
 
+// generate_mesh for marching squares (src/marching_squares/surface.jl:70-111, 153-176): cut cells in
+// order, each cell_interface segment (the gaps, endpoints swapped: out of the body) appended with
+// its vertices welded by exact coordinate equality in a map, numbered by first occurrence.
+template <class T>
+struct Contour {
+  std::vector<T> verts;
+  std::vector<int32_t> segs;
+  std::vector<int64_t> cells;
+  std::map<std::pair<T, T>, int32_t> ids;
+  int32_t vertex(const T* x) {
+    const std::pair<T, T> key(x[0] + T(0), x[1] + T(0));
+    auto it = ids.find(key);
+    if (it != ids.end()) return it->second;
+    const int32_t id = int32_t(verts.size() / 2);
+    ids.emplace(key, id);
+    verts.push_back(key.first);
+    verts.push_back(key.second);
+    return id;
+  }
+  void add_cell(const T nodes[4][2], const T ph[4], int64_t cell) {
+    Walk<T> w;
+    boundary_walk(nodes, ph, w);
+    T ia[2][2], ib[2][2];
+    const int n = gap_segments(w, ia, ib);
+    for (int s = 0; s < n; ++s) {  // cell_interface: (n, b, a)
+      const int32_t i1 = vertex(ib[s]);
+      const int32_t i2 = vertex(ia[s]);
+      segs.push_back(i1);
+      segs.push_back(i2);
+      cells.push_back(cell);
+    }
+  }
+};
+
+template <class T>
+Contour<T> ms_mesh_grid(const cc_grid& g, const T* phi) {
+  const int64_t n0 = g.n[0], n1 = g.n[1], nx = n0 + 1;
+  const T x0[2] = {T(g.x0[0]), T(g.x0[1])};
+  const T d[2] = {T(g.d[0]), T(g.d[1])};
+  Contour<T> c;
+  for (int64_t j = 0; j < n1; ++j)
+    for (int64_t i = 0; i < n0; ++i) {
+      T nodes[4][2], ph[4];
+      for (int q = 0; q < 4; ++q) {
+        const int64_t ii = i + MS_BITS[q][0], jj = j + MS_BITS[q][1];
+        nodes[q][0] = node_coord(x0[0], d[0], ii);
+        nodes[q][1] = node_coord(x0[1], d[1], jj);
+        ph[q] = phi[ii + nx * jj];
+      }
+      c.add_cell(nodes, ph, i + n0 * j);
+    }
+  return c;
+}
+
+template <class T>
+Contour<T> ms_mesh_tree(const double* x0d, const double* based, int64_t nl, const int32_t* level,
+                        const int32_t* coord, const T* phi4) {
+  const T x0[2] = {T(x0d[0]), T(x0d[1])};
+  Contour<T> c;
+  for (int64_t i = 0; i < nl; ++i) {
+    const T scale = T(std::ldexp(1.0, -level[i]));
+    const T h[2] = {T(based[0]) * scale, T(based[1]) * scale};
+    T nodes[4][2], ph[4];
+    for (int q = 0; q < 4; ++q) {
+      nodes[q][0] = x0[0] + T(int64_t(coord[2 * i]) + MS_BITS[q][0]) * h[0];
+      nodes[q][1] = x0[1] + T(int64_t(coord[2 * i + 1]) + MS_BITS[q][1]) * h[1];
+      ph[q] = phi4[4 * i + q];
+    }
+    c.add_cell(nodes, ph, i);
+  }
+  return c;
+}
+
 // _leaf_cells_kernel!, src/marching_squares/cache.jl:129-137
 template <class T>
 void ms_tree(const double* x0d, const double* based, int64_t nl, const int32_t* level,
@@ -1256,6 +1331,28 @@ int oc_mc_mesh(int prec, const cc_grid* g, const uint8_t* table, const void* phi
   };
   if (prec == 1) return run(oc::mc_mesh<double>(*g, tb, (const double*)phi));
   return run(oc::mc_mesh<float>(*g, tb, (const float*)phi));
+}
+
+// generate_mesh for marching squares: a grid (tree == 0) or leaves (tree != 0, then x0, base_d,
+// nl, level, coord describe them). Counts into *nv / *ns; arrays written when non-null.
+int oc_ms_mesh(int prec, int tree, const cc_grid* g, const double* x0, const double* based, int64_t nl,
+               const int32_t* level, const int32_t* coord, const void* phi, void* verts, int32_t* segs,
+               int64_t* cells, int64_t* nv, int64_t* ns) {
+  oc::MixedScope mixed(prec == 2);
+  auto out = [&](auto c) {
+    using TT = typename std::decay<decltype(c.verts[0])>::type;
+    *nv = int64_t(c.verts.size() / 2);
+    *ns = int64_t(c.cells.size());
+    if (verts) std::memcpy(verts, c.verts.data(), c.verts.size() * sizeof(TT));
+    if (segs) std::memcpy(segs, c.segs.data(), c.segs.size() * sizeof(int32_t));
+    if (cells) std::memcpy(cells, c.cells.data(), c.cells.size() * sizeof(int64_t));
+    return 0;
+  };
+  if (prec == 1)
+    return tree ? out(oc::ms_mesh_tree<double>(x0, based, nl, level, coord, (const double*)phi))
+                : out(oc::ms_mesh_grid<double>(*g, (const double*)phi));
+  return tree ? out(oc::ms_mesh_tree<float>(x0, based, nl, level, coord, (const float*)phi))
+              : out(oc::ms_mesh_grid<float>(*g, (const float*)phi));
 }
 
 int oc_ms_cells_from_phi(int prec, const cc_grid* g, const void* phi, const cc_cells* c) {

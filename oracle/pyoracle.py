@@ -57,6 +57,8 @@ def lib():
         L.oc_eval_tape.restype = C.c_double
         L.oc_ms_tree_update.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_ms_mesh.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_mc_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -151,6 +153,29 @@ def mc_mesh(g, phi, table: bytes, prec):
                           C.byref(nv), C.byref(nt))
     assert rc == 0
     return v, t, c
+
+
+def ms_mesh(domain, phi, prec):
+    """The marching-squares contour of phi over a grid (nodal phi) or a quadtree (phi [n, 4]):
+    (vertices [nv, 2], segments [ns, 2] int32, cell of each segment [ns] int64)."""
+    phi = np.ascontiguousarray(phi, dtype_of(prec))
+    nv, ns = C.c_int64(0), C.c_int64(0)
+    tree = hasattr(domain, "level")
+    if tree:
+        x0 = np.array(domain.x0, np.float64)
+        bd = np.array(domain.base_d, np.float64)
+        args = (None, _ptr(x0), _ptr(bd), domain.nleaves, _ptr(domain.level), _ptr(domain.coord))
+    else:
+        gs = grid_struct(domain)
+        args = (C.byref(gs), None, None, 0, None, None)
+    rc = lib().oc_ms_mesh(prec, int(tree), *args, _ptr(phi), None, None, None, C.byref(nv), C.byref(ns))
+    assert rc == 0
+    v = np.zeros((nv.value, 2), dtype_of(prec))
+    sg = np.zeros((ns.value, 2), np.int32)
+    c = np.zeros(ns.value, np.int64)
+    rc = lib().oc_ms_mesh(prec, int(tree), *args, _ptr(phi), _ptr(v), _ptr(sg), _ptr(c), C.byref(nv), C.byref(ns))
+    assert rc == 0
+    return v, sg, c
 
 
 def mc_update(g, tape, table: bytes, prec):

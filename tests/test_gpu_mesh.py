@@ -64,3 +64,49 @@ def test_mesh_edge_cases():
     assert m.nodes.shape[0] == 0 and m.elements.shape[0] == 0
     with pytest.raises(cc.DimensionMismatch):
         S.generate_mesh(empty, cc.grid3(17))
+
+
+DT2 = {0: torch.float32, 1: torch.float64, 2: torch.float32}
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_ms_contour_bitwise(prec):
+    pr = "mixed" if prec == 2 else "plain"
+    for g, body in ((cc.CartesianIsoGrid((-1.0, -1.0), (1.0, 1.0), 0.01), cc.Circle((0.0, 0.0), 0.5)),
+                    (cc.CartesianGrid((-1.3, 0.7), (37, 53), (0.09, 0.061)),
+                     cc.Union(cc.Circle((-0.1, 2.2), 1.1), cc.Box((0.5, 1.5), (0.3, 0.2))))):
+        cache = cc.update_cache(cc.allocate_cache(g, cc.MarchingSquaresCutCell(), dtype=DT2[prec], precision=pr),
+                                cc.flatten(body, 2), g)
+        m = S.generate_mesh(cache, g)
+        v, sg, c = po.ms_mesh(g, cache.phi.cpu().numpy(), prec)
+        assert m.nodes.shape[0] == v.shape[0] > 0 and m.elements.shape[0] == sg.shape[0]
+        assert np.array_equal(bits(m.nodes.cpu().numpy()), bits(v))
+        assert np.array_equal(m.elements.cpu().numpy(), sg)
+        assert np.array_equal(m.cells.cpu().numpy(), c)
+    # the tree: one segment per cut leaf on a uniformly refined band
+    tree, _, _ = cc.star_curve_tree(3, 4, 9)
+    tc = cc.allocate_cache(tree, cc.MarchingSquaresCutCell(), dtype=DT2[prec], precision=pr)
+    cc.update_cache(tc, cc.flatten(cc.Circle((0.013, -0.021), 0.53), 2), tree)
+    m = S.generate_mesh(tc, tree)
+    v, sg, c = po.ms_mesh(tree, tc.phi.cpu().numpy(), prec)
+    assert np.array_equal(bits(m.nodes.cpu().numpy()), bits(v))
+    assert np.array_equal(m.elements.cpu().numpy(), sg)
+    assert np.array_equal(m.cells.cpu().numpy(), c)
+    assert sg.shape[0] == int((tc.cells.kind == 2).sum().item())
+
+
+def test_ms_contour_length_and_orientation():
+    # test/test_moments.jl:456-463: the circle's contour length is 2 pi r to rtol 1e-3
+    g = cc.CartesianIsoGrid((-1.0, -1.0), (1.0, 1.0), 0.01)
+    cache = cc.update_cache(cc.allocate_cache(g, cc.MarchingSquaresCutCell()), cc.Circle((0.0, 0.0), 0.5), g)
+    m = S.generate_mesh(cache, g)
+    v, e = m.nodes.cpu().numpy(), m.elements.cpu().numpy()
+    d = v[e[:, 1]] - v[e[:, 0]]
+    assert abs(np.linalg.norm(d, axis=1).sum() / (2 * np.pi * 0.5) - 1) < 1e-3
+    mid = 0.5 * (v[e[:, 1]] + v[e[:, 0]])
+    assert np.all(d[:, 1] * mid[:, 0] - d[:, 0] * mid[:, 1] > 0)   # (v2, -v1) points out of the body
+    assert np.all(np.abs(np.linalg.norm(v, axis=1) - 0.5) < 2e-3)
+    # closed: every vertex starts one segment and ends one
+    assert np.array_equal(np.sort(e[:, 0]), np.arange(v.shape[0])) and np.array_equal(np.sort(e[:, 1]), np.arange(v.shape[0]))
+    with pytest.raises(cc.DimensionMismatch):
+        S.generate_mesh(cache, cc.CartesianIsoGrid((-1.0, -1.0), (1.01, 1.0), 0.01))
