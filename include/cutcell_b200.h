@@ -299,6 +299,38 @@ cc_status cc_ms_mesh_tree(cc_handle* h, const cc_tree* t, const void* phi4, int6
                           void* stream);
 cc_status cc_ms_mesh_fetch(cc_handle* h, void* vertices, int32_t* segments, int64_t* cells, void* stream);
 
+/* extract_surface_plic (src/plic/surface.jl:48-97 in 2D, :119-185 in 3D), on the device: the
+ * planes n . xi = a of n_entries cells (in each cell's unit frame, as a PLIC cache stores them)
+ * clipped to their cells. 3D: the polygon of the plane's crossings with the cube's edges (a corner
+ * on the plane taken once), ordered by angle about its centroid in the plane's basis
+ * (surface.jl:239-267) and fanned from its first vertex; a fan triangle with
+ * |cross|^2 < (2 min_tri_area_fraction min(d)^2)^2 is dropped, a polygon of fewer than 3 points
+ * draws nothing. 2D: one segment per entry, dropped when shorter than
+ * min_tri_area_fraction * min(d); an entry whose line does not cross its cell draws a zero-length
+ * segment. Entries contribute in order, and no node is shared between entries.
+ *   prec        CC_F32 / CC_MIXED (float planes and output) or CC_F64 (double).
+ *   normals     T[n_entries][D], intercepts T[n_entries], is_valid uint8[n_entries] or NULL (NULL:
+ *               a zero normal marks a degenerate fit, which draws nothing in 3D and a zero-length
+ *               segment in 2D).
+ *   cell_index  int64[n_entries], the linear (x-fastest, 0-based) cell of each entry; NULL means
+ *               every cell of g in order (n_entries is then ignored).
+ * Output: nodes T[n_nodes][D], elements int32[n_elements][D] (0-based: triangles in 3D, segments
+ * in 2D), element_cells int64[n_elements] (the cell each element was drawn for). Call with
+ * nodes = elements = NULL to count, then with arrays of at least the counted sizes. Blocking. */
+cc_status cc_plic_surface(int prec, const cc_grid* g, const void* normals, const void* intercepts,
+                          const uint8_t* is_valid, const int64_t* cell_index, int64_t n_entries,
+                          double min_tri_area_fraction, void* nodes, int64_t node_capacity, int32_t* elements,
+                          int64_t element_capacity, int64_t* element_cells, int64_t* n_nodes, int64_t* n_elements,
+                          void* stream);
+
+/* generate_mesh for a PLIC cache (src/plic/surface.jl:28-37): cc_plic_surface over every cell of the
+ * cache's grid, from the cache's own normals / intercepts / is_valid (the grid is checked against
+ * the cache's size). */
+cc_status cc_plic_mesh(cc_handle* h, const cc_grid* g, const void* normals, const void* intercepts,
+                       const uint8_t* is_valid, double min_tri_area_fraction, void* nodes, int64_t node_capacity,
+                       int32_t* elements, int64_t element_capacity, int64_t* element_cells, int64_t* n_nodes,
+                       int64_t* n_elements, void* stream);
+
 /* ---- batched marching squares -----------------------------------------------------------
  * Many MarchingSquaresCutCell updates (update_cache! on a CartesianGrid,
  * src/marching_squares/cache.jl:49-78, or on an AdaptiveMesh{2}'s leaves, :115-137), each with

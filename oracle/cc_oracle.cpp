@@ -1273,6 +1273,163 @@ T calc_volume(const cc_grid& g, const Tape<T>& tp) {
   return vol * pd;
 }
 
+// ---- generate_mesh for a PLIC cache (src/plic/surface.jl:28-267), serially ----
+// CartesianMeshes 0.2.3 `cell_plane_clip` / `local_to_global` are absent from the checkout; the
+// clip is written from the geometry: the plane n . xi = a in the unit cell meets the square's /
+// cube's edges where the corner values n . xi - a change sign strictly, and a corner with value 0
+// is a point of its own. The world point is x_node + xi * d.
+
+// Monotone stand-in for atan2(y, x) over (-pi, pi], in (-2, 2]: the order of the reference's
+// angle sort (surface.jl:254-265) without a transcendental, so it is reproducible bit for bit.
+template <class T> inline T pseudo_angle(T y, T x) {
+  if (x == T(0) && y == T(0)) return T(0);
+  if (y >= T(0)) return x >= T(0) ? y / (x + y) : T(1) + (-x) / (y - x);
+  return x >= T(0) ? -((-y) / (x - y)) : -(T(1) + (-x) / (-x - y));
+}
+
+template <class T> struct PlicMesh {
+  std::vector<T> nodes;
+  std::vector<int32_t> elems;
+  std::vector<int64_t> cells;
+};
+
+// 2D: one segment per cell -- the two crossings, walking the square's edges (0,0)->(1,0)->(1,1)->
+// (0,1); a line that does not cross draws a zero-length segment (at the one corner it touches,
+// else at the lower corner; a degenerate fit at the lower corner). Kept when its length is at
+// least min_frac * min(d) (surface.jl:91-94).
+template <class T>
+PlicMesh<T> plic_mesh2(const cc_grid& g, const T* normals, const T* intercepts, const uint8_t* valid, T min_frac) {
+  PlicMesh<T> out;
+  const T x0[2] = {T(g.x0[0]), T(g.x0[1])}, d[2] = {T(g.d[0]), T(g.d[1])};
+  const T min_d = d[1] < d[0] ? d[1] : d[0];
+  const T corner[4][2] = {{T(0), T(0)}, {T(1), T(0)}, {T(1), T(1)}, {T(0), T(1)}};
+  for (int64_t j = 0; j < g.n[1]; ++j)
+    for (int64_t i = 0; i < g.n[0]; ++i) {
+      const int64_t ci = i + g.n[0] * j;
+      const T org[2] = {node_coord(x0[0], d[0], i), node_coord(x0[1], d[1], j)};
+      T xi[2][2] = {{T(0), T(0)}, {T(0), T(0)}};
+      if (valid[ci]) {
+        const T n0 = normals[2 * ci], n1 = normals[2 * ci + 1], a = intercepts[ci];
+        T s[4];
+        for (int k = 0; k < 4; ++k) s[k] = (n0 * corner[k][0] + n1 * corner[k][1]) - a;
+        int m = 0;
+        for (int k = 0; k < 4 && m < 2; ++k) {
+          if (s[k] == T(0)) { xi[m][0] = corner[k][0]; xi[m][1] = corner[k][1]; ++m; continue; }
+          const int k1 = (k + 1) & 3;
+          if ((s[k] < T(0) && s[k1] > T(0)) || (s[k] > T(0) && s[k1] < T(0))) {
+            const T t = s[k] / (s[k] - s[k1]);
+            xi[m][0] = corner[k][0] + t * (corner[k1][0] - corner[k][0]);
+            xi[m][1] = corner[k][1] + t * (corner[k1][1] - corner[k][1]);
+            ++m;
+          }
+        }
+        if (m == 0) xi[0][0] = xi[0][1] = T(0);
+        if (m < 2) { xi[1][0] = xi[0][0]; xi[1][1] = xi[0][1]; }
+      }
+      T p[2][2];
+      for (int q = 0; q < 2; ++q) {
+        p[q][0] = org[0] + xi[q][0] * d[0];
+        p[q][1] = org[1] + xi[q][1] * d[1];
+      }
+      const T dx = p[1][0] - p[0][0], dy = p[1][1] - p[0][1];
+      if (!(std::sqrt(dx * dx + dy * dy) >= min_frac * min_d)) continue;
+      const int32_t base = int32_t(out.nodes.size() / 2);
+      for (int q = 0; q < 2; ++q) { out.nodes.push_back(p[q][0]); out.nodes.push_back(p[q][1]); }
+      out.elems.push_back(base);
+      out.elems.push_back(base + 1);
+      out.cells.push_back(ci);
+    }
+  return out;
+}
+
+// 3D: the polygon (corners on the plane, then strict edge crossings in the order x-edges, y-edges,
+// z-edges), ordered about its centroid in the basis of surface.jl:247-249, fanned from its first
+// vertex with the area floor of surface.jl:162-181. Cells with fewer than 3 points draw nothing.
+template <class T>
+PlicMesh<T> plic_mesh3(const cc_grid& g, const T* normals, const T* intercepts, const uint8_t* valid, T min_frac) {
+  PlicMesh<T> out;
+  const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])}, d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
+  T min_d = d[0];
+  for (int a = 1; a < 3; ++a) min_d = d[a] < min_d ? d[a] : min_d;
+  const T min_area = min_frac * (min_d * min_d);
+  const T min_cross_sq = (T(2) * min_area) * (T(2) * min_area);
+  static const int edge[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3},
+                                  {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  for (int64_t k3 = 0; k3 < g.n[2]; ++k3)
+    for (int64_t j = 0; j < g.n[1]; ++j)
+      for (int64_t i = 0; i < g.n[0]; ++i) {
+        const int64_t ci = i + g.n[0] * (j + g.n[1] * k3);
+        if (!valid[ci]) continue;
+        const T nr[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
+        const T a = intercepts[ci];
+        const T org[3] = {node_coord(x0[0], d[0], i), node_coord(x0[1], d[1], j), node_coord(x0[2], d[2], k3)};
+        T s[8];
+        for (int c = 0; c < 8; ++c)
+          s[c] = ((nr[0] * T(c & 1) + nr[1] * T((c >> 1) & 1)) + nr[2] * T((c >> 2) & 1)) - a;
+        T xi[6][3];
+        int m = 0;
+        for (int c = 0; c < 8 && m < 6; ++c)
+          if (s[c] == T(0)) { xi[m][0] = T(c & 1); xi[m][1] = T((c >> 1) & 1); xi[m][2] = T((c >> 2) & 1); ++m; }
+        for (int e = 0; e < 12 && m < 6; ++e) {
+          const int p = edge[e][0], q = edge[e][1];
+          if ((s[p] < T(0) && s[q] > T(0)) || (s[p] > T(0) && s[q] < T(0))) {
+            const T t = s[p] / (s[p] - s[q]);
+            for (int ax = 0; ax < 3; ++ax) {
+              const T cp = T((p >> ax) & 1), cq = T((q >> ax) & 1);
+              xi[m][ax] = cp + t * (cq - cp);
+            }
+            ++m;
+          }
+        }
+        if (m < 3) continue;
+        T pt[6][3];
+        for (int v = 0; v < m; ++v)
+          for (int ax = 0; ax < 3; ++ax) pt[v][ax] = org[ax] + xi[v][ax] * d[ax];
+        T cen[3] = {T(0), T(0), T(0)};
+        for (int v = 0; v < m; ++v)
+          for (int ax = 0; ax < 3; ++ax) cen[ax] = cen[ax] + pt[v][ax];
+        for (int ax = 0; ax < 3; ++ax) cen[ax] = cen[ax] / T(m);
+        const bool zr = std::fabs(nr[2]) < T(0.9);
+        const T r[3] = {zr ? T(0) : T(1), T(0), zr ? T(1) : T(0)};
+        T u[3] = {r[1] * nr[2] - r[2] * nr[1], r[2] * nr[0] - r[0] * nr[2], r[0] * nr[1] - r[1] * nr[0]};
+        const T ul = std::sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+        for (int ax = 0; ax < 3; ++ax) u[ax] = u[ax] / ul;
+        const T v[3] = {nr[1] * u[2] - nr[2] * u[1], nr[2] * u[0] - nr[0] * u[2], nr[0] * u[1] - nr[1] * u[0]};
+        T ang[6];
+        for (int q = 0; q < m; ++q) {
+          const T dx = pt[q][0] - cen[0], dy = pt[q][1] - cen[1], dz = pt[q][2] - cen[2];
+          ang[q] = pseudo_angle((dx * v[0] + dy * v[1]) + dz * v[2], (dx * u[0] + dy * u[1]) + dz * u[2]);
+        }
+        for (int q = 1; q < m; ++q) {  // insertion sort, as surface.jl:256-265
+          const T ka = ang[q];
+          T kp[3] = {pt[q][0], pt[q][1], pt[q][2]};
+          int w = q - 1;
+          while (w >= 0 && ang[w] > ka) {
+            ang[w + 1] = ang[w];
+            for (int ax = 0; ax < 3; ++ax) pt[w + 1][ax] = pt[w][ax];
+            --w;
+          }
+          ang[w + 1] = ka;
+          for (int ax = 0; ax < 3; ++ax) pt[w + 1][ax] = kp[ax];
+        }
+        const int32_t base = int32_t(out.nodes.size() / 3);
+        for (int q = 0; q < m; ++q)
+          for (int ax = 0; ax < 3; ++ax) out.nodes.push_back(pt[q][ax]);
+        for (int q = 1; q < m - 1; ++q) {
+          const T a0 = pt[q][0] - pt[0][0], a1 = pt[q][1] - pt[0][1], a2 = pt[q][2] - pt[0][2];
+          const T b0 = pt[q + 1][0] - pt[0][0], b1 = pt[q + 1][1] - pt[0][1], b2 = pt[q + 1][2] - pt[0][2];
+          const T c0 = a1 * b2 - a2 * b1, c1 = a2 * b0 - a0 * b2, c2 = a0 * b1 - a1 * b0;
+          if ((c0 * c0 + c1 * c1) + c2 * c2 >= min_cross_sq) {
+            out.elems.push_back(base);
+            out.elems.push_back(base + q);
+            out.elems.push_back(base + q + 1);
+            out.cells.push_back(ci);
+          }
+        }
+      }
+  return out;
+}
+
 }  // namespace oc
 
 // ======================================================================================
@@ -1353,6 +1510,28 @@ int oc_ms_mesh(int prec, int tree, const cc_grid* g, const double* x0, const dou
                 : out(oc::ms_mesh_grid<double>(*g, (const double*)phi));
   return tree ? out(oc::ms_mesh_tree<float>(x0, based, nl, level, coord, (const float*)phi))
               : out(oc::ms_mesh_grid<float>(*g, (const float*)phi));
+}
+
+// generate_mesh for a PLIC cache: counts into *nn / *ne; arrays written when non-null.
+int oc_plic_mesh(int prec, const cc_grid* g, const void* normals, const void* intercepts, const uint8_t* valid,
+                 double min_frac, void* nodes, int32_t* elems, int64_t* cells, int64_t* nn, int64_t* ne) {
+  auto out = [&](auto c, int D) {
+    using TT = typename std::decay<decltype(c.nodes[0])>::type;
+    *nn = int64_t(c.nodes.size() / D);
+    *ne = int64_t(c.cells.size());
+    if (nodes) std::memcpy(nodes, c.nodes.data(), c.nodes.size() * sizeof(TT));
+    if (elems) std::memcpy(elems, c.elems.data(), c.elems.size() * sizeof(int32_t));
+    if (cells) std::memcpy(cells, c.cells.data(), c.cells.size() * sizeof(int64_t));
+    return 0;
+  };
+  if (g->dim == 3) {
+    if (prec == 1)
+      return out(oc::plic_mesh3<double>(*g, (const double*)normals, (const double*)intercepts, valid, min_frac), 3);
+    return out(oc::plic_mesh3<float>(*g, (const float*)normals, (const float*)intercepts, valid, float(min_frac)), 3);
+  }
+  if (prec == 1)
+    return out(oc::plic_mesh2<double>(*g, (const double*)normals, (const double*)intercepts, valid, min_frac), 2);
+  return out(oc::plic_mesh2<float>(*g, (const float*)normals, (const float*)intercepts, valid, float(min_frac)), 2);
 }
 
 int oc_ms_cells_from_phi(int prec, const cc_grid* g, const void* phi, const cc_cells* c) {

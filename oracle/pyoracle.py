@@ -59,6 +59,8 @@ def lib():
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_ms_mesh.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_plic_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_mc_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -176,6 +178,25 @@ def ms_mesh(domain, phi, prec):
     rc = lib().oc_ms_mesh(prec, int(tree), *args, _ptr(phi), _ptr(v), _ptr(sg), _ptr(c), C.byref(nv), C.byref(ns))
     assert rc == 0
     return v, sg, c
+
+
+def plic_mesh(g, normals, intercepts, valid, prec, min_frac=1e-4):
+    """The PLIC surface of every cell's plane: (nodes [nn, D], elements [ne, D] int32, cell of each
+    element [ne] int64)."""
+    T = dtype_of(prec)
+    D = g.dim
+    normals = np.ascontiguousarray(normals, T)
+    intercepts = np.ascontiguousarray(intercepts, T)
+    valid = np.ascontiguousarray(valid, np.uint8)
+    nn, ne = C.c_int64(0), C.c_int64(0)
+    gs = grid_struct(g)
+    args = (prec, C.byref(gs), _ptr(normals), _ptr(intercepts), _ptr(valid), float(min_frac))
+    assert lib().oc_plic_mesh(*args, None, None, None, C.byref(nn), C.byref(ne)) == 0
+    v = np.zeros((nn.value, D), T)
+    e = np.zeros((ne.value, D), np.int32)
+    c = np.zeros(ne.value, np.int64)
+    assert lib().oc_plic_mesh(*args, _ptr(v), _ptr(e), _ptr(c), C.byref(nn), C.byref(ne)) == 0
+    return v, e, c
 
 
 def mc_update(g, tape, table: bytes, prec):

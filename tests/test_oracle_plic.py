@@ -151,3 +151,68 @@ def test_float32_finite():
     assert cols["face_fraction"].dtype == np.float32
     assert np.all(np.isfinite(cols["face_fraction"]))
     assert np.all((cols["volume_fraction"] >= 0) & (cols["volume_fraction"] <= 1))
+
+
+def test_surface_2d_counts_and_points():
+    # test/test_plic.jl:114-137: generate_mesh hands over every cell and draws exactly the cut
+    # ones (84 on this fixture), two unshared nodes per segment; at fraction 0 every cell draws one.
+    g = cc.CartesianIsoGrid((-1.5, -1.5), (1.5, 1.5), 0.1)
+    cols, normals, icpt, valid = plic(g, cc.Circle((0.0, 0.0), 1.0))
+    kind = cols["kind"]
+    v, e, owner = po.plic_mesh(g, normals, icpt, valid, 1)
+    assert e.shape[0] == int((kind == 2).sum()) == 84
+    assert v.shape[0] == 2 * e.shape[0]
+    assert np.array_equal(e.ravel(), np.arange(v.shape[0]))
+    assert np.array_equal(owner, np.flatnonzero(kind == 2))
+    assert po.plic_mesh(g, normals, icpt, valid, 1, 0.0)[1].shape[0] == g.ncell
+    assert po.plic_mesh(g, normals, icpt, valid, 1, 0.1)[1].shape[0] <= 84
+    # each end lies on its own cell's boundary and on its plane
+    for s in range(e.shape[0]):
+        ci = owner[s]
+        i, j = ci % g.n[0], ci // g.n[0]
+        lo = np.array([g.x0[0] + i * g.d[0], g.x0[1] + j * g.d[1]])
+        for p in v[e[s]]:
+            xi = (p - lo) / g.d[0]
+            assert np.all(xi > -1e-12) and np.all(xi < 1 + 1e-12)
+            assert min(abs(xi[0]), abs(xi[1]), abs(1 - xi[0]), abs(1 - xi[1])) < 1e-12
+            assert abs(normals[ci] @ xi - icpt[ci]) < 1e-12
+
+
+def test_surface_2d_corner_touch_draws_a_point():
+    # test/test_plic.jl:150-178: a line through cell corners. Every uncut cell draws a zero-length
+    # segment (or one no longer than roundoff), never a false diagonal; at the default floor only
+    # the cut cells' segments remain, both ends on the line.
+    g = cc.CartesianIsoGrid((-1.5, -1.5), (1.5, 1.5), 0.1)
+    nrm = np.array([1.0, 1.0]) / math.sqrt(2.0)
+    cols, normals, icpt, valid = plic(g, cc.Plane((0.0, 0.0), nrm))
+    cut = cols["kind"] == 2
+    assert cut.sum() > 0
+    v, e, owner = po.plic_mesh(g, normals, icpt, valid, 1, 0.0)
+    assert e.shape[0] == g.ncell
+    length = np.linalg.norm(v[e[:, 1]] - v[e[:, 0]], axis=1)
+    assert np.all(cut | (length < 1e-12 * g.d[0]))
+    assert int((~cut & (length == 0)).sum()) > 0
+    v2, e2, owner2 = po.plic_mesh(g, normals, icpt, valid, 1)
+    assert e2.shape[0] == int(cut.sum())
+    assert np.array_equal(v2.reshape(-1, 2, 2), v[e[cut]])
+    assert np.all(np.abs(v2 @ nrm) < 1e-12)
+
+
+def test_surface_3d_sphere_counts():
+    # test/test_plic.jl:139-145: the unit sphere at sz = 0.15 draws 3384 nodes and 1688 triangles.
+    g = cc.CartesianIsoGrid((-1.5,) * 3, (1.5,) * 3, 0.15)
+    sph = cc.Sphere((0.0, 0.0, 0.0), 1.0)
+    cols, normals, icpt, valid = plic(g, sph)
+    dom = g.ncell * np.prod(g.d)
+    assert math.isclose(dom - cols["volume_fraction"].sum() * np.prod(g.d), po.calc_volume(g, cc.flatten(sph, 3), 1),
+                        rel_tol=1e-12)
+    v, t, owner = po.plic_mesh(g, normals, icpt, valid, 1)
+    assert v.shape[0] == 3384
+    assert t.shape[0] == 1688
+    # every fan triangle is wound one way about its plane's normal; the area is the sphere's
+    tri = v[t]
+    cr = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    w = np.einsum("ij,ij->i", cr, normals[owner])
+    assert np.all(w > 0) or np.all(w < 0)
+    area = 0.5 * np.linalg.norm(cr, axis=1).sum()
+    assert abs(area / (4 * math.pi) - 1) < 0.02
