@@ -401,6 +401,8 @@ def plic_block(args, dev, cc):
                      "kind_differs_from_f64": int((c.cells.kind != ref.cells.kind).sum().item()),
                      "vf_err_vs_f64": {"max": vf.max().item(), "mean": vf.mean().item()},
                      "face_fraction_err_vs_f64": {"max": fd.max().item(), "mean": fd.mean().item()}}
+        if name == "f32":
+            out["surface_f32"] = plic_surface_timing(c, g, dev)
         del c, vf, fd
         torch.cuda.empty_cache()
     del ref
@@ -419,6 +421,31 @@ def plic_block(args, dev, cc):
                                                  "ms": mc_ms},
                               f64_minus_mc_in_sigmas=(vols["f64"] - mc) / sigma)
     return out
+
+
+def plic_surface_timing(cache, g, dev, reps=5):
+    """generate_mesh of a PLIC cache (every cell's plane clipped to its cell; count, scan, emit),
+    timed on the host around the blocking call."""
+    import importlib
+    import torch
+    S = importlib.import_module("cutcell_b200.surface")
+    for _ in range(2):
+        m = S.generate_mesh(cache, g)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m = S.generate_mesh(cache, g)
+    torch.cuda.synchronize(dev)
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    ncell = cache.intercepts.shape[0]
+    # per cell the two passes each read the plane (D+1 values) and the flag
+    plane_bytes = 2 * ncell * (4 * (g.dim + 1) + 1)
+    out_bytes = m.nodes.numel() * 4 + m.elements.numel() * 4 + m.cells.numel() * 8
+    r = {"ms": ms, "cells_per_s": ncell / (ms * 1e-3), "nodes": int(m.nodes.shape[0]),
+         "triangles": int(m.elements.shape[0]), "algorithmic_gb": (plane_bytes + out_bytes) / 1e9,
+         "roofline_frac": (plane_bytes + out_bytes) / (ms * 1e-3) / 1e9 / measured_peak()[0]}
+    del m
+    return r
 
 
 def mesh_block(args, dev, cc):

@@ -324,6 +324,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->mesh_scan) cudaFree(h->mesh_scan);
   if (h->prune) cudaFree(h->prune);
   cci::free_ms_mesh(h);
+  cci::free_plic_mesh(h);
   delete h;
   return CC_OK;
 }
@@ -500,6 +501,7 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
+  ++h->generation;
   if (h->prec == CC_F64) {
     if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     e = g->dim == 3 ? cci::launch_plic<double, 3>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),

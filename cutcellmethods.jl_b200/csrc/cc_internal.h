@@ -108,6 +108,7 @@ int tape_prunable(const cc_optape* t);
 
 // Release the contour a marching-squares handle holds (ms_mesh.cu).
 void free_ms_mesh(cc_handle* h);
+void free_plic_mesh(cc_handle* h);
 
 // Record the message cc_last_error() returns on this thread.
 void set_last_error(const std::string& msg);
@@ -146,5 +147,7 @@ struct cc_handle {
   void* prune = nullptr;  // marching cubes: per fill CTA pruned op lists of a union of spheres
   size_t prune_bytes = 0;
   void* ms_mesh = nullptr;  // marching squares: the last contour built (ms_mesh.cu)
+  void* plic_mesh = nullptr;  // PLIC: the last surface count's block offsets (plic_mesh.cu)
+  uint64_t generation = 0;    // bumped by every update, so a stored count knows its planes are stale
 };
 

@@ -19,8 +19,8 @@
 // geometry, so its vertex order may differ from that package's; the sort makes the polygon's
 // winding the same.
 //
-// Two passes over the entries (count, then emit at scanned offsets), each thread owning IPT
-// consecutive entries, so the output is in entry order with no atomics.
+// Two passes over the entries (count, then emit at scanned offsets), so the output is in entry
+// order with no atomics.
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
@@ -33,8 +33,9 @@ namespace {
 using namespace ccd;
 
 constexpr int MB = 256;
-constexpr int IPT = 8;
+constexpr int IPT = 32;  // rounds per block: a block's one long clip pass is spread over MB * IPT entries
 constexpr int BLK = MB * IPT;
+constexpr int KEEP = 1024;  // compacted entries a block hands from the count to the emit pass
 
 template <class T, int D>
 struct PlicIn {
@@ -77,7 +78,10 @@ __device__ int clip_cell(const PlicIn<T, D>& P, long long entry, T out[6][3]) {
     T s[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) s[k] = (nrm[0] * c[k][0] + nrm[1] * c[k][1]) - a;
-    for (int k = 0; k < 4 && m < 2 && ok; ++k) {
+    // one strict sign at every corner: no corner on the line and no crossing (m stays 0)
+    const bool miss = (s[0] > T(0) && s[1] > T(0) && s[2] > T(0) && s[3] > T(0)) ||
+                      (s[0] < T(0) && s[1] < T(0) && s[2] < T(0) && s[3] < T(0));
+    for (int k = 0; k < 4 && m < 2 && ok && !miss; ++k) {
       if (s[k] == T(0)) { xi[m][0] = c[k][0]; xi[m][1] = c[k][1]; ++m; continue; }
       const int k1 = (k + 1) & 3;
       if ((s[k] < T(0) && s[k1] > T(0)) || (s[k] > T(0) && s[k1] < T(0))) {
@@ -104,13 +108,22 @@ __device__ int clip_cell(const PlicIn<T, D>& P, long long entry, T out[6][3]) {
   if (!ok) return 0;
   // 3D: corners by bits (x = bit 0, y = bit 1, z = bit 2); the 12 edges as corner pairs
   T s[8];
+  bool pos = true, neg = true;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) s[c] = ((nrm[0] * T(c & 1) + nrm[1] * T((c >> 1) & 1)) + nrm[2] * T((c >> 2) & 1)) - a;
+  for (int c = 0; c < 8; ++c) {
+    s[c] = ((nrm[0] * T(c & 1) + nrm[1] * T((c >> 1) & 1)) + nrm[2] * T((c >> 2) & 1)) - a;
+    pos = pos && s[c] > T(0);
+    neg = neg && s[c] < T(0);
+  }
+  // one strict sign at every corner: no corner on the plane and no crossing -- most cells
+  if (pos || neg) return 0;
   for (int c = 0; c < 8 && m < 6; ++c)
     if (s[c] == T(0)) { xi[m][0] = T(c & 1); xi[m][1] = T((c >> 1) & 1); xi[m][2] = T((c >> 2) & 1); ++m; }
-  const int e[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  // the 12 edges, x-edges then y- then z-: edge j of axis ax runs from corner p (bit ax clear,
+  // the other two bits j) to p | 1 << ax
   for (int k = 0; k < 12 && m < 6; ++k) {
-    const int p = e[k][0], q = e[k][1];
+    const int ax0 = k >> 2, j = k & 3;
+    const int p = ((j >> ax0) << (ax0 + 1)) | (j & ((1 << ax0) - 1)), q = p | (1 << ax0);
     if ((s[p] < T(0) && s[q] > T(0)) || (s[p] > T(0) && s[q] < T(0))) {
       const T t = s[p] / (s[p] - s[q]);
 #pragma unroll
@@ -219,57 +232,136 @@ __global__ void scan2_kernel(unsigned long long* a, long long n, unsigned long l
   if (threadIdx.x < 2) total[threadIdx.x] = carry[threadIdx.x];
 }
 
+// True when entry k certainly draws nothing: a degenerate fit, or a plane that misses its cell
+// by more than rounding (3D), or -- in 2D -- such a miss when the length floor drops the
+// zero-length segment it leaves. Conservative: a true here implies clip_cell + cell_counts give no
+// node, a false only sends the entry to the full clip. The cube's (square's) corner values
+// n . c - a span [sum min(n_i, 0) - a, sum max(n_i, 0) - a]; the full clip's corner sums are
+// within 3 u (|n|_1 + |a|) of exact (u the unit roundoff), these bounds within 2 u |n|_1, so a gap
+// of 64 u (|n|_1 + |a|) leaves every corner value one strict sign. NaN or inf fails both tests.
 template <class T, int D>
-__global__ void __launch_bounds__(MB) plic_count_kernel(const PlicIn<T, D> P, T min_d, unsigned long long* bsum) {
-  const long long nc = P.count;
-  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
-  unsigned long long nn = 0, ne = 0;
-  for (int q = 0; q < IPT; ++q) {
-    const long long k = c0 + q;
-    if (k >= nc) break;
-    T p[6][3];
-    const int m = clip_cell<T, D>(P, k, p);
-    int a, b;
-    unsigned keep;
-    cell_counts<T, D>(P, m, p, min_d, a, b, keep);
-    nn += a;
-    ne += b;
-  }
-  unsigned long long t0, t1;
-  block_scan(nn, &t0);
-  block_scan(ne, &t1);
-  if (threadIdx.x == 0) { bsum[2 * blockIdx.x] = t0; bsum[2 * blockIdx.x + 1] = t1; }
+__device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, long long k, T min_d) {
+  const T n0 = P.normals[D * k], n1 = P.normals[D * k + 1], n2 = D == 3 ? P.normals[D * k + 2] : T(0);
+  const T a = P.intercepts[k];
+  const bool ok = P.valid ? P.valid[k] != 0 : (n0 != T(0) || n1 != T(0) || n2 != T(0));
+  const T zero = T(0);
+  const T lo = (fmin(n0, zero) + fmin(n1, zero)) + fmin(n2, zero);
+  const T hi = (fmax(n0, zero) + fmax(n1, zero)) + fmax(n2, zero);
+  const T tol = (sizeof(T) == 4 ? T(0x1p-18) : T(0x1p-47)) * (((fabs(n0) + fabs(n1)) + fabs(n2)) + fabs(a));
+  const bool miss = (a - hi > tol) || (lo - a > tol);
+  if (D == 2) return (!ok || miss) && !(T(0) >= P.min_frac * min_d);
+  return !ok || miss;
 }
 
+// Each block owns BLK consecutive entries, taken round-major (round q covers entries
+// blk*BLK + q*MB + [0, MB), one per thread, so the plane loads coalesce). Pass 1 tests all IPT
+// rounds with no barrier in between (their loads overlap) into a bit mask, and the entries that
+// may draw something are placed in entry order -- round, then warp, then lane -- into shared memory
+// through warp ballots and one table of per-(round, warp) counts. Pass 2 (the caller) runs the full
+// clip over the compacted entries, MB at a time, so the long path runs on dense warps rather than
+// one lane of many. Returns the number of compacted entries (block-uniform).
+template <class T, int D>
+__device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d, int* cand) {
+  __shared__ int wcnt[IPT][MB / 32];
+  const long long start = (long long)blockIdx.x * BLK;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  static_assert(IPT <= 32, "one bit per round");
+  unsigned bits = 0;
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q) {
+    const long long k = start + (long long)q * MB + threadIdx.x;
+    if (k < P.count && !draws_nothing<T, D>(P, k, min_d)) bits |= 1u << q;
+  }
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q) {
+    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+    if (lane == 0) wcnt[q][w] = __popc(bal);
+  }
+  __syncthreads();
+  int before = 0;  // compacted entries of the earlier rounds (and, within a round, earlier warps)
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q) {
+    int round = 0, mine = 0;
+    for (int x = 0; x < MB / 32; ++x) {
+      const int c = wcnt[q][x];
+      mine += x < w ? c : 0;
+      round += c;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+    if ((bits >> q) & 1u) cand[before + mine + __popc(bal & below)] = q * MB + threadIdx.x;
+    before += round;
+  }
+  __syncthreads();
+  return before;
+}
+
+// Node and element counts travel packed in one 64-bit word (nodes high, elements low; a block's
+// element count stays far below 2^32).
+// The count pass also saves each block's compacted entries (up to KEEP; -1 in kept_n when more),
+// so the emit pass clips them without testing every entry again.
+template <class T, int D>
+__global__ void __launch_bounds__(MB, 5) plic_count_kernel(const PlicIn<T, D> P, T min_d, unsigned long long* bsum,
+                                                        int* kept, int* kept_n) {
+  __shared__ int cand[BLK];
+  const int ncand = compact_candidates<T, D>(P, min_d, cand);
+  const long long start = (long long)blockIdx.x * BLK;
+  if (threadIdx.x == 0) kept_n[blockIdx.x] = ncand <= KEEP ? ncand : -1;
+  if (ncand <= KEEP)
+    for (int i = threadIdx.x; i < ncand; i += MB) kept[(size_t)blockIdx.x * KEEP + i] = cand[i];
+  unsigned long long packed = 0;
+  for (int i = threadIdx.x; i < ncand; i += MB) {
+    T p[6][3];
+    const int m = clip_cell<T, D>(P, start + cand[i], p);
+    int a, b;
+    unsigned keep;
+    cell_counts<T, D>(P, m, p, min_d, a, b, keep);
+    packed += ((unsigned long long)a << 32) | (unsigned long long)b;
+  }
+  unsigned long long t;
+  block_scan(packed, &t);
+  if (threadIdx.x == 0) { bsum[2 * blockIdx.x] = t >> 32; bsum[2 * blockIdx.x + 1] = t & 0xffffffffull; }
+}
+
+// The writes are checked against the output capacities: offsets from a count of other planes (a
+// caller that changed them between its two calls) raise *overflow instead of writing past the end.
 template <class T, int D>
 __global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, T min_d, const unsigned long long* boff,
-                                                       T* nodes, int32_t* elems, int64_t* cells) {
-  const long long nc = P.count;
-  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
-  unsigned long long nn = 0, ne = 0;
-  for (int q = 0; q < IPT; ++q) {
-    const long long k = c0 + q;
-    if (k >= nc) break;
-    T p[6][3];
-    const int m = clip_cell<T, D>(P, k, p);
-    int a, b;
-    unsigned keep;
-    cell_counts<T, D>(P, m, p, min_d, a, b, keep);
-    nn += a;
-    ne += b;
+                                                       T* nodes, unsigned long long ncap, int32_t* elems,
+                                                       unsigned long long ecap, int64_t* cells,
+                                                       unsigned long long* overflow, const int* kept,
+                                                       const int* kept_n) {
+  __shared__ int cand[BLK];
+  int ncand = kept_n[blockIdx.x];  // block-uniform
+  if (ncand == 0) return;
+  if (ncand > 0) {
+    for (int i = threadIdx.x; i < ncand; i += MB) cand[i] = kept[(size_t)blockIdx.x * KEEP + i];
+    __syncthreads();
+  } else {
+    ncand = compact_candidates<T, D>(P, min_d, cand);
   }
-  unsigned long long t0, t1;
-  unsigned long long vn = boff[2 * blockIdx.x] + block_scan(nn, &t0);
-  unsigned long long ve = boff[2 * blockIdx.x + 1] + block_scan(ne, &t1);
-  for (int q = 0; q < IPT; ++q) {
-    const long long k = c0 + q;
-    if (k >= nc) break;
+  const long long start = (long long)blockIdx.x * BLK;
+  unsigned long long run_n = boff[2 * blockIdx.x], run_e = boff[2 * blockIdx.x + 1];
+  for (int c0 = 0; c0 < ncand; c0 += MB) {  // block-uniform
+    const int i = c0 + threadIdx.x;
+    const long long k = i < ncand ? start + cand[i] : 0;
     T p[6][3];
-    const int m = clip_cell<T, D>(P, k, p);
-    int a, b;
-    unsigned keep;
-    cell_counts<T, D>(P, m, p, min_d, a, b, keep);
+    int m = 0, a = 0, b = 0;
+    unsigned keep = 0;
+    if (i < ncand) {
+      m = clip_cell<T, D>(P, k, p);
+      cell_counts<T, D>(P, m, p, min_d, a, b, keep);
+    }
+    unsigned long long t;
+    const unsigned long long pre = block_scan(((unsigned long long)a << 32) | (unsigned long long)b, &t);
+    unsigned long long vn = run_n + (pre >> 32), ve = run_e + (pre & 0xffffffffull);
+    run_n += t >> 32;
+    run_e += t & 0xffffffffull;
     if (a == 0) continue;
+    if (vn + a > ncap || ve + b > ecap) {
+      atomicOr(overflow, 1ull);
+      continue;
+    }
     const long long ci = P.index ? (long long)P.index[k] : k;
     for (int v = 0; v < a; ++v)
 #pragma unroll
@@ -279,7 +371,6 @@ __global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, T m
         elems[2 * ve] = int32_t(vn);
         elems[2 * ve + 1] = int32_t(vn + 1);
         cells[ve] = ci;
-        ++ve;
       }
     } else {
       for (int v = 1; v < m - 1; ++v) {
@@ -291,7 +382,6 @@ __global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, T m
         ++ve;
       }
     }
-    vn += a;
   }
 }
 
@@ -304,10 +394,32 @@ cc_status cuda_fail(cudaError_t e, const char* where) {
   return CC_CUDA_ERR;
 }
 
+// A surface count kept on a handle between the count call and the emit call of generate_mesh:
+// the scanned block offsets and totals, and what they were counted from.
+struct Stored {
+  unsigned long long* bsum = nullptr;  // offsets, totals, overflow flag, the kept entries
+  size_t cap = 0;                      // entries of bsum
+  bool valid = false;
+  uint64_t generation = 0;
+  const void *normals = nullptr, *intercepts = nullptr, *is_valid = nullptr;
+  cc_grid g{};
+  double min_frac = 0.0;
+  int prec = -1;
+  unsigned long long tot[2] = {0, 0};
+  bool same(const cc_handle* h, const cc_grid* gg, const void* n, const void* i, const void* v, double f) const {
+    if (!valid || generation != h->generation || normals != n || intercepts != i || is_valid != v ||
+        prec != h->prec || min_frac != f || g.dim != gg->dim)
+      return false;
+    for (int a = 0; a < gg->dim; ++a)
+      if (g.n[a] != gg->n[a] || g.x0[a] != gg->x0[a] || g.d[a] != gg->d[a]) return false;
+    return true;
+  }
+};
+
 template <class T, int D>
 cc_status run(const cc_grid* g, const void* normals, const void* intercepts, const uint8_t* valid,
               const int64_t* index, int64_t count, double min_frac, void* nodes, int64_t ncap, int32_t* elems,
-              int64_t ecap, int64_t* cells, int64_t* n_nodes, int64_t* n_elems, cudaStream_t s) {
+              int64_t ecap, int64_t* cells, int64_t* n_nodes, int64_t* n_elems, cudaStream_t s, cc_handle* h) {
   PlicIn<T, D> P;
   for (int a = 0; a < 3; ++a) {
     P.x0[a] = a < D ? T(g->x0[a]) : T(0);
@@ -329,52 +441,119 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
     return CC_OK;
   }
   const long long nb = (nc + BLK - 1) / BLK;
-  unsigned long long* bsum = nullptr;
-  cudaError_t e = cudaMalloc(&bsum, (2 * size_t(nb) + 2) * sizeof(unsigned long long));
-  if (e != cudaSuccess) return cuda_fail(e, "generate_mesh scratch");
-  plic_count_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum);
-  scan2_kernel<<<1, MB, 0, s>>>(bsum, nb, bsum + 2 * nb);
-  unsigned long long tot[2] = {0, 0};
-  if ((e = cudaGetLastError()) == cudaSuccess)
-    e = cudaMemcpyAsync(tot, bsum + 2 * nb, sizeof tot, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e == cudaSuccess) {
-    if (n_nodes) *n_nodes = (int64_t)tot[0];
-    if (n_elems) *n_elems = (int64_t)tot[1];
-    if (tot[0] > 0x7fffffffull) {
-      cudaFree(bsum);
-      return fail(CC_TOO_LARGE, "generate_mesh: more nodes than int32 element indices address");
+  // bsum: 2*nb block offsets, 2 totals, 1 overflow flag; then kept_n[nb] and kept[nb * KEEP]
+  const size_t words = 2 * size_t(nb) + 3;
+  const size_t need = words + (size_t(nb) * (KEEP + 1) + 1) / 2;
+  const bool emit = nodes || elems;
+  // With a handle the buffer is kept, and an emit call right after a count of the same planes
+  // (same update, arrays, grid and fraction) starts from that count's offsets.
+  Stored local;
+  Stored* st = &local;
+  if (h) {
+    if (!h->plic_mesh) h->plic_mesh = new Stored();
+    st = static_cast<Stored*>(h->plic_mesh);
+  }
+  cudaError_t e = cudaSuccess;
+  if (st->cap < need) {
+    if (st->bsum) cudaFree(st->bsum);
+    st->bsum = nullptr;
+    st->cap = 0;
+    st->valid = false;
+    if ((e = cudaMalloc(&st->bsum, need * sizeof(unsigned long long))) != cudaSuccess)
+      return cuda_fail(e, "generate_mesh scratch");
+    st->cap = need;
+  }
+  const bool reuse = h && emit && st->same(h, g, normals, intercepts, valid, min_frac);
+  unsigned long long* bsum = st->bsum;
+  int* kept_n = reinterpret_cast<int*>(bsum + words);
+  int* kept = kept_n + nb;
+  auto release = [&]() {
+    if (!h && local.bsum) cudaFree(local.bsum);
+  };
+  unsigned long long tot[2] = {st->tot[0], st->tot[1]};
+  if (!reuse) {
+    st->valid = false;
+    plic_count_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, kept, kept_n);
+    scan2_kernel<<<1, MB, 0, s>>>(bsum, nb, bsum + 2 * nb);
+    if ((e = cudaGetLastError()) == cudaSuccess)
+      e = cudaMemcpyAsync(tot, bsum + 2 * nb, sizeof tot, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      release();
+      return cuda_fail(e, "generate_mesh count");
     }
-    if (nodes || elems) {
-      if (!nodes || !elems || !cells || ncap < (int64_t)tot[0] || ecap < (int64_t)tot[1]) {
-        cudaFree(bsum);
-        return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
-      }
-      if (tot[1] > 0)
-        plic_emit_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, static_cast<T*>(nodes), elems, cells);
-      e = cudaGetLastError();
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (h) {
+      st->valid = true;
+      st->generation = h->generation;
+      st->normals = normals;
+      st->intercepts = intercepts;
+      st->is_valid = valid;
+      st->g = *g;
+      st->min_frac = min_frac;
+      st->prec = h->prec;
+      st->tot[0] = tot[0];
+      st->tot[1] = tot[1];
     }
   }
-  cudaFree(bsum);
+  if (n_nodes) *n_nodes = (int64_t)tot[0];
+  if (n_elems) *n_elems = (int64_t)tot[1];
+  if (tot[0] > 0x7fffffffull) {
+    release();
+    return fail(CC_TOO_LARGE, "generate_mesh: more nodes than int32 element indices address");
+  }
+  if (emit) {
+    if (!nodes || !elems || !cells || ncap < (int64_t)tot[0] || ecap < (int64_t)tot[1]) {
+      release();
+      return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
+    }
+    unsigned long long overflow = 0;
+    if (tot[1] > 0) {
+      e = cudaMemsetAsync(bsum + 2 * nb + 2, 0, sizeof(unsigned long long), s);
+      if (e == cudaSuccess) {
+        plic_emit_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, static_cast<T*>(nodes),
+                                                           (unsigned long long)ncap, elems, (unsigned long long)ecap,
+                                                           cells, bsum + 2 * nb + 2, kept, kept_n);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&overflow, bsum + 2 * nb + 2, sizeof overflow, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (h) st->valid = false;  // one emit per count
+    if (e == cudaSuccess && overflow) {
+      release();
+      return fail(CC_BAD_ARG, "generate_mesh: the planes changed between the count and the emit call");
+    }
+  }
+  release();
   return e == cudaSuccess ? CC_OK : cuda_fail(e, "generate_mesh");
 }
 
 cc_status surface(int prec, const cc_grid* g, const void* normals, const void* intercepts, const uint8_t* valid,
                   const int64_t* index, int64_t count, double min_frac, void* nodes, int64_t ncap, int32_t* elems,
-                  int64_t ecap, int64_t* cells, int64_t* n_nodes, int64_t* n_elems, cudaStream_t s) {
+                  int64_t ecap, int64_t* cells, int64_t* n_nodes, int64_t* n_elems, cudaStream_t s, cc_handle* h) {
   if (prec == CC_F64)
     return g->dim == 3 ? run<double, 3>(g, normals, intercepts, valid, index, count, min_frac, nodes, ncap, elems, ecap,
-                                        cells, n_nodes, n_elems, s)
+                                        cells, n_nodes, n_elems, s, h)
                        : run<double, 2>(g, normals, intercepts, valid, index, count, min_frac, nodes, ncap, elems, ecap,
-                                        cells, n_nodes, n_elems, s);
+                                        cells, n_nodes, n_elems, s, h);
   return g->dim == 3 ? run<float, 3>(g, normals, intercepts, valid, index, count, min_frac, nodes, ncap, elems, ecap,
-                                     cells, n_nodes, n_elems, s)
+                                     cells, n_nodes, n_elems, s, h)
                      : run<float, 2>(g, normals, intercepts, valid, index, count, min_frac, nodes, ncap, elems, ecap,
-                                     cells, n_nodes, n_elems, s);
+                                     cells, n_nodes, n_elems, s, h);
 }
 
 }  // namespace
+
+namespace cci {
+void free_plic_mesh(cc_handle* h) {
+  if (!h || !h->plic_mesh) return;
+  Stored* st = static_cast<Stored*>(h->plic_mesh);
+  if (st->bsum) cudaFree(st->bsum);
+  delete st;
+  h->plic_mesh = nullptr;
+}
+}  // namespace cci
 
 extern "C" {
 
@@ -393,7 +572,7 @@ cc_status cc_plic_surface(int prec, const cc_grid* g, const void* normals, const
   if (!(min_tri_area_fraction >= 0.0)) return fail(CC_BAD_ARG, "min_tri_area_fraction must be >= 0");
   return surface(prec, g, normals, intercepts, is_valid, cell_index, n_entries, min_tri_area_fraction, nodes,
                  node_capacity, elements, element_capacity, element_cells, n_nodes, n_elements,
-                 static_cast<cudaStream_t>(stream));
+                 static_cast<cudaStream_t>(stream), nullptr);
 }
 
 cc_status cc_plic_mesh(cc_handle* h, const cc_grid* g, const void* normals, const void* intercepts,
@@ -411,7 +590,7 @@ cc_status cc_plic_mesh(cc_handle* h, const cc_grid* g, const void* normals, cons
   if (old != h->device) cudaSetDevice(h->device);
   const cc_status st = surface(h->prec, g, normals, intercepts, is_valid, nullptr, 0, min_tri_area_fraction, nodes,
                                node_capacity, elements, element_capacity, element_cells, n_nodes, n_elements,
-                               static_cast<cudaStream_t>(stream));
+                               static_cast<cudaStream_t>(stream), h);
   if (old >= 0 && old != h->device) cudaSetDevice(old);
   return st;
 }

@@ -168,3 +168,41 @@ def test_large_grid_properties():
     assert float(dist.abs().max()) < 1e-4
     area = 0.5 * torch.linalg.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]).norm(dim=1).sum()
     assert abs(float(area) / (4 * math.pi * 0.77 ** 2) - 1) < 2e-3
+
+
+def test_count_then_emit_reuse_and_changed_planes():
+    """The handle keeps the count for the emit call that follows it; planes written between the
+    two calls make the emit fail cleanly (its writes are checked against the counted capacities)
+    rather than run past the arrays, and the next generate_mesh counts afresh."""
+    import ctypes as C
+    L = __import__("cutcell_b200._lib", fromlist=["_lib"])
+    cache_mod = __import__("cutcell_b200.cache", fromlist=["cache"])
+    g = cc.CartesianIsoGrid((-1.0,) * 3, (1.0,) * 3, 0.05)
+    c = plic_cache(g, cc.Sphere((0.01, 0.02, -0.03), 0.7), 1)
+    first = S.generate_mesh(c, g)
+    again = S.generate_mesh(c, g)                       # count, then emit from the kept offsets
+    assert torch.equal(first.nodes, again.nodes) and torch.equal(first.elements, again.elements)
+    lib = c.handle.lib
+    gs = cache_mod.grid_struct(g)
+    nn, ne = C.c_int64(0), C.c_int64(0)
+    head = (c.handle.h, C.byref(gs), c.normals.data_ptr(), c.intercepts.data_ptr(), c.is_valid.data_ptr(), 1e-4)
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.cc_plic_mesh(*head, None, 0, None, 0, None, C.byref(nn), C.byref(ne), s) == 0
+    assert (nn.value, ne.value) == (first.nodes.shape[0], first.elements.shape[0])
+    nodes = torch.empty(nn.value, 3, dtype=torch.float64, device="cuda")
+    elems = torch.empty(ne.value, 3, dtype=torch.int32, device="cuda")
+    cells = torch.empty(ne.value, dtype=torch.int64, device="cuda")
+    # every plane now cuts its cell through the middle: far more triangles than were counted
+    saved_n, saved_i, saved_v = c.normals.clone(), c.intercepts.clone(), c.is_valid.clone()
+    c.normals.zero_()
+    c.normals[:, 0] = 1.0
+    c.intercepts.fill_(0.5)
+    c.is_valid.fill_(1)
+    rc = lib.cc_plic_mesh(*head, nodes.data_ptr(), nn.value, elems.data_ptr(), ne.value, cells.data_ptr(),
+                          C.byref(nn), C.byref(ne), s)
+    assert rc == L.CC_BAD_ARG
+    c.normals.copy_(saved_n)
+    c.intercepts.copy_(saved_i)
+    c.is_valid.copy_(saved_v)
+    after = S.generate_mesh(c, g)
+    assert torch.equal(first.nodes, after.nodes) and torch.equal(first.elements, after.elements)
