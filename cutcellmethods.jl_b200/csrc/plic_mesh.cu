@@ -240,10 +240,11 @@ __global__ void scan2_kernel(unsigned long long* a, long long n, unsigned long l
 // within 3 u (|n|_1 + |a|) of exact (u the unit roundoff), these bounds within 2 u |n|_1, so a gap
 // of 64 u (|n|_1 + |a|) leaves every corner value one strict sign. NaN or inf fails both tests.
 template <class T, int D>
-__device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, long long k, T min_d) {
-  const T n0 = P.normals[D * k], n1 = P.normals[D * k + 1], n2 = D == 3 ? P.normals[D * k + 2] : T(0);
-  const T a = P.intercepts[k];
-  const bool ok = P.valid ? P.valid[k] != 0 : (n0 != T(0) || n1 != T(0) || n2 != T(0));
+__device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, const T* nrm, const T* icp, const uint8_t* val,
+                                              int r, T min_d) {
+  const T n0 = nrm[D * r], n1 = nrm[D * r + 1], n2 = D == 3 ? nrm[D * r + 2] : T(0);
+  const T a = icp[r];
+  const bool ok = val ? val[r] != 0 : (n0 != T(0) || n1 != T(0) || n2 != T(0));
   const T zero = T(0);
   const T lo = (fmin(n0, zero) + fmin(n1, zero)) + fmin(n2, zero);
   const T hi = (fmax(n0, zero) + fmax(n1, zero)) + fmax(n2, zero);
@@ -262,38 +263,39 @@ __device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, long long k
 // one lane of many. Returns the number of compacted entries (block-uniform).
 template <class T, int D>
 __device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d, int* cand) {
-  __shared__ int wcnt[IPT][MB / 32];
+  static_assert(IPT <= 32 && IPT * (MB / 32) == MB, "one bit per round; one (round, warp) slot per thread");
+  __shared__ int slot[IPT * (MB / 32)];  // per (round, warp): its count, then its first position
   const long long start = (long long)blockIdx.x * BLK;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  static_assert(IPT <= 32, "one bit per round");
+  // this block's entries, addressed by 32-bit offsets
+  const int here = P.count - start < BLK ? int(P.count - start) : BLK;
+  const T* nrm = P.normals + D * start;
+  const T* icp = P.intercepts + start;
+  const uint8_t* val = P.valid ? P.valid + start : nullptr;
   unsigned bits = 0;
 #pragma unroll 8
   for (int q = 0; q < IPT; ++q) {
-    const long long k = start + (long long)q * MB + threadIdx.x;
-    if (k < P.count && !draws_nothing<T, D>(P, k, min_d)) bits |= 1u << q;
+    const int r = q * MB + threadIdx.x;
+    if (r < here && !draws_nothing<T, D>(P, nrm, icp, val, r, min_d)) bits |= 1u << q;
   }
 #pragma unroll 8
   for (int q = 0; q < IPT; ++q) {
     const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if (lane == 0) wcnt[q][w] = __popc(bal);
+    if (lane == 0) slot[q * (MB / 32) + w] = __popc(bal);
   }
   __syncthreads();
-  int before = 0;  // compacted entries of the earlier rounds (and, within a round, earlier warps)
+  unsigned long long total;
+  const unsigned long long first = block_scan((unsigned long long)slot[threadIdx.x], &total);
+  slot[threadIdx.x] = (int)first;  // block_scan's closing barrier ordered every read before this
+  __syncthreads();
   const unsigned below = (1u << lane) - 1u;
 #pragma unroll 8
   for (int q = 0; q < IPT; ++q) {
-    int round = 0, mine = 0;
-    for (int x = 0; x < MB / 32; ++x) {
-      const int c = wcnt[q][x];
-      mine += x < w ? c : 0;
-      round += c;
-    }
     const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if ((bits >> q) & 1u) cand[before + mine + __popc(bal & below)] = q * MB + threadIdx.x;
-    before += round;
+    if ((bits >> q) & 1u) cand[slot[q * (MB / 32) + w] + __popc(bal & below)] = q * MB + threadIdx.x;
   }
   __syncthreads();
-  return before;
+  return (int)total;
 }
 
 // Node and element counts travel packed in one 64-bit word (nodes high, elements low; a block's
