@@ -391,6 +391,7 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   cci::DevTape tape{nullptr, 0, 0, 0};
   cudaError_t e;
+  ++h->generation;
   if (h->prec == CC_F64) {
     if (body && (st = upload_tape<double>(h, body, 3, s, &tape)) != CC_OK) return st;
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;

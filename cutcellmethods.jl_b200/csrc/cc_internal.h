@@ -125,6 +125,19 @@ cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* am
 }  // namespace cci
 
 // The library-side state of one cache (created at allocate_cache time, include/cutcell_b200.h).
+namespace cci {
+// What a marching-cubes generate_mesh count was taken from, so the emit call that follows can
+// start from its block offsets and survivors (mesh.cu).
+struct MeshKey {
+  bool valid = false;
+  uint64_t generation = 0;
+  const void* phi = nullptr;
+  cc_grid g{};
+  int prec = -1;
+  unsigned long long tot[3] = {0, 0, 0};
+};
+}  // namespace cci
+
 struct cc_handle {
   int device = 0, method = 0, dim = 3, prec = 0;
   int64_t n[3] = {0, 0, 0};
@@ -148,6 +161,7 @@ struct cc_handle {
   size_t prune_bytes = 0;
   void* ms_mesh = nullptr;  // marching squares: the last contour built (ms_mesh.cu)
   void* plic_mesh = nullptr;  // PLIC: the last surface count's block offsets (plic_mesh.cu)
+  cci::MeshKey mesh_key;      // marching cubes: what the kept mesh count was taken from
   uint64_t generation = 0;    // bumped by every update, so a stored count knows its planes are stale
 };
 

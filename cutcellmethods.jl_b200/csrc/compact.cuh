@@ -1,0 +1,93 @@
+// compact.cuh -- in-order block compaction for the surface extractors (mesh.cu, plic_mesh.cu).
+//
+// A surface pass visits every node or cell, but only a thin band (about one in a hundred at
+// 512^3) contributes anything, and that band's work (a clip, a tile, an edge walk) is long and
+// branchy. Run in place, it would leave 31 lanes of most warps waiting on one. So a block owns
+// BLK = MB * IPT consecutive items, taken round-major (round q covers items q*MB + [0, MB), one
+// per thread, so loads coalesce), tests them all cheaply with no barrier in between (their loads
+// overlap), and places the survivors' local indices in item order -- round, warp, lane -- into
+// shared memory, through warp ballots and one block scan of the per-(round, warp) counts. The
+// long work then runs over the survivors on dense warps, MB at a time, and an in-block scan per
+// chunk keeps the output in item order with no atomics.
+#pragma once
+#include <cstdint>
+
+namespace cccompact {
+
+// Exclusive scan of one value per thread over a block of MB threads; *total gets the sum.
+template <int MB>
+__device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long* total) {
+  __shared__ unsigned long long warp_sum[MB / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long v = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) warp_sum[w] = v;
+  __syncthreads();
+  unsigned long long base = 0, all = 0;
+  for (int q = 0; q < MB / 32; ++q) {
+    if (q < w) base += warp_sum[q];
+    all += warp_sum[q];
+  }
+  __syncthreads();
+  *total = all;
+  return base + v - x;
+}
+
+// Places in cand[0 .. n) (n returned, block-uniform) the local indices r = q*MB + threadIdx.x of
+// this block's items for which keep(q) is true, in increasing order. keep(q) is called by every
+// thread for q = 0 .. IPT-1 in order and must itself answer false past the block's last item.
+template <int MB, int IPT, class Keep>
+__device__ __forceinline__ int compact(int* cand, Keep keep) {
+  static_assert(IPT <= 32 && IPT * (MB / 32) == MB, "one bit per round; one (round, warp) slot per thread");
+  __shared__ int slot[MB];  // per (round, warp): its count, then its first position
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned bits = 0;
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q)
+    if (keep(q)) bits |= 1u << q;
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q) {
+    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+    if (lane == 0) slot[q * (MB / 32) + w] = __popc(bal);
+  }
+  __syncthreads();
+  unsigned long long total;
+  const unsigned long long first = block_scan<MB>((unsigned long long)slot[threadIdx.x], &total);
+  slot[threadIdx.x] = (int)first;  // block_scan's closing barrier ordered every read before this
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll 8
+  for (int q = 0; q < IPT; ++q) {
+    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+    if ((bits >> q) & 1u) cand[slot[q * (MB / 32) + w] + __popc(bal & below)] = q * MB + threadIdx.x;
+  }
+  __syncthreads();
+  return (int)total;
+}
+
+// In-place exclusive scan of `n` per-block counts (`lanes` interleaved series, lanes <= 4) in one
+// CTA of MB threads; totals[l] receives series l's sum.
+template <int MB>
+__global__ void scan_series_kernel(unsigned long long* a, long long n, int lanes, unsigned long long* totals) {
+  __shared__ unsigned long long carry[4];
+  if (threadIdx.x < 4) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int l = 0; l < lanes; ++l)
+    for (long long base = 0; base < n; base += MB) {
+      const long long q = base + threadIdx.x;
+      const unsigned long long x = q < n ? a[lanes * q + l] : 0ull;
+      unsigned long long t;
+      const unsigned long long pre = block_scan<MB>(x, &t);
+      if (q < n) a[lanes * q + l] = carry[l] + pre;
+      __syncthreads();
+      if (threadIdx.x == 0) carry[l] += t;
+      __syncthreads();
+    }
+  if (threadIdx.x < lanes) totals[threadIdx.x] = carry[threadIdx.x];
+}
+
+}  // namespace cccompact

@@ -289,6 +289,7 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
   Dev dg(h->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   cc_mlp* m = const_cast<cc_mlp*>(mlp);
+  ++h->generation;
   cudaError_t e = cudaMemsetAsync(m->fallback, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cc_mc_update_learned");
   // the fill pass alone (cut band listed), then the fused cut + network pass

@@ -12,9 +12,16 @@
 // The numbering is deterministic: first the edge vertices, each owned by its edge's lower node,
 // nodes in linear order (x fastest) and each node's x, y, z edges in that order; then the
 // interior vertices, cells in linear order; triangles by cell in linear order, each cell's in
-// tile order. Two passes of three kernels each count per block, scan the block totals and emit
-// through in-block scans. The edge pass keeps each node's first vertex, so a cell's triangles can
-// name the vertices of edges other nodes own.
+// tile order.
+//
+// Two passes, edge vertices (nodes) and cells. Each counts per block of 8192 items, the block
+// counts are scanned, and an emit writes through in-block scans; both compact the thin band that
+// contributes (nodes with a cut edge, cut cells) per block before the long work, so it runs on
+// dense warps (compact.cuh). The count call keeps each block's survivors and the scanned offsets
+// on the handle, and an emit call that follows it for the same phi and grid, with no update in
+// between, starts from them. The edge pass keeps each surviving node's first vertex, so a cell's
+// triangles can name the vertices of edges other nodes own. Every write of an emit is checked
+// against the output capacities.
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
@@ -22,6 +29,7 @@
 #include "cc_device.cuh"
 #include "cc_internal.h"
 #include "mc_cell.cuh"
+#include "compact.cuh"
 
 namespace {
 
@@ -31,8 +39,9 @@ using cci::DevGrid;
 using cci::DevTable;
 
 constexpr int MB = 256;          // threads per block
-constexpr int IPT = 16;          // items per thread
+constexpr int IPT = 32;          // rounds per block
 constexpr int BLK = MB * IPT;    // nodes or cells per block
+constexpr int KEEP = 1024;       // survivors a block hands from the count to the emit pass
 
 template <class T>
 __device__ __forceinline__ bool outside(T v) { return nudge(v) >= T(0); }
@@ -71,76 +80,106 @@ __device__ __forceinline__ void edge_vertex(const T* __restrict__ phi, const Dev
   for (int q = 0; q < 3; ++q) out[q] = fa >= T(0) ? xa[q] + s * (xb[q] - xa[q]) : xb[q] + s * (xa[q] - xb[q]);
 }
 
-// Exclusive scan of one value per thread over the block; returns the prefix, *total the sum.
-__device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long* total) {
-  __shared__ unsigned long long warp_sum[MB / 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned long long v = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += y;
+// Walks item coordinates (i, j, k) over an n0 x n1 x * box from item `start + threadIdx.x` in steps
+// of MB, one 64-bit division at the start.
+struct Walker {
+  long long v, i, j, k, n0, n1;
+  __device__ Walker(long long start, long long n0_, long long n1_) : n0(n0_), n1(n1_) {
+    v = start + threadIdx.x;
+    i = v % n0;
+    j = (v / n0) % n1;
+    k = v / (n0 * n1);
   }
-  if (lane == 31) warp_sum[w] = v;
-  __syncthreads();
-  unsigned long long base = 0, all = 0;
-  for (int q = 0; q < MB / 32; ++q) {
-    if (q < w) base += warp_sum[q];
-    all += warp_sum[q];
+  __device__ __forceinline__ void step() {
+    v += MB;
+    i += MB;
+    while (i >= n0) {
+      i -= n0;
+      if (++j == n1) { j = 0; ++k; }
+    }
   }
-  __syncthreads();
-  *total = all;
-  return base + v - x;
+};
+
+// This block's survivors: from the count pass (kept_n >= 0) or compacted again (kept_n < 0,
+// more than KEEP). Returns their number (block-uniform).
+template <class Keep>
+__device__ __forceinline__ int survivors(int* cand, const int* kept, const int* kept_n, Keep keep) {
+  int n = kept_n[blockIdx.x];
+  if (n == 0) return 0;
+  if (n > 0) {
+    for (int x = threadIdx.x; x < n; x += MB) cand[x] = kept[(size_t)blockIdx.x * KEEP + x];
+    __syncthreads();
+    return n;
+  }
+  return cccompact::compact<MB, IPT>(cand, keep);
+}
+
+__device__ __forceinline__ void keep_survivors(const int* cand, int n, int* kept, int* kept_n) {
+  if (threadIdx.x == 0) kept_n[blockIdx.x] = n <= KEEP ? n : -1;
+  if (n <= KEEP)
+    for (int x = threadIdx.x; x < n; x += MB) kept[(size_t)blockIdx.x * KEEP + x] = cand[x];
 }
 
 // ---- the edge vertices ----------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(MB) node_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                        unsigned long long* bsum) {
+__global__ void __launch_bounds__(MB, 4) node_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                           unsigned long long* bsum, int* kept, int* kept_n) {
+  __shared__ int cand[BLK];
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
-  const long long v0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  const long long start = (long long)blockIdx.x * BLK;
+  Walker w(start, nx, ny);
+  const int n = cccompact::compact<MB, IPT>(cand, [&](int) {
+    const bool r = w.v < nn && node_edges(phi, w.i, w.j, w.k, g.n) != 0u;
+    w.step();
+    return r;
+  });
+  keep_survivors(cand, n, kept, kept_n);
   unsigned long long c = 0;
-  for (int q = 0; q < IPT; ++q) {
-    const long long v = v0 + q;
-    if (v < nn) c += __popc(node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n));
+  for (int x = threadIdx.x; x < n; x += MB) {
+    const long long v = start + cand[x];
+    c += __popc(node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n));
   }
   unsigned long long total;
-  block_scan(c, &total);
+  cccompact::block_scan<MB>(c, &total);
   if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
 template <class T>
-__global__ void __launch_bounds__(MB) node_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                       const unsigned long long* __restrict__ boff,
-                                                       unsigned* __restrict__ vbase, T* __restrict__ verts) {
+__global__ void __launch_bounds__(MB, 4) node_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                          const unsigned long long* __restrict__ boff,
+                                                          const int* kept, const int* kept_n, unsigned* __restrict__ vbase,
+                                                          T* __restrict__ verts, unsigned long long vcap,
+                                                          unsigned long long* overflow) {
+  __shared__ int cand[BLK];
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
-  const long long v0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
-  unsigned m[IPT];
-  unsigned long long c = 0;
-#pragma unroll
-  for (int q = 0; q < IPT; ++q) {
-    const long long v = v0 + q;
-    m[q] = v < nn ? node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n) : 0u;
-    c += __popc(m[q]);
-  }
-  unsigned long long total;
-  unsigned long long id = boff[blockIdx.x] + block_scan(c, &total);
-#pragma unroll
-  for (int q = 0; q < IPT; ++q) {
-    const long long v = v0 + q;
-    if (v >= nn) break;
+  const long long start = (long long)blockIdx.x * BLK;
+  Walker w(start, nx, ny);
+  const int n = survivors(cand, kept, kept_n, [&](int) {
+    const bool r = w.v < nn && node_edges(phi, w.i, w.j, w.k, g.n) != 0u;
+    w.step();
+    return r;
+  });
+  unsigned long long run = boff[blockIdx.x];
+  for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
+    const int x = c0 + threadIdx.x;
+    const long long v = x < n ? start + cand[x] : 0;
+    const long long i = v % nx, j = (v / nx) % ny, k = v / (nx * ny);
+    const unsigned m = x < n ? node_edges(phi, i, j, k, g.n) : 0u;
+    unsigned long long total;
+    unsigned long long id = run + cccompact::block_scan<MB>((unsigned long long)__popc(m), &total);
+    run += total;
+    if (x >= n) continue;
+    if (id + __popc(m) > vcap) {
+      atomicOr(overflow, 1ull);
+      continue;
+    }
     vbase[v] = unsigned(id);
-    if (verts) {
-      const long long i = v % nx, j = (v / nx) % ny, k = v / (nx * ny);
-      for (int a = 0; a < 3; ++a) {
-        if (!(m[q] >> a & 1u)) continue;
-        T p[3];
-        edge_vertex(phi, g, i, j, k, a, p);
-        verts[3 * id] = p[0]; verts[3 * id + 1] = p[1]; verts[3 * id + 2] = p[2];
-        ++id;
-      }
-    } else {
-      id += __popc(m[q]);
+    for (int a = 0; a < 3; ++a) {
+      if (!(m >> a & 1u)) continue;
+      T p[3];
+      edge_vertex(phi, g, i, j, k, a, p);
+      verts[3 * id] = p[0]; verts[3 * id + 1] = p[1]; verts[3 * id + 2] = p[2];
+      ++id;
     }
   }
 }
@@ -155,6 +194,18 @@ __device__ __forceinline__ void corners(const T* __restrict__ phi, const long lo
                   phi[b0 + bz], phi[b0 + bz + 1], phi[b0 + bz + nx + 1], phi[b0 + bz + nx]};
 #pragma unroll
   for (int c = 0; c < 8; ++c) ph[c] = nudge(r[c]);
+}
+
+// A cell is cut when its corners are not all on one side.
+template <class T>
+__device__ __forceinline__ bool cell_cut(const T* __restrict__ phi, const long long n[3], long long i, long long j,
+                                         long long k) {
+  T ph[8];
+  corners(phi, n, i, j, k, ph);
+  int nout = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) nout += ph[c] >= T(0) ? 1 : 0;
+  return nout != 0 && nout != 8;
 }
 
 // A cell's triangle count and whether its tile uses the interior vertex (code 13); -1 tile if
@@ -176,14 +227,22 @@ __device__ __forceinline__ int cell_tile(const T ph[8], const DevTable& tb, int&
 }
 
 template <class T, bool MX>
-__global__ void __launch_bounds__(MB) cell_count_kernel(const T* __restrict__ phi, const DevGrid<T> g, const DevTable tb,
-                                                        unsigned long long* bsum) {
+__global__ void __launch_bounds__(MB, 4) cell_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                           const DevTable tb, unsigned long long* bsum, int* kept,
+                                                           int* kept_n) {
+  __shared__ int cand[BLK];
   const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
-  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
+  const long long start = (long long)blockIdx.x * BLK;
+  Walker w(start, n0, n1);
+  const int n = cccompact::compact<MB, IPT>(cand, [&](int) {
+    const bool r = w.v < nc && cell_cut(phi, g.n, w.i, w.j, w.k);
+    w.step();
+    return r;
+  });
+  keep_survivors(cand, n, kept, kept_n);
   unsigned long long t = 0, in = 0;
-  for (int q = 0; q < IPT; ++q) {
-    const long long c = c0 + q;
-    if (c >= nc) break;
+  for (int x = threadIdx.x; x < n; x += MB) {
+    const long long c = start + cand[x];
     T ph[8];
     corners(phi, g.n, c % n0, (c / n0) % n1, c / (n0 * n1), ph);
     int nt, it;
@@ -192,8 +251,8 @@ __global__ void __launch_bounds__(MB) cell_count_kernel(const T* __restrict__ ph
     in += it;
   }
   unsigned long long tt, ti;
-  block_scan(t, &tt);
-  block_scan(in, &ti);
+  cccompact::block_scan<MB>(t, &tt);
+  cccompact::block_scan<MB>(in, &ti);
   if (threadIdx.x == 0) {
     bsum[2 * blockIdx.x] = tt;
     bsum[2 * blockIdx.x + 1] = ti;
@@ -201,41 +260,52 @@ __global__ void __launch_bounds__(MB) cell_count_kernel(const T* __restrict__ ph
 }
 
 template <class T, bool MX>
-__global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g, const DevTable tb,
-                                                       const unsigned long long* __restrict__ boff,
-                                                       const unsigned* __restrict__ vbase, unsigned long long n_edge_verts,
-                                                       T* __restrict__ verts, int32_t* __restrict__ tris,
-                                                       int64_t* __restrict__ tri_cells) {
+__global__ void __launch_bounds__(MB, 4) cell_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                          const DevTable tb, const unsigned long long* __restrict__ boff,
+                                                          const int* kept, const int* kept_n,
+                                                          const unsigned* __restrict__ vbase,
+                                                          unsigned long long n_edge_verts, T* __restrict__ verts,
+                                                          unsigned long long vcap, int32_t* __restrict__ tris,
+                                                          unsigned long long tcap, int64_t* __restrict__ tri_cells,
+                                                          unsigned long long* overflow) {
+  __shared__ int cand[BLK];
   const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
-  const long long c0 = (long long)blockIdx.x * BLK + (long long)threadIdx.x * IPT;
-  unsigned long long t = 0, in = 0;
-  for (int q = 0; q < IPT; ++q) {
-    const long long c = c0 + q;
-    if (c >= nc) break;
-    T ph[8];
-    corners(phi, g.n, c % n0, (c / n0) % n1, c / (n0 * n1), ph);
-    int nt, it;
-    cell_tile<T, MX>(ph, tb, nt, it);
-    t += nt;
-    in += it;
-  }
-  unsigned long long tt, ti;
-  unsigned long long tri_id = boff[2 * blockIdx.x] + block_scan(t, &tt);
-  unsigned long long int_id = n_edge_verts + boff[2 * blockIdx.x + 1] + block_scan(in, &ti);
-  for (int q = 0; q < IPT; ++q) {
-    const long long c = c0 + q;
-    if (c >= nc) break;
+  const long long start = (long long)blockIdx.x * BLK;
+  Walker w(start, n0, n1);
+  const int n = survivors(cand, kept, kept_n, [&](int) {
+    const bool r = w.v < nc && cell_cut(phi, g.n, w.i, w.j, w.k);
+    w.step();
+    return r;
+  });
+  unsigned long long run_t = boff[2 * blockIdx.x], run_i = n_edge_verts + boff[2 * blockIdx.x + 1];
+  for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
+    const int x = c0 + threadIdx.x;
+    const long long c = x < n ? start + cand[x] : 0;
     const long long i = c % n0, j = (c / n0) % n1, k = c / (n0 * n1);
     T ph[8];
-    corners(phi, g.n, i, j, k, ph);
-    int nt, it;
-    const int tile = cell_tile<T, MX>(ph, tb, nt, it);
+    int nt = 0, it = 0, tile = -1;
+    if (x < n) {
+      corners(phi, g.n, i, j, k, ph);
+      tile = cell_tile<T, MX>(ph, tb, nt, it);
+    }
+    unsigned long long tot;
+    const unsigned long long pre =
+        cccompact::block_scan<MB>(((unsigned long long)nt << 32) | (unsigned long long)it, &tot);
+    unsigned long long tri_id = run_t + (pre >> 32), int_id = run_i + (pre & 0xffffffffull);
+    run_t += tot >> 32;
+    run_i += tot & 0xffffffffull;
     if (tile < 0) continue;
-    // the vertex of each of the cell's twelve edges (code e + 1), from its lower node's numbering
+    if (tri_id + nt > tcap || (it && int_id >= vcap)) {
+      atomicOr(overflow, 1ull);
+      continue;
+    }
+    // the vertex of each of the cell's cut edges (code e + 1), from its lower node's numbering
     unsigned vid[12];
 #pragma unroll
     for (int e = 0; e < 12; ++e) {
       const int ca = edge_node(e, 0), cb = edge_node(e, 1);
+      vid[e] = 0;
+      if ((ph[ca] >= T(0)) == (ph[cb] >= T(0))) continue;
       const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
       const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
       const long long li = i + cbit(lo, 0), lj = j + cbit(lo, 1), lk = k + cbit(lo, 2);
@@ -245,7 +315,7 @@ __global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi
     }
     unsigned centre = 0;
     if (it) {
-      centre = unsigned(int_id++);
+      centre = unsigned(int_id);
       T acc[3] = {T(0), T(0), T(0)};
       int ncr = 0;
       for (int e = 0; e < 12; ++e) {
@@ -258,11 +328,9 @@ __global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi
         acc[0] = acc[0] + p[0]; acc[1] = acc[1] + p[1]; acc[2] = acc[2] + p[2];
         ++ncr;
       }
-      if (verts) {
-        verts[3 * (long long)centre] = acc[0] / T(ncr);
-        verts[3 * (long long)centre + 1] = acc[1] / T(ncr);
-        verts[3 * (long long)centre + 2] = acc[2] / T(ncr);
-      }
+      verts[3 * (long long)centre] = acc[0] / T(ncr);
+      verts[3 * (long long)centre + 1] = acc[1] / T(ncr);
+      verts[3 * (long long)centre + 2] = acc[2] / T(ncr);
     }
     const cc_mc_tile tl = tb.tiles[tile];
     const uint8_t* codes = tb.codes + tl.code_off;
@@ -275,27 +343,6 @@ __global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi
       if (tri_cells) tri_cells[tri_id] = c;
     }
   }
-}
-
-// Exclusive scan of `n` per-block counts (stride values apart, `lanes` interleaved series) in one
-// CTA, in place; totals[l] receives series l's sum.
-__global__ void scan_blocks_kernel(unsigned long long* a, long long n, int lanes, unsigned long long* totals) {
-  __shared__ unsigned long long carry[4];
-  if (threadIdx.x < 4) carry[threadIdx.x] = 0;
-  __syncthreads();
-  for (int l = 0; l < lanes; ++l) {
-    for (long long base = 0; base < n; base += MB) {
-      const long long q = base + threadIdx.x;
-      const unsigned long long x = q < n ? a[q * lanes + l] : 0ull;
-      unsigned long long total;
-      const unsigned long long pre = block_scan(x, &total);
-      if (q < n) a[q * lanes + l] = carry[l] + pre;
-      __syncthreads();
-      if (threadIdx.x == 0) carry[l] += total;
-      __syncthreads();
-    }
-  }
-  if (threadIdx.x < lanes) totals[threadIdx.x] = carry[threadIdx.x];
 }
 
 cc_status fail(cc_status s, const std::string& m) {
@@ -326,20 +373,27 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
   const long long nc = g.n[0] * g.n[1] * g.n[2];
   const long long nbn = (nn + BLK - 1) / BLK, nbc = (nc + BLK - 1) / BLK;
   if (nn > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 nodes");
+  cci::MeshKey& key = h->mesh_key;
   cudaError_t e = cudaSuccess;
   if (size_t(nn) > h->mesh_vbase_n) {
     if (h->mesh_vbase) cudaFree(h->mesh_vbase);
     h->mesh_vbase = nullptr;
     h->mesh_vbase_n = 0;
+    key.valid = false;
     if ((e = cudaMalloc(&h->mesh_vbase, size_t(nn) * sizeof(unsigned))) != cudaSuccess)
       return cuda_fail(e, "generate_mesh scratch");
     h->mesh_vbase_n = size_t(nn);
   }
-  const size_t scan_n = size_t(nbn + 2 * nbc + 8);
+  // 64-bit words: node block offsets, cell block offsets (tris, interior) interleaved, 3 totals,
+  // the overflow flag; then 32-bit: node kept_n, node kept, cell kept_n, cell kept
+  const size_t words = size_t(nbn + 2 * nbc + 4);
+  const size_t ints = size_t(nbn) * (KEEP + 1) + size_t(nbc) * (KEEP + 1);
+  const size_t scan_n = words + (ints + 1) / 2;
   if (scan_n > h->mesh_scan_n) {
     if (h->mesh_scan) cudaFree(h->mesh_scan);
     h->mesh_scan = nullptr;
     h->mesh_scan_n = 0;
+    key.valid = false;
     if ((e = cudaMalloc(&h->mesh_scan, scan_n * sizeof(unsigned long long))) != cudaSuccess)
       return cuda_fail(e, "generate_mesh scratch");
     h->mesh_scan_n = scan_n;
@@ -347,25 +401,54 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
   unsigned long long* nb = h->mesh_scan;              // node blocks
   unsigned long long* cb = nb + nbn;                  // cell blocks (tris, interior) interleaved
   unsigned long long* tot = cb + 2 * nbc;             // edge vertices, tris, interior vertices
-  node_count_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb);
-  scan_blocks_kernel<<<1, MB, 0, s>>>(nb, nbn, 1, tot);
-  cell_count_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb);
-  scan_blocks_kernel<<<1, MB, 0, s>>>(cb, nbc, 2, tot + 1);
-  unsigned long long t[3];
-  if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(t, tot, sizeof t, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return cuda_fail(e, "generate_mesh count");
+  unsigned long long* overflow = tot + 3;
+  int* node_kept_n = reinterpret_cast<int*>(h->mesh_scan + words);
+  int* node_kept = node_kept_n + nbn;
+  int* cell_kept_n = node_kept + size_t(nbn) * KEEP;
+  int* cell_kept = cell_kept_n + nbc;
+  const bool emit = verts || tris;
+  bool reuse = emit && key.valid && key.generation == h->generation && key.phi == phi && key.prec == h->prec;
+  for (int a = 0; a < 3 && reuse; ++a)
+    reuse = key.g.n[a] == gg->n[a] && key.g.x0[a] == gg->x0[a] && key.g.d[a] == gg->d[a];
+  unsigned long long t[3] = {key.tot[0], key.tot[1], key.tot[2]};
+  if (!reuse) {
+    key.valid = false;
+    node_count_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, node_kept, node_kept_n);
+    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(nb, nbn, 1, tot);
+    cell_count_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, cell_kept, cell_kept_n);
+    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(cb, nbc, 2, tot + 1);
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(t, tot, sizeof t, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "generate_mesh count");
+    key.valid = true;
+    key.generation = h->generation;
+    key.phi = phi;
+    key.prec = h->prec;
+    key.g = *gg;
+    for (int q = 0; q < 3; ++q) key.tot[q] = t[q];
+  }
   const long long n_vert = (long long)(t[0] + t[2]), n_tri = (long long)t[1];
   if (nv) *nv = n_vert;
   if (nt) *nt = n_tri;
-  if (!verts && !tris) return CC_OK;  // counting only
+  if (!emit) return CC_OK;  // counting only
   if (!verts || !tris || vcap < n_vert || tcap < n_tri)
     return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
   if (n_vert > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 vertices");
-  node_emit_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, h->mesh_vbase, verts);
-  cell_emit_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, h->mesh_vbase, t[0], verts, tris, tri_cells);
-  if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(s);
+  unsigned long long flag = 0;
+  e = cudaMemsetAsync(overflow, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) {
+    node_emit_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, node_kept, node_kept_n, h->mesh_vbase, verts,
+                                                     (unsigned long long)vcap, overflow);
+    cell_emit_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, cell_kept, cell_kept_n, h->mesh_vbase, t[0],
+                                                         verts, (unsigned long long)vcap, tris,
+                                                         (unsigned long long)tcap, tri_cells, overflow);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, overflow, sizeof flag, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  key.valid = false;  // one emit per count
   if (e != cudaSuccess) return cuda_fail(e, "generate_mesh emit");
+  if (flag) return fail(CC_BAD_ARG, "generate_mesh: phi changed between the count and the emit call");
   return CC_OK;
 }
 
