@@ -27,6 +27,7 @@
 #include "../../include/cutcell_b200.h"
 #include "cc_device.cuh"
 #include "cc_internal.h"
+#include "compact.cuh"
 
 namespace {
 
@@ -191,47 +192,6 @@ __device__ __forceinline__ void cell_counts(const PlicIn<T, D>& P, int m, const 
   }
 }
 
-// Exclusive scan of x over the block; *total gets the block's sum.
-__device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long* total) {
-  __shared__ unsigned long long warp_sum[MB / 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned long long v = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += y;
-  }
-  if (lane == 31) warp_sum[w] = v;
-  __syncthreads();
-  unsigned long long base = 0, all = 0;
-  for (int q = 0; q < MB / 32; ++q) {
-    if (q < w) base += warp_sum[q];
-    all += warp_sum[q];
-  }
-  __syncthreads();
-  *total = all;
-  return base + v - x;
-}
-
-// In-place exclusive scan of the per-block (nodes, elements) pairs; the totals go to total[0..1].
-__global__ void scan2_kernel(unsigned long long* a, long long n, unsigned long long* total) {
-  __shared__ unsigned long long carry[2];
-  if (threadIdx.x < 2) carry[threadIdx.x] = 0;
-  __syncthreads();
-  for (int l = 0; l < 2; ++l)
-    for (long long base = 0; base < n; base += MB) {
-      const long long q = base + threadIdx.x;
-      const unsigned long long x = q < n ? a[2 * q + l] : 0ull;
-      unsigned long long t;
-      const unsigned long long pre = block_scan(x, &t);
-      if (q < n) a[2 * q + l] = carry[l] + pre;
-      __syncthreads();
-      if (threadIdx.x == 0) carry[l] += t;
-      __syncthreads();
-    }
-  if (threadIdx.x < 2) total[threadIdx.x] = carry[threadIdx.x];
-}
-
 // True when entry k certainly draws nothing: a degenerate fit, or a plane that misses its cell
 // by more than rounding (3D), or -- in 2D -- such a miss when the length floor drops the
 // zero-length segment it leaves. Conservative: a true here implies clip_cell + cell_counts give no
@@ -254,48 +214,19 @@ __device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, const T* nr
   return !ok || miss;
 }
 
-// Each block owns BLK consecutive entries, taken round-major (round q covers entries
-// blk*BLK + q*MB + [0, MB), one per thread, so the plane loads coalesce). Pass 1 tests all IPT
-// rounds with no barrier in between (their loads overlap) into a bit mask, and the entries that
-// may draw something are placed in entry order -- round, then warp, then lane -- into shared memory
-// through warp ballots and one table of per-(round, warp) counts. Pass 2 (the caller) runs the full
-// clip over the compacted entries, MB at a time, so the long path runs on dense warps rather than
-// one lane of many. Returns the number of compacted entries (block-uniform).
+// A block's entries that may draw something, in entry order, into cand (compact.cuh).
 template <class T, int D>
 __device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d, int* cand) {
-  static_assert(IPT <= 32 && IPT * (MB / 32) == MB, "one bit per round; one (round, warp) slot per thread");
-  __shared__ int slot[IPT * (MB / 32)];  // per (round, warp): its count, then its first position
   const long long start = (long long)blockIdx.x * BLK;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   // this block's entries, addressed by 32-bit offsets
   const int here = P.count - start < BLK ? int(P.count - start) : BLK;
   const T* nrm = P.normals + D * start;
   const T* icp = P.intercepts + start;
   const uint8_t* val = P.valid ? P.valid + start : nullptr;
-  unsigned bits = 0;
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q) {
+  return cccompact::compact<MB, IPT>(cand, [&](int q) {
     const int r = q * MB + threadIdx.x;
-    if (r < here && !draws_nothing<T, D>(P, nrm, icp, val, r, min_d)) bits |= 1u << q;
-  }
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q) {
-    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if (lane == 0) slot[q * (MB / 32) + w] = __popc(bal);
-  }
-  __syncthreads();
-  unsigned long long total;
-  const unsigned long long first = block_scan((unsigned long long)slot[threadIdx.x], &total);
-  slot[threadIdx.x] = (int)first;  // block_scan's closing barrier ordered every read before this
-  __syncthreads();
-  const unsigned below = (1u << lane) - 1u;
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q) {
-    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if ((bits >> q) & 1u) cand[slot[q * (MB / 32) + w] + __popc(bal & below)] = q * MB + threadIdx.x;
-  }
-  __syncthreads();
-  return (int)total;
+    return r < here && !draws_nothing<T, D>(P, nrm, icp, val, r, min_d);
+  });
 }
 
 // Node and element counts travel packed in one 64-bit word (nodes high, elements low; a block's
@@ -321,7 +252,7 @@ __global__ void __launch_bounds__(MB, 5) plic_count_kernel(const PlicIn<T, D> P,
     packed += ((unsigned long long)a << 32) | (unsigned long long)b;
   }
   unsigned long long t;
-  block_scan(packed, &t);
+  cccompact::block_scan<MB>(packed, &t);
   if (threadIdx.x == 0) { bsum[2 * blockIdx.x] = t >> 32; bsum[2 * blockIdx.x + 1] = t & 0xffffffffull; }
 }
 
@@ -355,7 +286,7 @@ __global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, T m
       cell_counts<T, D>(P, m, p, min_d, a, b, keep);
     }
     unsigned long long t;
-    const unsigned long long pre = block_scan(((unsigned long long)a << 32) | (unsigned long long)b, &t);
+    const unsigned long long pre = cccompact::block_scan<MB>(((unsigned long long)a << 32) | (unsigned long long)b, &t);
     unsigned long long vn = run_n + (pre >> 32), ve = run_e + (pre & 0xffffffffull);
     run_n += t >> 32;
     run_e += t & 0xffffffffull;
@@ -476,7 +407,7 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
   if (!reuse) {
     st->valid = false;
     plic_count_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, kept, kept_n);
-    scan2_kernel<<<1, MB, 0, s>>>(bsum, nb, bsum + 2 * nb);
+    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(bsum, nb, 2, bsum + 2 * nb);
     if ((e = cudaGetLastError()) == cudaSuccess)
       e = cudaMemcpyAsync(tot, bsum + 2 * nb, sizeof tot, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

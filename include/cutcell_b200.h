@@ -275,7 +275,11 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
  * (the cell of each triangle; may be NULL). Order: edge vertices by lower node (linear, x fastest)
  * then axis x, y, z; then interior vertices by cell; triangles by cell, each cell's in tile order.
  * Call with vertices = triangles = NULL to count; then with arrays of at least the counted
- * sizes. Blocking. Scratch: 4 bytes per node, kept on the handle. */
+ * sizes. Blocking. The handle keeps the counting call's per-block results: an emitting call that
+ * follows it with the same phi pointer and grid, and no update in between, skips the second
+ * count. phi must not be written between the two calls; an emit that would then run past the
+ * counted capacities writes nothing beyond them and returns CC_BAD_ARG. Scratch kept on the
+ * handle: 4 bytes per node, plus about 1 byte per node and per cell for the kept counts. */
 cc_status cc_mc_mesh(cc_handle* h, const cc_grid* g, const void* phi, void* vertices, int64_t vertex_capacity,
                      int32_t* triangles, int64_t triangle_capacity, int64_t* triangle_cells,
                      int64_t* n_vertices, int64_t* n_triangles, void* stream);

@@ -110,3 +110,37 @@ def test_ms_contour_length_and_orientation():
     assert np.array_equal(np.sort(e[:, 0]), np.arange(v.shape[0])) and np.array_equal(np.sort(e[:, 1]), np.arange(v.shape[0]))
     with pytest.raises(cc.DimensionMismatch):
         S.generate_mesh(cache, cc.CartesianIsoGrid((-1.0, -1.0), (1.01, 1.0), 0.01))
+
+
+def test_count_then_emit_reuse_and_changed_phi():
+    """The handle keeps the count for the emit call that follows it; a phi written between the two
+    calls makes the emit fail cleanly (its writes are checked against the counted capacities), and
+    the next generate_mesh counts afresh."""
+    import ctypes as C
+    L = __import__("cutcell_b200._lib", fromlist=["_lib"])
+    cache_mod = __import__("cutcell_b200.cache", fromlist=["cache"])
+    g = cc.grid3(40)
+    cache = cache_for(g, cc.Sphere((0.01, 0.02, -0.03), 1.0), 1)
+    first = S.generate_mesh(cache, g)
+    again = S.generate_mesh(cache, g)
+    assert torch.equal(first.nodes, again.nodes) and torch.equal(first.elements, again.elements)
+    lib = cache.handle.lib
+    gs = cache_mod.grid_struct(g)
+    nv, nt = C.c_int64(0), C.c_int64(0)
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.cc_mc_mesh(cache.handle.h, C.byref(gs), cache.phi.data_ptr(), None, 0, None, 0, None,
+                          C.byref(nv), C.byref(nt), s) == 0
+    assert (nv.value, nt.value) == (first.nodes.shape[0], first.elements.shape[0])
+    verts = torch.empty(nv.value, 3, dtype=torch.float64, device="cuda")
+    tris = torch.empty(nt.value, 3, dtype=torch.int32, device="cuda")
+    cells = torch.empty(nt.value, dtype=torch.int64, device="cuda")
+    saved = cache.phi.clone()
+    # a field that changes sign between every pair of nodes: far more surface than was counted
+    idx = torch.arange(cache.phi.numel(), device="cuda")
+    cache.phi.copy_(torch.where(idx % 2 == 0, 1.0, -1.0).to(cache.phi.dtype))
+    rc = lib.cc_mc_mesh(cache.handle.h, C.byref(gs), cache.phi.data_ptr(), verts.data_ptr(), nv.value,
+                        tris.data_ptr(), nt.value, cells.data_ptr(), C.byref(nv), C.byref(nt), s)
+    assert rc == L.CC_BAD_ARG
+    cache.phi.copy_(saved)
+    after = S.generate_mesh(cache, g)
+    assert torch.equal(first.nodes, after.nodes) and torch.equal(first.elements, after.elements)
