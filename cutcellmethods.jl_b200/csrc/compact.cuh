@@ -38,17 +38,20 @@ __device__ __forceinline__ unsigned long long block_scan(unsigned long long x, u
 }
 
 // Places in cand[0 .. n) (n returned, block-uniform) the local indices r = q*MB + threadIdx.x of
-// this block's items for which keep(q) is true, in increasing order. keep(q) is called by every
-// thread for q = 0 .. IPT-1 in order and must itself answer false past the block's last item.
-template <int MB, int IPT, class Keep>
+// this block's items that are kept, in increasing order. keep(q0) is called by every thread for
+// q0 = 0, G, 2G, .. in order and returns the kept bits of rounds q0 .. q0+G-1 (bit u for round
+// q0+u), answering 0 past the block's last item. A group is the unit of memory-level parallelism:
+// keep should issue all of its G rounds' loads (from clamped, always valid addresses) before
+// testing any, so a round does not wait on the one before it.
+template <int MB, int IPT, int G, class Keep>
 __device__ __forceinline__ int compact(int* cand, Keep keep) {
   static_assert(IPT <= 32 && IPT * (MB / 32) == MB, "one bit per round; one (round, warp) slot per thread");
+  static_assert(IPT % G == 0, "whole groups");
   __shared__ int slot[MB];  // per (round, warp): its count, then its first position
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned bits = 0;
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q)
-    if (keep(q)) bits |= 1u << q;
+#pragma unroll 1
+  for (int q0 = 0; q0 < IPT; q0 += G) bits |= keep(q0) << q0;
 #pragma unroll 8
   for (int q = 0; q < IPT; ++q) {
     const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);

@@ -81,28 +81,104 @@ __device__ __forceinline__ void edge_vertex(const T* __restrict__ phi, const Dev
 }
 
 // Walks item coordinates (i, j, k) over an n0 x n1 x * box from item `start + threadIdx.x` in steps
-// of MB, one 64-bit division at the start.
+// of MB (one 64-bit division at the start), carrying the item's node index b = i + sx j + sz k
+// (for the node box, b is the item itself; for the cell box, the cell's lower corner). The steps
+// are arithmetic only, so the loads they address do not wait on one another.
 struct Walker {
-  long long v, i, j, k, n0, n1;
-  __device__ Walker(long long start, long long n0_, long long n1_) : n0(n0_), n1(n1_) {
+  long long v, b;
+  int i, j, k;
+  const int n0, n1;
+  const long long sx, sz;
+  __device__ Walker(long long start, long long n0_, long long n1_, long long sx_, long long sz_)
+      : n0(int(n0_)), n1(int(n1_)), sx(sx_), sz(sz_) {
     v = start + threadIdx.x;
-    i = v % n0;
-    j = (v / n0) % n1;
-    k = v / (n0 * n1);
+    i = int(v % n0_);
+    j = int((v / n0_) % n1_);
+    k = int(v / (n0_ * n1_));
+    b = i + sx * j + sz * k;
   }
   __device__ __forceinline__ void step() {
     v += MB;
     i += MB;
+    b += MB;
     while (i >= n0) {
       i -= n0;
-      if (++j == n1) { j = 0; ++k; }
+      b += sx - n0;
+      if (++j == n1) {
+        j = 0;
+        ++k;
+        b += sz - sx * n1;
+      }
     }
   }
 };
 
+// outside(v) without the nudge: |v| < eps reads as +eps, so v is outside exactly when v > -eps
+// (a NaN is neither).
+template <class T>
+__device__ __forceinline__ bool out_fast(T v) { return v > -Eps<T>::v(); }
+
+// The cheap tests, in groups of G rounds: each round's item is clamped to the box's last item
+// (past it the round answers false), and every load of the group is issued before any is tested.
+// A node has a cut edge when a neighbour along +x, +y or +z (inside the box) lies on the other side;
+// a cell is cut when its corners are not all on one side.
+template <class T, int G>
+__device__ __forceinline__ unsigned nodes_with_cut(const T* __restrict__ phi, Walker& w, long long nn,
+                                                   const long long n[3], long long nx, long long nz) {
+  T p0[G], px[G], py[G], pz[G];
+  bool in[G];
+#pragma unroll
+  for (int u = 0; u < G; ++u) {
+    in[u] = w.v < nn;
+    const long long b = in[u] ? w.b : nn - 1;
+    const T* p = phi + b;
+    p0[u] = p[0];
+    px[u] = p[in[u] && w.i < n[0] ? 1 : 0];
+    py[u] = p[in[u] && w.j < n[1] ? nx : 0];
+    pz[u] = p[in[u] && w.k < n[2] ? nz : 0];
+    w.step();
+  }
+  unsigned m = 0;
+#pragma unroll
+  for (int u = 0; u < G; ++u) {
+    const bool o = out_fast(p0[u]);
+    const bool cut = (out_fast(px[u]) != o) | (out_fast(py[u]) != o) | (out_fast(pz[u]) != o);
+    if (in[u] & cut) m |= 1u << u;
+  }
+  return m;
+}
+
+template <class T, int G>
+__device__ __forceinline__ unsigned cells_with_cut(const T* __restrict__ phi, Walker& w, long long nc, long long nx,
+                                                   long long nz) {
+  T c[G][8];
+  bool in[G];
+#pragma unroll
+  for (int u = 0; u < G; ++u) {
+    in[u] = w.v < nc;
+    const T* p = phi + (in[u] ? w.b : 0);
+    c[u][0] = p[0]; c[u][1] = p[1]; c[u][2] = p[nx]; c[u][3] = p[nx + 1];
+    c[u][4] = p[nz]; c[u][5] = p[nz + 1]; c[u][6] = p[nz + nx]; c[u][7] = p[nz + nx + 1];
+    w.step();
+  }
+  unsigned m = 0;
+#pragma unroll
+  for (int u = 0; u < G; ++u) {
+    const bool o = out_fast(c[u][0]);
+    bool cut = false;
+#pragma unroll
+    for (int q = 1; q < 8; ++q) cut |= out_fast(c[u][q]) != o;
+    if (in[u] & cut) m |= 1u << u;
+  }
+  return m;
+}
+
+template <class T> struct Groups { static constexpr int node = 8, cell = 4; };
+template <> struct Groups<double> { static constexpr int node = 4, cell = 2; };
+
 // This block's survivors: from the count pass (kept_n >= 0) or compacted again (kept_n < 0,
 // more than KEEP). Returns their number (block-uniform).
-template <class Keep>
+template <int G, class Keep>
 __device__ __forceinline__ int survivors(int* cand, const int* kept, const int* kept_n, Keep keep) {
   int n = kept_n[blockIdx.x];
   if (n == 0) return 0;
@@ -111,7 +187,7 @@ __device__ __forceinline__ int survivors(int* cand, const int* kept, const int* 
     __syncthreads();
     return n;
   }
-  return cccompact::compact<MB, IPT>(cand, keep);
+  return cccompact::compact<MB, IPT, G>(cand, keep);
 }
 
 __device__ __forceinline__ void keep_survivors(const int* cand, int n, int* kept, int* kept_n) {
@@ -127,12 +203,9 @@ __global__ void __launch_bounds__(MB, 4) node_count_kernel(const T* __restrict__
   __shared__ int cand[BLK];
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
   const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, nx, ny);
-  const int n = cccompact::compact<MB, IPT>(cand, [&](int) {
-    const bool r = w.v < nn && node_edges(phi, w.i, w.j, w.k, g.n) != 0u;
-    w.step();
-    return r;
-  });
+  Walker w(start, nx, ny, nx, nx * ny);
+  const int n = cccompact::compact<MB, IPT, Groups<T>::node>(
+      cand, [&](int) { return nodes_with_cut<T, Groups<T>::node>(phi, w, nn, g.n, nx, nx * ny); });
   keep_survivors(cand, n, kept, kept_n);
   unsigned long long c = 0;
   for (int x = threadIdx.x; x < n; x += MB) {
@@ -153,12 +226,9 @@ __global__ void __launch_bounds__(MB, 4) node_emit_kernel(const T* __restrict__ 
   __shared__ int cand[BLK];
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
   const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, nx, ny);
-  const int n = survivors(cand, kept, kept_n, [&](int) {
-    const bool r = w.v < nn && node_edges(phi, w.i, w.j, w.k, g.n) != 0u;
-    w.step();
-    return r;
-  });
+  Walker w(start, nx, ny, nx, nx * ny);
+  const int n = survivors<Groups<T>::node>(
+      cand, kept, kept_n, [&](int) { return nodes_with_cut<T, Groups<T>::node>(phi, w, nn, g.n, nx, nx * ny); });
   unsigned long long run = boff[blockIdx.x];
   for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
     const int x = c0 + threadIdx.x;
@@ -196,18 +266,6 @@ __device__ __forceinline__ void corners(const T* __restrict__ phi, const long lo
   for (int c = 0; c < 8; ++c) ph[c] = nudge(r[c]);
 }
 
-// A cell is cut when its corners are not all on one side.
-template <class T>
-__device__ __forceinline__ bool cell_cut(const T* __restrict__ phi, const long long n[3], long long i, long long j,
-                                         long long k) {
-  T ph[8];
-  corners(phi, n, i, j, k, ph);
-  int nout = 0;
-#pragma unroll
-  for (int c = 0; c < 8; ++c) nout += ph[c] >= T(0) ? 1 : 0;
-  return nout != 0 && nout != 8;
-}
-
 // A cell's triangle count and whether its tile uses the interior vertex (code 13); -1 tile if
 // the cell is not cut.
 template <class T, bool MX>
@@ -233,12 +291,10 @@ __global__ void __launch_bounds__(MB, 4) cell_count_kernel(const T* __restrict__
   __shared__ int cand[BLK];
   const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
   const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, n0, n1);
-  const int n = cccompact::compact<MB, IPT>(cand, [&](int) {
-    const bool r = w.v < nc && cell_cut(phi, g.n, w.i, w.j, w.k);
-    w.step();
-    return r;
-  });
+  const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
+  Walker w(start, n0, n1, nx, nz);
+  const int n = cccompact::compact<MB, IPT, Groups<T>::cell>(
+      cand, [&](int) { return cells_with_cut<T, Groups<T>::cell>(phi, w, nc, nx, nz); });
   keep_survivors(cand, n, kept, kept_n);
   unsigned long long t = 0, in = 0;
   for (int x = threadIdx.x; x < n; x += MB) {
@@ -271,12 +327,10 @@ __global__ void __launch_bounds__(MB, 4) cell_emit_kernel(const T* __restrict__ 
   __shared__ int cand[BLK];
   const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
   const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, n0, n1);
-  const int n = survivors(cand, kept, kept_n, [&](int) {
-    const bool r = w.v < nc && cell_cut(phi, g.n, w.i, w.j, w.k);
-    w.step();
-    return r;
-  });
+  const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
+  Walker w(start, n0, n1, nx, nz);
+  const int n = survivors<Groups<T>::cell>(
+      cand, kept, kept_n, [&](int) { return cells_with_cut<T, Groups<T>::cell>(phi, w, nc, nx, nz); });
   unsigned long long run_t = boff[2 * blockIdx.x], run_i = n_edge_verts + boff[2 * blockIdx.x + 1];
   for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
     const int x = c0 + threadIdx.x;

@@ -200,11 +200,7 @@ __device__ __forceinline__ void cell_counts(const PlicIn<T, D>& P, int m, const 
 // within 3 u (|n|_1 + |a|) of exact (u the unit roundoff), these bounds within 2 u |n|_1, so a gap
 // of 64 u (|n|_1 + |a|) leaves every corner value one strict sign. NaN or inf fails both tests.
 template <class T, int D>
-__device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, const T* nrm, const T* icp, const uint8_t* val,
-                                              int r, T min_d) {
-  const T n0 = nrm[D * r], n1 = nrm[D * r + 1], n2 = D == 3 ? nrm[D * r + 2] : T(0);
-  const T a = icp[r];
-  const bool ok = val ? val[r] != 0 : (n0 != T(0) || n1 != T(0) || n2 != T(0));
+__device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, T n0, T n1, T n2, T a, bool ok, T min_d) {
   const T zero = T(0);
   const T lo = (fmin(n0, zero) + fmin(n1, zero)) + fmin(n2, zero);
   const T hi = (fmax(n0, zero) + fmax(n1, zero)) + fmax(n2, zero);
@@ -214,18 +210,38 @@ __device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, const T* nr
   return !ok || miss;
 }
 
-// A block's entries that may draw something, in entry order, into cand (compact.cuh).
+// A block's entries that may draw something, in entry order, into cand (compact.cuh): G rounds'
+// planes are loaded (the index clamped to the block's last entry) before any is tested.
 template <class T, int D>
 __device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d, int* cand) {
+  constexpr int G = sizeof(T) == 4 ? 8 : 4;
   const long long start = (long long)blockIdx.x * BLK;
   // this block's entries, addressed by 32-bit offsets
   const int here = P.count - start < BLK ? int(P.count - start) : BLK;
   const T* nrm = P.normals + D * start;
   const T* icp = P.intercepts + start;
   const uint8_t* val = P.valid ? P.valid + start : nullptr;
-  return cccompact::compact<MB, IPT>(cand, [&](int q) {
-    const int r = q * MB + threadIdx.x;
-    return r < here && !draws_nothing<T, D>(P, nrm, icp, val, r, min_d);
+  return cccompact::compact<MB, IPT, G>(cand, [&](int q0) {
+    T n0[G], n1[G], n2[G], a[G];
+    bool ok[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int r = (q0 + u) * MB + threadIdx.x;
+      const int rr = r < here ? r : here - 1;
+      n0[u] = nrm[D * rr];
+      n1[u] = nrm[D * rr + 1];
+      n2[u] = D == 3 ? nrm[D * rr + 2] : T(0);
+      a[u] = icp[rr];
+      ok[u] = val ? val[rr] != 0 : true;
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int r = (q0 + u) * MB + threadIdx.x;
+      const bool okk = val ? ok[u] : (n0[u] != T(0) || n1[u] != T(0) || n2[u] != T(0));
+      if (r < here && !draws_nothing<T, D>(P, n0[u], n1[u], n2[u], a[u], okk, min_d)) m |= 1u << u;
+    }
+    return m;
   });
 }
 
@@ -234,7 +250,7 @@ __device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d
 // The count pass also saves each block's compacted entries (up to KEEP; -1 in kept_n when more),
 // so the emit pass clips them without testing every entry again.
 template <class T, int D>
-__global__ void __launch_bounds__(MB, 5) plic_count_kernel(const PlicIn<T, D> P, T min_d, unsigned long long* bsum,
+__global__ void __launch_bounds__(MB, sizeof(T) == 4 ? 5 : 4) plic_count_kernel(const PlicIn<T, D> P, T min_d, unsigned long long* bsum,
                                                         int* kept, int* kept_n) {
   __shared__ int cand[BLK];
   const int ncand = compact_candidates<T, D>(P, min_d, cand);
