@@ -50,7 +50,7 @@ __device__ __forceinline__ int compact(int* cand, Keep keep) {
   __shared__ int slot[MB];  // per (round, warp): its count, then its first position
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned bits = 0;
-#pragma unroll 1
+#pragma unroll 2
   for (int q0 = 0; q0 < IPT; q0 += G) bits |= keep(q0) << q0;
 #pragma unroll 8
   for (int q = 0; q < IPT; ++q) {
