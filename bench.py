@@ -30,7 +30,8 @@ larger than the 126 MB L2, so no flush is needed between steps).
   events, the same caches).
 * ``plic``: PLICCutCell over [0,1]^3 at the same n, a union of 64 seeded spheres: update times
   in Float32, Float64 and mixed precision, the resolved face fractions' single-valuedness, the
-  errors against Float64, and calc_volume against a 10^8-point Monte Carlo estimate.
+  errors against Float64, calc_volume against a 10^8-point Monte Carlo estimate, and
+  ``surface_f32``: generate_mesh of the Float32 cache (every cell's plane clipped to its cell).
 * ``mesh``: generate_mesh (count and emit) of the Float32 CSG cache on the device, and the oracle's
   serial march of a bounded slab of the same field.
 * ``cpu_baseline`` / ``--impl reference``: the oracle (a C++ restatement of the reference's CPU
@@ -438,9 +439,10 @@ def plic_surface_timing(cache, g, dev, reps=5):
     torch.cuda.synchronize(dev)
     ms = (time.perf_counter() - t0) / reps * 1e3
     ncell = cache.intercepts.shape[0]
-    # per cell the two passes each read the plane (D+1 values) and the flag
-    plane_bytes = 2 * ncell * (4 * (g.dim + 1) + 1)
-    out_bytes = m.nodes.numel() * 4 + m.elements.numel() * 4 + m.cells.numel() * 8
+    # per cell the count pass reads the plane (D+1 values) and the flag; the emit pass reads only
+    # the survivors the count kept (counted with the output, below the rounding of this figure)
+    plane_bytes = ncell * (cache.intercepts.element_size() * (g.dim + 1) + 1)
+    out_bytes = m.nodes.numel() * m.nodes.element_size() + m.elements.numel() * 4 + m.cells.numel() * 8
     r = {"ms": ms, "cells_per_s": ncell / (ms * 1e-3), "nodes": int(m.nodes.shape[0]),
          "triangles": int(m.elements.shape[0]), "algorithmic_gb": (plane_bytes + out_bytes) / 1e9,
          "roofline_frac": (plane_bytes + out_bytes) / (ms * 1e-3) / 1e9 / measured_peak()[0]}
