@@ -603,6 +603,24 @@ def learned_block(args, dev, cc):
                             "plain_ms_at_that_n": cost_eq, "learned_speedup_at_equal_l1": cost_eq / ms_learned}}
 
 
+def run_only(args):
+    """One block alone: the marching-cubes mesh of the Float32 CSG cache, or the PLIC surface of the
+    Float32 64-sphere cache, at --n."""
+    import torch
+    from __graft_entry__ import load_package
+    cc = load_package()
+    dev = torch.device("cuda", 0)
+    if args.only == "mesh":
+        args.no_cpu = True
+        out = mesh_block(args, dev, cc)
+    else:
+        g = cc.workloads.unit_grid(args.n)
+        c = cc.allocate_cache(g, cc.PLICCutCell(), dtype=torch.float32, device=dev)
+        cc.update_cache(c, cc.flatten(cc.workloads.sphere_cloud(0, 64), 3), g)
+        out = dict(plic_surface_timing(c, g, dev), grid=f"[0,1]^3 at {args.n}^3, union of 64 spheres, Float32")
+    print(json.dumps({"only": args.only, **out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -615,7 +633,12 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-plic", action="store_true")
+    ap.add_argument("--only", choices=["mesh", "plic-surface"],
+                    help="run one block alone at --n and print its JSON (for profiling)")
     args = ap.parse_args()
+    if args.only:
+        run_only(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

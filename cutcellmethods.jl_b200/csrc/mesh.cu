@@ -82,20 +82,22 @@ __device__ __forceinline__ void edge_vertex(const T* __restrict__ phi, const Dev
 
 // Walks item coordinates (i, j, k) over an n0 x n1 x * box from item `start + threadIdx.x` in steps
 // of MB (one 64-bit division at the start), carrying the item's node index b = i + sx j + sz k
-// (for the node box, b is the item itself; for the cell box, the cell's lower corner). The steps
-// are arithmetic only, so the loads they address do not wait on one another.
+// (for the node box, b is the item itself; for the cell box, the cell's lower corner). Indices
+// are 32-bit: a mesh grid has fewer than 2^32 nodes. The steps are arithmetic only, so the loads
+// they address do not wait on one another.
 struct Walker {
-  long long v, b;
+  unsigned v, b;
   int i, j, k;
   const int n0, n1;
-  const long long sx, sz;
+  const unsigned sx, sz;
   __device__ Walker(long long start, long long n0_, long long n1_, long long sx_, long long sz_)
-      : n0(int(n0_)), n1(int(n1_)), sx(sx_), sz(sz_) {
-    v = start + threadIdx.x;
-    i = int(v % n0_);
-    j = int((v / n0_) % n1_);
-    k = int(v / (n0_ * n1_));
-    b = i + sx * j + sz * k;
+      : n0(int(n0_)), n1(int(n1_)), sx(unsigned(sx_)), sz(unsigned(sz_)) {
+    const long long v64 = start + threadIdx.x;
+    v = unsigned(v64);
+    i = int(v64 % n0_);
+    j = int((v64 / n0_) % n1_);
+    k = int(v64 / (n0_ * n1_));
+    b = unsigned(i) + sx * unsigned(j) + sz * unsigned(k);
   }
   __device__ __forceinline__ void step() {
     v += MB;
@@ -103,11 +105,11 @@ struct Walker {
     b += MB;
     while (i >= n0) {
       i -= n0;
-      b += sx - n0;
+      b += sx - unsigned(n0);
       if (++j == n1) {
         j = 0;
         ++k;
-        b += sz - sx * n1;
+        b += sz - sx * unsigned(n1);
       }
     }
   }
@@ -123,19 +125,18 @@ __device__ __forceinline__ bool out_fast(T v) { return v > -Eps<T>::v(); }
 // A node has a cut edge when a neighbour along +x, +y or +z (inside the box) lies on the other side;
 // a cell is cut when its corners are not all on one side.
 template <class T, int G>
-__device__ __forceinline__ unsigned nodes_with_cut(const T* __restrict__ phi, Walker& w, long long nn,
-                                                   const long long n[3], long long nx, long long nz) {
+__device__ __forceinline__ unsigned nodes_with_cut(const T* __restrict__ phi, Walker& w, unsigned nn, int m0, int m1,
+                                                   int m2, unsigned nx, unsigned nz, bool full) {
   T p0[G], px[G], py[G], pz[G];
   bool in[G];
 #pragma unroll
   for (int u = 0; u < G; ++u) {
-    in[u] = w.v < nn;
-    const long long b = in[u] ? w.b : nn - 1;
-    const T* p = phi + b;
+    in[u] = full || w.v < nn;
+    const T* p = phi + (in[u] ? w.b : nn - 1);
     p0[u] = p[0];
-    px[u] = p[in[u] && w.i < n[0] ? 1 : 0];
-    py[u] = p[in[u] && w.j < n[1] ? nx : 0];
-    pz[u] = p[in[u] && w.k < n[2] ? nz : 0];
+    px[u] = p[in[u] && w.i < m0 ? 1u : 0u];
+    py[u] = p[in[u] && w.j < m1 ? nx : 0u];
+    pz[u] = p[in[u] && w.k < m2 ? nz : 0u];
     w.step();
   }
   unsigned m = 0;
@@ -149,14 +150,14 @@ __device__ __forceinline__ unsigned nodes_with_cut(const T* __restrict__ phi, Wa
 }
 
 template <class T, int G>
-__device__ __forceinline__ unsigned cells_with_cut(const T* __restrict__ phi, Walker& w, long long nc, long long nx,
-                                                   long long nz) {
+__device__ __forceinline__ unsigned cells_with_cut(const T* __restrict__ phi, Walker& w, unsigned nc, unsigned nx,
+                                                   unsigned nz, bool full) {
   T c[G][8];
   bool in[G];
 #pragma unroll
   for (int u = 0; u < G; ++u) {
-    in[u] = w.v < nc;
-    const T* p = phi + (in[u] ? w.b : 0);
+    in[u] = full || w.v < nc;
+    const T* p = phi + (in[u] ? w.b : 0u);
     c[u][0] = p[0]; c[u][1] = p[1]; c[u][2] = p[nx]; c[u][3] = p[nx + 1];
     c[u][4] = p[nz]; c[u][5] = p[nz + 1]; c[u][6] = p[nz + nx]; c[u][7] = p[nz + nx + 1];
     w.step();
@@ -204,8 +205,11 @@ __global__ void __launch_bounds__(MB, 4) node_count_kernel(const T* __restrict__
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
   const long long start = (long long)blockIdx.x * BLK;
   Walker w(start, nx, ny, nx, nx * ny);
-  const int n = cccompact::compact<MB, IPT, Groups<T>::node>(
-      cand, [&](int) { return nodes_with_cut<T, Groups<T>::node>(phi, w, nn, g.n, nx, nx * ny); });
+  const bool full = start + BLK <= nn;  // block-uniform: no item past the grid
+  const int n = cccompact::compact<MB, IPT, Groups<T>::node>(cand, [&](int) {
+    return nodes_with_cut<T, Groups<T>::node>(phi, w, unsigned(nn), int(g.n[0]), int(g.n[1]), int(g.n[2]),
+                                              unsigned(nx), unsigned(nx * ny), full);
+  });
   keep_survivors(cand, n, kept, kept_n);
   unsigned long long c = 0;
   for (int x = threadIdx.x; x < n; x += MB) {
@@ -227,8 +231,11 @@ __global__ void __launch_bounds__(MB, 4) node_emit_kernel(const T* __restrict__ 
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
   const long long start = (long long)blockIdx.x * BLK;
   Walker w(start, nx, ny, nx, nx * ny);
-  const int n = survivors<Groups<T>::node>(
-      cand, kept, kept_n, [&](int) { return nodes_with_cut<T, Groups<T>::node>(phi, w, nn, g.n, nx, nx * ny); });
+  const bool full = start + BLK <= nn;  // block-uniform: no item past the grid
+  const int n = survivors<Groups<T>::node>(cand, kept, kept_n, [&](int) {
+    return nodes_with_cut<T, Groups<T>::node>(phi, w, unsigned(nn), int(g.n[0]), int(g.n[1]), int(g.n[2]),
+                                              unsigned(nx), unsigned(nx * ny), full);
+  });
   unsigned long long run = boff[blockIdx.x];
   for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
     const int x = c0 + threadIdx.x;
@@ -293,8 +300,10 @@ __global__ void __launch_bounds__(MB, 4) cell_count_kernel(const T* __restrict__
   const long long start = (long long)blockIdx.x * BLK;
   const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
   Walker w(start, n0, n1, nx, nz);
-  const int n = cccompact::compact<MB, IPT, Groups<T>::cell>(
-      cand, [&](int) { return cells_with_cut<T, Groups<T>::cell>(phi, w, nc, nx, nz); });
+  const bool full = start + BLK <= nc;  // block-uniform: no item past the grid
+  const int n = cccompact::compact<MB, IPT, Groups<T>::cell>(cand, [&](int) {
+    return cells_with_cut<T, Groups<T>::cell>(phi, w, unsigned(nc), unsigned(nx), unsigned(nz), full);
+  });
   keep_survivors(cand, n, kept, kept_n);
   unsigned long long t = 0, in = 0;
   for (int x = threadIdx.x; x < n; x += MB) {
@@ -329,8 +338,10 @@ __global__ void __launch_bounds__(MB, 4) cell_emit_kernel(const T* __restrict__ 
   const long long start = (long long)blockIdx.x * BLK;
   const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
   Walker w(start, n0, n1, nx, nz);
-  const int n = survivors<Groups<T>::cell>(
-      cand, kept, kept_n, [&](int) { return cells_with_cut<T, Groups<T>::cell>(phi, w, nc, nx, nz); });
+  const bool full = start + BLK <= nc;  // block-uniform: no item past the grid
+  const int n = survivors<Groups<T>::cell>(cand, kept, kept_n, [&](int) {
+    return cells_with_cut<T, Groups<T>::cell>(phi, w, unsigned(nc), unsigned(nx), unsigned(nz), full);
+  });
   unsigned long long run_t = boff[2 * blockIdx.x], run_i = n_edge_verts + boff[2 * blockIdx.x + 1];
   for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
     const int x = c0 + threadIdx.x;
@@ -426,7 +437,8 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
   const long long nn = (g.n[0] + 1) * (g.n[1] + 1) * (g.n[2] + 1);
   const long long nc = g.n[0] * g.n[1] * g.n[2];
   const long long nbn = (nn + BLK - 1) / BLK, nbc = (nc + BLK - 1) / BLK;
-  if (nn > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 nodes");
+  // 32-bit item indices, with room for the last block's rounds past the end
+  if (nn > 0xffffffffLL - BLK) return fail(CC_TOO_LARGE, "generate_mesh takes fewer than 2^32 - 8192 nodes");
   cci::MeshKey& key = h->mesh_key;
   cudaError_t e = cudaSuccess;
   if (size_t(nn) > h->mesh_vbase_n) {
