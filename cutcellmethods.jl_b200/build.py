@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-std=c++17",
                 "-Xcompiler", "-fPIC"]
 SOURCES = ["capi.cu", "mc.cu", "ms.cu", "plic.cu", "noalloc.cu", "learned.cu", "learned_api.cu", "batch.cu", "mesh.cu", "ms_mesh.cu", "plic_mesh.cu"]
-HEADERS = ["cc_device.cuh", "cc_internal.h", "mc_cell.cuh", "ms_cell.cuh"]
+HEADERS = ["cc_device.cuh", "cc_internal.h", "mc_cell.cuh", "ms_cell.cuh", "compact.cuh"]
 
 
 def _inputs():
