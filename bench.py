@@ -244,7 +244,7 @@ def run_ours(args, rank, world, dist):
     precision["degenerate_deciders"] = degenerate_decider_errors(cc, dev)
 
     learned = None if args.no_learned else learned_block(args, dev, cc)
-    batched = None if args.no_batch else batch_block(args, dev, cc)
+    batched = None if args.no_batch else batch_block(args, dev, cc, k=args.batch_updates)
     mesh = mesh_block(args, dev, cc)
     plic = None if args.no_plic else plic_block(args, dev, cc)
     clk.__exit__(None, None, None)
@@ -518,7 +518,7 @@ def batch_block(args, dev, cc, k=256):
         cells = sum(g.ncell for g, _, _ in ups)
         nodes = sum(g.nnode for g, _, _ in ups)
         elem = 4 if dtype == torch.float32 else 8
-        algo = cells * (2 + 9 * elem) + nodes * elem
+        algo = cells * (2 + 13 * elem) + nodes * elem  # kind, ambiguous, vf, c 2, ff 4, fcl 4, ic 2
 
         def per_update():
             for c, (g, _, _), t in zip(caches, ups, tapes):
@@ -604,8 +604,8 @@ def learned_block(args, dev, cc):
 
 
 def run_only(args):
-    """One block alone: the marching-cubes mesh of the Float32 CSG cache, or the PLIC surface of the
-    Float32 64-sphere cache, at --n."""
+    """One block alone: the marching-cubes mesh of the Float32 CSG cache or the PLIC surface of the
+    Float32 64-sphere cache at --n, or the batched marching-squares workloads (--batch-updates)."""
     import torch
     from __graft_entry__ import load_package
     cc = load_package()
@@ -613,6 +613,8 @@ def run_only(args):
     if args.only == "mesh":
         args.no_cpu = True
         out = mesh_block(args, dev, cc)
+    elif args.only == "batch":
+        out = batch_block(args, dev, cc, k=args.batch_updates)
     else:
         g = cc.workloads.unit_grid(args.n)
         c = cc.allocate_cache(g, cc.PLICCutCell(), dtype=torch.float32, device=dev)
@@ -633,7 +635,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-plic", action="store_true")
-    ap.add_argument("--only", choices=["mesh", "plic-surface"],
+    ap.add_argument("--batch-updates", type=int, default=256, help="updates in the batched marching-squares block")
+    ap.add_argument("--only", choices=["mesh", "plic-surface", "batch"],
                     help="run one block alone at --n and print its JSON (for profiling)")
     args = ap.parse_args()
     if args.only:

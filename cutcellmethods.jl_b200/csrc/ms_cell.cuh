@@ -17,6 +17,44 @@ __host__ __device__ constexpr int dir_edge(int dir) { return dir == 0 ? 3 : dir 
 
 // cut_cell_moments (2D), src/marching_squares/moments.jl:66-164, from global corner
 // coordinates `nd` (MS_NODE_BITS order) and corner values `ph`; writes cell `ci`'s columns.
+// One cell's fields into the columns. Where the four wide columns are 16-byte aligned (every
+// caller's allocation here), a cell's centroid and interface centroid leave as one 2-vector each
+// and its face fractions and face centroids as 16-byte vectors, so a warp's store covers whole
+// sectors; otherwise element by element.
+template <class T>
+__device__ __forceinline__ void store_cell2(const Cols& cols, long long ci, int kind, int amb, T vf, T c0, T c1,
+                                            const T ff[4], const T fcl[4], T i0, T i1) {
+  cols.kind[ci] = int8_t(kind);
+  cols.amb[ci] = uint8_t(amb);
+  static_cast<T*>(cols.vf)[ci] = vf;
+  T* c = static_cast<T*>(cols.c);
+  T* f = static_cast<T*>(cols.ff);
+  T* l = static_cast<T*>(cols.fcl);
+  T* ic = static_cast<T*>(cols.ic);
+  const bool vec = ((reinterpret_cast<uintptr_t>(c) | reinterpret_cast<uintptr_t>(f) | reinterpret_cast<uintptr_t>(l) |
+                     reinterpret_cast<uintptr_t>(ic)) & 15u) == 0;
+  if (vec) {
+    if (sizeof(T) == 4) {
+      reinterpret_cast<float2*>(c)[ci] = make_float2(float(c0), float(c1));
+      reinterpret_cast<float2*>(ic)[ci] = make_float2(float(i0), float(i1));
+      reinterpret_cast<float4*>(f)[ci] = make_float4(float(ff[0]), float(ff[1]), float(ff[2]), float(ff[3]));
+      reinterpret_cast<float4*>(l)[ci] = make_float4(float(fcl[0]), float(fcl[1]), float(fcl[2]), float(fcl[3]));
+    } else {
+      reinterpret_cast<double2*>(c)[ci] = make_double2(double(c0), double(c1));
+      reinterpret_cast<double2*>(ic)[ci] = make_double2(double(i0), double(i1));
+      reinterpret_cast<double2*>(f)[2 * ci] = make_double2(double(ff[0]), double(ff[1]));
+      reinterpret_cast<double2*>(f)[2 * ci + 1] = make_double2(double(ff[2]), double(ff[3]));
+      reinterpret_cast<double2*>(l)[2 * ci] = make_double2(double(fcl[0]), double(fcl[1]));
+      reinterpret_cast<double2*>(l)[2 * ci + 1] = make_double2(double(fcl[2]), double(fcl[3]));
+    }
+    return;
+  }
+  c[2 * ci] = c0; c[2 * ci + 1] = c1;
+#pragma unroll
+  for (int dir = 0; dir < 4; ++dir) { f[4 * ci + dir] = ff[dir]; l[4 * ci + dir] = fcl[dir]; }
+  ic[2 * ci] = i0; ic[2 * ci + 1] = i1;
+}
+
 template <class T, bool MX>
 __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Cols& cols, long long ci) {
   const T o0 = nd[0][0], o1 = nd[0][1];
@@ -25,12 +63,7 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
   int nout = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) nout += ph[k] >= T(0) ? 1 : 0;
-  T* vf = static_cast<T*>(cols.vf);
-  T* c = static_cast<T*>(cols.c);
-  T* ff = static_cast<T*>(cols.ff);
-  T* fcl = static_cast<T*>(cols.fcl);
-  T* ic = static_cast<T*>(cols.ic);
-  T fc[4];
+  T fc[4], ffv[4];
   if (nout == 4 || nout == 0) {
     const bool out = nout == 4;
 #pragma unroll
@@ -38,14 +71,9 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
       const int k = dir_edge(dir), k1 = (k + 1) & 3;
       const int p = dir < 2 ? 1 : 0;
       fc[dir] = T(0.5) * (nd[k][p] + nd[k1][p]) - nd[0][p];
+      ffv[dir] = out ? T(1) : T(0);
     }
-    cols.kind[ci] = out ? 1 : 0;
-    cols.amb[ci] = 0;
-    vf[ci] = out ? T(1) : T(0);
-    c[2 * ci] = ce0; c[2 * ci + 1] = ce1;
-#pragma unroll
-    for (int dir = 0; dir < 4; ++dir) { ff[4 * ci + dir] = out ? T(1) : T(0); fcl[4 * ci + dir] = fc[dir]; }
-    ic[2 * ci] = ce0; ic[2 * ci + 1] = ce1;
+    store_cell2<T>(cols, ci, out ? 1 : 0, 0, out ? T(1) : T(0), ce0, ce1, ffv, fc, ce0, ce1);
     return;
   }
   // cell_boundary_walk, marching_squares.jl:240-251
@@ -75,8 +103,7 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
     const int p = dir < 2 ? 1 : 0;
     const T x = pr[k] ? T(0.5) * (sa[k][p] + sb[k][p]) : T(0.5) * (nd[k][p] + nd[k1][p]);
     fc[dir] = x - nd[0][p];
-    ff[4 * ci + dir] = fr[k];
-    fcl[4 * ci + dir] = fc[dir];
+    ffv[dir] = fr[k];
   }
   T area2 = T(0), m0 = T(0), m1 = T(0);
 #pragma unroll
@@ -117,17 +144,17 @@ __device__ void ms_cell(const T nd[4][2], const T ph[4], const T cs[2], const Co
     }
   }
   const T area = T(0.5) * area2;
-  cols.kind[ci] = 2;
-  cols.amb[ci] = nint > 1 ? 1 : 0;
-  vf[ci] = area / vol_cell;
+  T c0 = ce0, c1 = ce1, i0 = ce0, i1 = ce1;
   if (area2 != T(0)) {
     const T den = T(3) * area2;
-    c[2 * ci] = o0 + m0 / den; c[2 * ci + 1] = o1 + m1 / den;
-  } else {
-    c[2 * ci] = ce0; c[2 * ci + 1] = ce1;
+    c0 = o0 + m0 / den;
+    c1 = o1 + m1 / den;
   }
-  if (ilen > T(0)) { ic[2 * ci] = im0 / ilen; ic[2 * ci + 1] = im1 / ilen; }
-  else { ic[2 * ci] = ce0; ic[2 * ci + 1] = ce1; }
+  if (ilen > T(0)) {
+    i0 = im0 / ilen;
+    i1 = im1 / ilen;
+  }
+  store_cell2<T>(cols, ci, 2, nint > 1 ? 1 : 0, area / vol_cell, c0, c1, ffv, fc, i0, i1);
 }
 
 // cell_interface (src/marching_squares/marching_squares.jl:343-351): the cell's n <= 2 contour
