@@ -657,6 +657,10 @@ __device__ __forceinline__ T gvf2(T n1, T n2, T a) {
   if (n2 < T(0)) alpha = alpha + m2;
   const T s = m1 + m2;
   if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  // a plane that misses the square: alpha / s <= 0 exactly when alpha <= 0, and alpha / s >= 1 when
+  // alpha >= s (rounding is monotone), so these are the returns below without the divisions
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= s) return T(1);
   m1 = m1 / s; m2 = m2 / s; alpha = alpha / s;
   if (alpha <= T(0)) return T(0);
   if (alpha >= T(1)) return T(1);
@@ -680,6 +684,9 @@ __device__ __forceinline__ T gvf3(T n1, T n2, T n3, T a) {
   if (n3 < T(0)) alpha = alpha + m2_;
   const T s = (m0 + m1_) + m2_;
   if (!(s > T(0))) return alpha >= T(0) ? T(1) : T(0);
+  // a plane that misses the cube: the returns below without the divisions (as in gvf2)
+  if (alpha <= T(0)) return T(0);
+  if (alpha >= s) return T(1);
   m0 = m0 / s; m1_ = m1_ / s; m2_ = m2_ / s; alpha = alpha / s;
   if (alpha <= T(0)) return T(0);
   if (alpha >= T(1)) return T(1);

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const 
 
 // _cell_wet + _face_area, src/plic/apertures.jl:73-125 (k is the 0-based direction)
 template <class T, int D, bool MX>
-__device__ __noinline__ T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k) {
+__device__ __forceinline__ T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k) {
   const T s = (k & 1) ? T(1) : T(0);
   if constexpr (D == 2) {
     const int c = k < 2 ? 0 : 1, p = k < 2 ? 1 : 0;
@@ -174,16 +174,15 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
   constexpr int E0 = P::Y * P::Z, E1 = P::X * P::Z, E2 = P::X * P::Y;  // halo face sizes per axis
   constexpr int HB[3] = {0, 2 * E0, 2 * E0 + 2 * E1};                  // halo base per axis
   constexpr int NH = D == 3 ? 2 * (E0 + E1 + E2) : 2 * (E0 + E1);
-  __shared__ T own[NT * NF];
+  static_assert(P::X * P::Y * P::Z == NT, "one cell per thread");
+  __shared__ T own[NF][NT];                  // one-sided areas, face-major (no bank conflicts)
   __shared__ T halo[NH];
+  __shared__ __align__(16) T res[NT * NF];   // resolved fractions, cell-major as in the column
   const long long n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
   const T* vf = static_cast<const T*>(cols.vf);
   T* ff = static_cast<T*>(cols.ff);
   const T cs[3] = {g.d[0], g.d[1], D == 3 ? g.d[2] : T(1)};
   const long long tx = (n[0] + P::X - 1) / P::X, ty = (n[1] + P::Y - 1) / P::Y, tz = (n[2] + P::Z - 1) / P::Z;
-  auto area = [&](long long cj, int k) {
-    return face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs, k);
-  };
   for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
     const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
     const int q = threadIdx.x;
@@ -191,9 +190,14 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
     const long long idx[3] = {i0[0] + lq[0], i0[1] + lq[1], i0[2] + lq[2]};
     const bool in = idx[0] < n[0] && idx[1] < n[1] && idx[2] < n[2];
     const long long ci = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
-    if (in) {
+    if (in) {  // this cell's plane, read once, on all its faces
+      T nrm[D];
 #pragma unroll
-      for (int k = 0; k < NF; ++k) own[q * NF + k] = area(ci, k);
+      for (int a = 0; a < D; ++a) nrm[a] = normals[D * ci + a];
+      const T a = intercepts[ci], frac = vf[ci];
+      const bool ok = valid[ci] != 0;
+#pragma unroll
+      for (int k = 0; k < NF; ++k) own[k][q] = face_area<T, D, MX>(nrm, a, frac, ok, cs, k);
     }
     // the halo: for each axis and side, the cell beyond the tile shows its face toward the tile
     for (int h = threadIdx.x; h < NH; h += NT) {
@@ -207,8 +211,11 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
       nb[ax] = side == 0 ? i0[ax] - 1 : i0[ax] + EXT[ax];
       nb[o1] = i0[o1] + pos % EXT[o1];
       nb[o2] = i0[o2] + pos / EXT[o1];
-      if (nb[ax] >= 0 && nb[ax] < n[ax] && nb[o1] < n[o1] && nb[o2] < n[o2])
-        halo[h] = area(nb[0] + n[0] * (nb[1] + n[1] * nb[2]), side == 0 ? 2 * ax + 1 : 2 * ax);
+      if (nb[ax] >= 0 && nb[ax] < n[ax] && nb[o1] < n[o1] && nb[o2] < n[o2]) {
+        const long long cj = nb[0] + n[0] * (nb[1] + n[1] * nb[2]);
+        halo[h] = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs,
+                                      side == 0 ? 2 * ax + 1 : 2 * ax);
+      }
     }
     __syncthreads();
     if (in) {
@@ -221,22 +228,39 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
         else full = (T(1) * cs[o1]) * cs[o2];
         const int lstride = c == 0 ? 1 : (c == 1 ? P::X : P::X * P::Y);
         const int hpos = lq[o1] + EXT[o1] * (D == 3 ? lq[o2] : 0);
-        const T mine = own[q * NF + k];
+        const T mine = own[k][q];
         T r;
         if ((k & 1) == 0) {
           const bool has = idx[c] >= 1;
-          const T below = lq[c] > 0 ? own[(q - lstride) * NF + k + 1] : halo[HB[c] + hpos];
+          const T below = lq[c] > 0 ? own[k + 1][q - lstride] : halo[HB[c] + hpos];
           r = has ? (below / full + mine / full) / T(2) : mine / full;
         } else {
           const bool has = idx[c] <= n[c] - 2;
           const int Ec = c == 0 ? E0 : (c == 1 ? E1 : E2);
-          const T above = lq[c] < EXT[c] - 1 ? own[(q + lstride) * NF + k - 1] : halo[HB[c] + Ec + hpos];
+          const T above = lq[c] < EXT[c] - 1 ? own[k - 1][q + lstride] : halo[HB[c] + Ec + hpos];
           r = has ? (mine / full + above / full) / T(2) : mine / full;
         }
-        ff[2 * D * ci + k] = r;
+        res[q * NF + k] = r;
       }
     }
-    __syncthreads();  // the next tile reuses own and halo
+    __syncthreads();
+    // the tile's rows leave whole: a row is P::X cells x NF values, contiguous in the column
+    const int rowcells = (int)(n[0] - i0[0] < P::X ? n[0] - i0[0] : P::X);
+    constexpr int RV = P::X * NF * int(sizeof(T)) / 16;  // 16-byte vectors per full row
+    for (int w = threadIdx.x; w < P::Y * P::Z * RV; w += NT) {
+      const int row = w / RV, v = w - row * RV;
+      const long long j = i0[1] + row % P::Y, k = i0[2] + row / P::Y;
+      if (j >= n[1] || k >= n[2]) continue;
+      const long long c0 = i0[0] + n[0] * (j + n[1] * k);
+      if (rowcells == P::X && (reinterpret_cast<uintptr_t>(ff + NF * c0) & 15u) == 0) {
+        reinterpret_cast<uint4*>(ff + NF * c0)[v] = reinterpret_cast<const uint4*>(res + row * P::X * NF)[v];
+      } else {
+        constexpr int PER = 16 / int(sizeof(T));
+        for (int e = v * PER; e < (v + 1) * PER; ++e)
+          if (e < rowcells * NF) ff[NF * c0 + e] = res[row * P::X * NF + e];
+      }
+    }
+    __syncthreads();  // the next tile reuses own, halo and res
   }
 }
 
