@@ -160,6 +160,15 @@ __device__ __forceinline__ T face_area(const T* n, T a, T frac, bool valid, cons
   }
 }
 
+__host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
+
+// m / full for a face area m of a face of area full > 0, bit for bit: an area of exactly 0 or
+// exactly full (every face the plane misses) gives m itself (0 / full keeps m's sign) or 1
+// without the division. The resolved value's halving, (a + b) / 2, is taken as (a + b) * 0.5:
+// both round the same real number.
+template <class T>
+__device__ __forceinline__ T frac_of(T m, T full) { return m == T(0) ? m : (m == full ? T(1) : m / full); }
+
 // The resolved faces (src/plic/cache.jl:118-162) of one tile: every cell's one-sided areas
 // (_face_area, apertures.jl:73-125) computed once into shared memory, with the faces the
 // neighbouring cells outside the tile show it; each shared face is then resolved from its two
@@ -175,6 +184,9 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
   constexpr int HB[3] = {0, 2 * E0, 2 * E0 + 2 * E1};                  // halo base per axis
   constexpr int NH = D == 3 ? 2 * (E0 + E1 + E2) : 2 * (E0 + E1);
   static_assert(P::X * P::Y * P::Z == NT, "one cell per thread");
+  static_assert((P::X & (P::X - 1)) == 0 && (P::Y & (P::Y - 1)) == 0 && (P::Z & (P::Z - 1)) == 0, "powers of two");
+  constexpr int LX = ilog2(P::X), LY = ilog2(P::Y), LZ = ilog2(P::Z);
+  constexpr int LE0 = LY + LZ, LE1 = LX + LZ, LE2 = LX + LY;  // log2 of the halo face sizes
   __shared__ T own[NF][NT];                  // one-sided areas, face-major (no bank conflicts)
   __shared__ T halo[NH];
   __shared__ __align__(16) T res[NT * NF];   // resolved fractions, cell-major as in the column
@@ -204,13 +216,15 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
       int ax = 0;
       if (D == 3 && h >= HB[2]) ax = 2;
       else if (h >= HB[1]) ax = 1;
-      const int E = ax == 0 ? E0 : (ax == 1 ? E1 : E2);
-      const int side = (h - HB[ax]) / E, pos = (h - HB[ax]) % E;
+      // the extents are powers of two: shifts and masks, not divisions
+      const int lE = ax == 0 ? LE0 : (ax == 1 ? LE1 : LE2);
+      const int side = (h - HB[ax]) >> lE, pos = (h - HB[ax]) & ((1 << lE) - 1);
       const int o1 = ax == 0 ? 1 : 0, o2 = ax == 2 ? 1 : 2;  // the other two axes, increasing
+      const int lX = o1 == 0 ? LX : LY;
       long long nb[3];
       nb[ax] = side == 0 ? i0[ax] - 1 : i0[ax] + EXT[ax];
-      nb[o1] = i0[o1] + pos % EXT[o1];
-      nb[o2] = i0[o2] + pos / EXT[o1];
+      nb[o1] = i0[o1] + (pos & ((1 << lX) - 1));
+      nb[o2] = i0[o2] + (pos >> lX);
       if (nb[ax] >= 0 && nb[ax] < n[ax] && nb[o1] < n[o1] && nb[o2] < n[o2]) {
         const long long cj = nb[0] + n[0] * (nb[1] + n[1] * nb[2]);
         halo[h] = face_area<T, D, MX>(normals + D * cj, intercepts[cj], vf[cj], valid[cj] != 0, cs,
@@ -233,12 +247,12 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
         if ((k & 1) == 0) {
           const bool has = idx[c] >= 1;
           const T below = lq[c] > 0 ? own[k + 1][q - lstride] : halo[HB[c] + hpos];
-          r = has ? (below / full + mine / full) / T(2) : mine / full;
+          r = has ? (frac_of(below, full) + frac_of(mine, full)) * T(0.5) : frac_of(mine, full);
         } else {
           const bool has = idx[c] <= n[c] - 2;
           const int Ec = c == 0 ? E0 : (c == 1 ? E1 : E2);
           const T above = lq[c] < EXT[c] - 1 ? own[k - 1][q + lstride] : halo[HB[c] + Ec + hpos];
-          r = has ? (mine / full + above / full) / T(2) : mine / full;
+          r = has ? (frac_of(mine, full) + frac_of(above, full)) * T(0.5) : frac_of(mine, full);
         }
         res[q * NF + k] = r;
       }
