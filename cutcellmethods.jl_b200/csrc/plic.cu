@@ -342,6 +342,12 @@ __device__ __forceinline__ void report_cell(int k, int a, T v, unsigned long lon
   if (k == 2 && v > T(0) && v < vmin) vmin = v;
 }
 
+// 0x80 in each byte of x that is zero, nothing elsewhere (no carry crosses a byte: (b & 0x7f) +
+// 0x7f <= 0xfe).
+__device__ __forceinline__ unsigned zero_bytes(unsigned x) {
+  return ~(((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x | 0x7f7f7f7fu);
+}
+
 template <class T>
 __global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_t* __restrict__ kind,
                                                     const uint8_t* __restrict__ amb, const T* __restrict__ vf,
@@ -357,13 +363,17 @@ __global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_
     const unsigned aw[4] = {aa.x, aa.y, aa.z, aa.w};
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int k = (int)(signed char)((kw[w] >> (8 * b)) & 0xffu);
-        const int a = (int)((aw[w] >> (8 * b)) & 0xffu);
-        // the fraction is only read for cut cells, which are few
-        const T v = k == 2 ? vf[16 * g + 4 * w + b] : T(1);
-        report_cell<T>(k, a, v, cut, ins, out, am, vmin);
+      // four cells at once: the bytes of a word equal to 2 (cut), 0 (inside), 1 (outside), and
+      // the nonzero ambiguous bytes, counted exactly whatever the byte values
+      const unsigned cutm = zero_bytes(kw[w] ^ 0x02020202u);
+      cut += __popc(cutm);
+      ins += __popc(zero_bytes(kw[w]));
+      out += __popc(zero_bytes(kw[w] ^ 0x01010101u));
+      am += 4 - __popc(zero_bytes(aw[w]));
+      // the fraction is only read for cut cells, which are few
+      for (unsigned m = cutm; m; m &= m - 1) {
+        const T v = vf[16 * g + 4 * w + ((__ffs(m) - 1) >> 3)];
+        if (v > T(0) && v < vmin) vmin = v;
       }
     }
   }

@@ -134,3 +134,29 @@ def test_dimension_mismatch_and_moved_grid():
     cc.update_cache(cache, sph, moved)
     fresh = cc.update_cache(cc.allocate_cache(moved, cc.MarchingCubesCutCell()), sph, moved)
     assert_cells_bitwise(cache.to_host(), fresh.to_host())
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_report_on_arbitrary_columns(dtype):
+    """cut_cell_report counts exactly whatever the bytes in the kind and ambiguous columns
+    (src/cut_cell.jl:302-319: is_cut / is_inside / is_outside compare the kind, is_ambiguous reads
+    the flag), including a ragged tail past the 16-cell vectors and unaligned columns."""
+    rng = np.random.default_rng(7)
+    for ncell, off in ((1_000_003, 0), (4096, 0), (17, 0), (100_001, 1)):
+        kind = rng.choice(np.array([0, 1, 2, 3, -1, -128, 127, 2, 2], np.int8), ncell)
+        amb = rng.choice(np.array([0, 1, 2, 255, 0, 0], np.uint8), ncell)
+        vf = rng.uniform(-0.1, 1.1, ncell).astype(np.float32 if dtype == torch.float32 else np.float64)
+        vf[rng.random(ncell) < 0.1] = 0
+        dev = torch.device("cuda", 0)
+        # an offset view makes the columns unaligned for the vector path
+        kb = torch.from_numpy(np.concatenate([np.zeros(off, np.int8), kind])).to(dev)[off:]
+        ab = torch.from_numpy(np.concatenate([np.zeros(off, np.uint8), amb])).to(dev)[off:]
+        vb = torch.from_numpy(vf).to(dev)
+        g = cc.CartesianGrid((0.0, 0.0, 0.0), (ncell, 1, 1), (1.0, 1.0, 1.0))
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=dtype)
+        cache.cells.kind, cache.cells.ambiguous, cache.cells.volume_fraction = kb, ab, vb
+        rep = cc.cut_cell_report(cache)
+        hr = cc.readers.cut_cell_report(kind, amb, vf)
+        assert (rep["n"], rep["cut"], rep["inside"], rep["outside"], rep["ambiguous"]) == \
+               (hr["n"], hr["cut"], hr["inside"], hr["outside"], hr["ambiguous"])
+        assert rep["min_volume_fraction"] == float(hr["min_volume_fraction"])
