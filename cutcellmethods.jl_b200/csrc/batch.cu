@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
         // one grid tile: its nodes into shared memory (owned ones to phi), then its cells
         const long long n0 = I.n0, n1 = I.n1;
         const T gx0 = T(I.x0[0]), gy0 = T(I.x0[1]), dx = T(I.d[0]), dy = T(I.d[1]);
-        const long long i0 = (lt % I.tiles_x) * A.tx, j0 = (lt / I.tiles_x) * A.ty;
+        const unsigned ltu = unsigned(lt), row = ltu / unsigned(I.tiles_x);  // 32-bit: tiles of one grid
+        const long long i0 = (long long)(ltu - row * unsigned(I.tiles_x)) * A.tx, j0 = (long long)row * A.ty;
         T* phi = static_cast<T*>(I.phi);
         for (int v = threadIdx.x; v < nxn * nyn; v += nt) {
           const int a = v % nxn, b = v / nxn;

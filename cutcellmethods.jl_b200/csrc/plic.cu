@@ -70,6 +70,16 @@ template <int D> struct PTile;
 template <> struct PTile<3> { static constexpr int X = 32, Y = 4, Z = 2; };
 template <> struct PTile<2> { static constexpr int X = 32, Y = 8, Z = 1; };
 
+// Tile t's first cell, tiles numbered x fastest, from 32-bit quotients (a grid has far fewer
+// than 2^32 tiles: that would be 2^40 cells).
+template <int D>
+__device__ __forceinline__ void tile_origin(unsigned t, unsigned tx, unsigned ty, long long i0[3]) {
+  const unsigned a = t / tx, b = a / ty;
+  i0[0] = (long long)(t - a * tx) * PTile<D>::X;
+  i0[1] = (long long)(a - b * ty) * PTile<D>::Y;
+  i0[2] = (long long)b * PTile<D>::Z;
+}
+
 // Shared-memory layout of a centroid kernel: the tape, then the pruned ops and the bounds.
 struct CentroidSmem {
   int ops_off, ls_off, us_off, bytes;
@@ -117,8 +127,10 @@ __global__ void __launch_bounds__(NT) plic_fit_kernel(const DevGrid<T> g, const 
   const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
   const long long tx = (n0 + P::X - 1) / P::X, ty = (n1 + P::Y - 1) / P::Y, tz = (n2 + P::Z - 1) / P::Z;
   T* vf = static_cast<T*>(cols.vf);
-  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
-    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+  const unsigned ntiles = unsigned(tx * ty * tz);
+  for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    long long i0[3];
+    tile_origin<D>(tile, unsigned(tx), unsigned(ty), i0);
     const STape<T> u = tile_tape<T, D>(t, tape, g, i0, smem, &s_count);
     const int q = threadIdx.x;
     const long long idx[3] = {i0[0] + q % P::X, i0[1] + (q / P::X) % P::Y, i0[2] + q / (P::X * P::Y)};
@@ -175,7 +187,7 @@ __device__ __forceinline__ T frac_of(T m, T full) { return m == T(0) ? m : (m ==
 // one-sided areas, (left / full + right / full) / 2, the same expression in the same order from
 // either side, so the face is single-valued bit for bit. Boundary faces are one-sided.
 template <class T, int D, bool MX>
-__global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const Cols cols, const T* __restrict__ normals,
+__global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, const Cols cols, const T* __restrict__ normals,
                                                        const T* __restrict__ intercepts, const uint8_t* __restrict__ valid) {
   using P = PTile<D>;
   constexpr int NF = 2 * D;
@@ -195,8 +207,10 @@ __global__ void __launch_bounds__(NT) plic_face_kernel(const DevGrid<T> g, const
   T* ff = static_cast<T*>(cols.ff);
   const T cs[3] = {g.d[0], g.d[1], D == 3 ? g.d[2] : T(1)};
   const long long tx = (n[0] + P::X - 1) / P::X, ty = (n[1] + P::Y - 1) / P::Y, tz = (n[2] + P::Z - 1) / P::Z;
-  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
-    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+  const unsigned ntiles = unsigned(tx * ty * tz);
+  for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    long long i0[3];
+    tile_origin<D>(tile, unsigned(tx), unsigned(ty), i0);
     const int q = threadIdx.x;
     const int lq[3] = {q % P::X, (q / P::X) % P::Y, q / (P::X * P::Y)};
     const long long idx[3] = {i0[0] + lq[0], i0[1] + lq[1], i0[2] + lq[2]};
@@ -300,8 +314,10 @@ __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, con
   const long long n0 = g.n[0], n1 = g.n[1], n2 = D == 3 ? g.n[2] : 1;
   const long long tx = (n0 + P::X - 1) / P::X, ty = (n1 + P::Y - 1) / P::Y, tz = (n2 + P::Z - 1) / P::Z;
   KSum acc{0.0, 0.0};
-  for (long long tile = blockIdx.x; tile < tx * ty * tz; tile += gridDim.x) {
-    const long long i0[3] = {(tile % tx) * P::X, ((tile / tx) % ty) * P::Y, (tile / (tx * ty)) * P::Z};
+  const unsigned ntiles = unsigned(tx * ty * tz);
+  for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    long long i0[3];
+    tile_origin<D>(tile, unsigned(tx), unsigned(ty), i0);
     const STape<T> u = tile_tape<T, D>(t, tape, g, i0, smem, &s_count);
     const int q = threadIdx.x;
     const long long idx[3] = {i0[0] + q % P::X, i0[1] + (q / P::X) % P::Y, i0[2] + q / (P::X * P::Y)};
