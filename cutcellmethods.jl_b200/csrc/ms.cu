@@ -20,6 +20,19 @@ using cci::DevTape;
 
 constexpr int NT = 256;
 
+// (i, j) of item v of an n0-wide box: a 32-bit quotient where the box has fewer than 2^32 items
+// (every grid that fits a device), else 64-bit.
+__device__ __forceinline__ void split2(long long v, long long n0, bool small, long long& i, long long& j) {
+  if (small) {
+    const unsigned q = unsigned(v) / unsigned(n0);
+    j = q;
+    i = (long long)(unsigned(v) - q * unsigned(n0));
+  } else {
+    j = v / n0;
+    i = v - j * n0;
+  }
+}
+
 
 template <class T>
 __global__ void __launch_bounds__(NT) ms_sample_kernel(const DevGrid<T> g, const DevTape tape, T* phi) {
@@ -27,8 +40,10 @@ __global__ void __launch_bounds__(NT) ms_sample_kernel(const DevGrid<T> g, const
   const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
   __syncthreads();
   const long long nx = g.n[0] + 1, ny = g.n[1] + 1, total = nx * ny;
+  const bool small = total + (long long)gridDim.x * NT < (1LL << 32);
   for (long long v = blockIdx.x * (long long)NT + threadIdx.x; v < total; v += (long long)gridDim.x * NT) {
-    const long long i = v % nx, j = v / nx;
+    long long i, j;
+    split2(v, nx, small, i, j);
     const T x[2] = {node_coord(g.x0[0], g.d[0], i), node_coord(g.x0[1], g.d[1], j)};
     phi[v] = tape_eval<T, 2, T>(t, x);
   }
@@ -38,8 +53,10 @@ template <class T, bool MX>
 __global__ void __launch_bounds__(NT) ms_cells_kernel(const DevGrid<T> g, const T* __restrict__ phi, const Cols cols) {
   const long long n0 = g.n[0], n1 = g.n[1], nx = n0 + 1, total = n0 * n1;
   const T cs[2] = {g.d[0], g.d[1]};
+  const bool small = total + (long long)gridDim.x * NT < (1LL << 32);
   for (long long ci = blockIdx.x * (long long)NT + threadIdx.x; ci < total; ci += (long long)gridDim.x * NT) {
-    const long long i = ci % n0, j = ci / n0;
+    long long i, j;
+    split2(ci, n0, small, i, j);
     const T xa = node_coord(g.x0[0], g.d[0], i), xb = node_coord(g.x0[0], g.d[0], i + 1);
     const T ya = node_coord(g.x0[1], g.d[1], j), yb = node_coord(g.x0[1], g.d[1], j + 1);
     const T nd[4][2] = {{xa, ya}, {xb, ya}, {xb, yb}, {xa, yb}};
