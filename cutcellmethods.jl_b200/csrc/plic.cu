@@ -181,7 +181,7 @@ __host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v
 template <class T>
 __device__ __forceinline__ T frac_of(T m, T full) { return m == T(0) ? m : (m == full ? T(1) : m / full); }
 
-// The resolved faces (src/plic/cache.jl:118-162) of one tile: every cell's one-sided areas
+// The resolved faces (src/plic/cache.jl:118-162) in 2D (3D marches z, plic_face_z_kernel) of one tile: every cell's one-sided areas
 // (_face_area, apertures.jl:73-125) computed once into shared memory, with the faces the
 // neighbouring cells outside the tile show it; each shared face is then resolved from its two
 // one-sided areas, (left / full + right / full) / 2, the same expression in the same order from
@@ -289,6 +289,119 @@ __global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, co
       }
     }
     __syncthreads();  // the next tile reuses own, halo and res
+  }
+}
+
+// The resolved faces in 3D, marching z: a CTA owns a column of FZ_X x FZ_Y cells and FZ_KZ slices.
+// Per slice it computes the next slice's one-sided areas (whose -z face is this slice's +z
+// neighbour), this slice's x and y halo, then resolves the slice and writes its rows; this
+// slice's +z areas are kept as the next slice's -z neighbours. So every plane is read once (the
+// column's first slice also reads the plane below it), with no z-halo, in two barriers per slice.
+// The areas and the resolve expression are plic_face_kernel's, so the faces are the same bits.
+constexpr int FZ_X = 32, FZ_Y = 8, FZ_KZ = 32;
+
+template <class T, bool MX>
+__global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
+                                                            const T* __restrict__ normals,
+                                                            const T* __restrict__ intercepts,
+                                                            const uint8_t* __restrict__ valid) {
+  constexpr int X = FZ_X, Y = FZ_Y, NF = 6;
+  static_assert(X * Y == NT, "one cell of the slice per thread");
+  __shared__ T bufA[NF][NT], bufB[NF][NT];
+  __shared__ T prev5[NT];                   // the slice below's +z areas
+  __shared__ T hx[2][Y], hy[2][X];          // this slice's x and y halo
+  __shared__ __align__(16) T res[NT * NF];  // resolved fractions, cell-major as in the column
+  const long long n[3] = {g.n[0], g.n[1], g.n[2]};
+  const T* vf = static_cast<const T*>(cols.vf);
+  T* ff = static_cast<T*>(cols.ff);
+  const T cs[3] = {g.d[0], g.d[1], g.d[2]};
+  const unsigned ntx = unsigned((n[0] + X - 1) / X), nty = unsigned((n[1] + Y - 1) / Y);
+  unsigned b = blockIdx.x;
+  const unsigned bx = b % ntx;
+  b /= ntx;
+  const unsigned by = b % nty;
+  b /= nty;
+  const long long i0 = (long long)bx * X, j0 = (long long)by * Y, k0 = (long long)b * FZ_KZ;
+  const long long k1 = k0 + FZ_KZ < n[2] ? k0 + FZ_KZ : n[2];
+  const int q = threadIdx.x, lx = q % X, ly = q / X;
+  const long long ix = i0 + lx, jy = j0 + ly;
+  const bool inxy = ix < n[0] && jy < n[1];
+  auto area_of = [&](long long ci, int f) {
+    return face_area<T, 3, MX>(normals + 3 * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, f);
+  };
+  auto own6 = [&](T (*buf)[NT], long long k) {  // this thread's cell of slice k, all six faces
+    if (!inxy) return;
+    const long long ci = ix + n[0] * (jy + n[1] * k);
+    const T nrm[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
+    const T a = intercepts[ci], fr = vf[ci];
+    const bool ok = valid[ci] != 0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) buf[f][q] = face_area<T, 3, MX>(nrm, a, fr, ok, cs, f);
+  };
+  T (*cur)[NT] = bufA;
+  T (*nxt)[NT] = bufB;
+  own6(cur, k0);
+  if (inxy && k0 >= 1) prev5[q] = area_of(ix + n[0] * (jy + n[1] * (k0 - 1)), 5);
+  for (long long k = k0; k < k1; ++k) {
+    if (k + 1 < n[2]) own6(nxt, k + 1);
+    for (int h = q; h < 2 * Y + 2 * X; h += NT) {
+      if (h < 2 * Y) {
+        const int side = h / Y, y = h % Y;
+        const long long ii = side == 0 ? i0 - 1 : i0 + X, jj = j0 + y;
+        if (ii >= 0 && ii < n[0] && jj < n[1]) hx[side][y] = area_of(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
+      } else {
+        const int side = (h - 2 * Y) / X, x = (h - 2 * Y) % X;
+        const long long ii = i0 + x, jj = side == 0 ? j0 - 1 : j0 + Y;
+        if (jj >= 0 && jj < n[1] && ii < n[0]) hy[side][x] = area_of(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
+      }
+    }
+    __syncthreads();
+    if (inxy) {
+      const long long idx[3] = {ix, jy, k};
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const int c = f >> 1;
+        const int o1 = c == 0 ? 1 : 0, o2 = c == 2 ? 1 : 2;
+        const T full = (T(1) * cs[o1]) * cs[o2];
+        const T mine = cur[f][q];
+        T r;
+        if ((f & 1) == 0) {
+          const bool has = idx[c] >= 1;
+          T below = T(0);
+          if (has) below = c == 0 ? (lx > 0 ? cur[1][q - 1] : hx[0][ly])
+                                  : c == 1 ? (ly > 0 ? cur[3][q - X] : hy[0][lx]) : prev5[q];
+          r = has ? (frac_of(below, full) + frac_of(mine, full)) * T(0.5) : frac_of(mine, full);
+        } else {
+          const bool has = idx[c] <= n[c] - 2;
+          T above = T(0);
+          if (has) above = c == 0 ? (lx < X - 1 ? cur[0][q + 1] : hx[1][ly])
+                                  : c == 1 ? (ly < Y - 1 ? cur[2][q + X] : hy[1][lx]) : nxt[4][q];
+          r = has ? (frac_of(mine, full) + frac_of(above, full)) * T(0.5) : frac_of(mine, full);
+        }
+        res[q * NF + f] = r;
+      }
+    }
+    __syncthreads();
+    // the slice's rows leave whole (16-byte vectors where the row is full and aligned)
+    const int rowcells = (int)(n[0] - i0 < X ? n[0] - i0 : X);
+    constexpr int RV = X * NF * int(sizeof(T)) / 16;
+    for (int w = q; w < Y * RV; w += NT) {
+      const int row = w / RV, v = w - row * RV;
+      const long long j = j0 + row;
+      if (j >= n[1]) continue;
+      const long long c0 = i0 + n[0] * (j + n[1] * k);
+      if (rowcells == X && (reinterpret_cast<uintptr_t>(ff + NF * c0) & 15u) == 0) {
+        reinterpret_cast<uint4*>(ff + NF * c0)[v] = reinterpret_cast<const uint4*>(res + row * X * NF)[v];
+      } else {
+        constexpr int PER = 16 / int(sizeof(T));
+        for (int e = v * PER; e < (v + 1) * PER; ++e)
+          if (e < rowcells * NF) ff[NF * c0 + e] = res[row * X * NF + e];
+      }
+    }
+    if (inxy) prev5[q] = cur[5][q];
+    T (*t)[NT] = cur;
+    cur = nxt;
+    nxt = t;
   }
 }
 
@@ -486,12 +599,16 @@ cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& co
       e = cudaFuncSetAttribute(plic_fit_kernel<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
   }
+  // 3D faces march z, one CTA per FZ_X x FZ_Y x FZ_KZ column; 2D faces work in tiles
+  const long long zcols = ((g.n[0] + FZ_X - 1) / FZ_X) * ((g.n[1] + FZ_Y - 1) / FZ_Y) * ((g.n[2] + FZ_KZ - 1) / FZ_KZ);
   if (mixed && sizeof(T) == 4) {
     plic_fit_kernel<T, D, true><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
-    plic_face_kernel<T, D, true><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+    if constexpr (D == 3) plic_face_z_kernel<T, true><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+    else plic_face_kernel<T, D, true><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
   } else {
     plic_fit_kernel<T, D, false><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
-    plic_face_kernel<T, D, false><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+    if constexpr (D == 3) plic_face_z_kernel<T, false><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+    else plic_face_kernel<T, D, false><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
   }
   return cudaGetLastError();
 }

@@ -62,6 +62,10 @@ def test_plic_bitwise(prec):
              (cc.workloads.unit_grid(40), cc.workloads.sphere_cloud(1, 64)),
              (cc.CartesianGrid((-1.5, -1.5), (3, 3), (1.0, 1.0)), cc.Circle((0.0, 0.0), 1.0)),
              (cc.workloads.unit_grid(36), cc.workloads.smooth_blob(5)),
+             # ragged 3D: partial x / y tiles, several z columns, a z remainder
+             (cc.CartesianGrid((-0.1, -0.05, 0.02), (37, 19, 45), (0.028,) * 3), cc.workloads.sphere_cloud(2, 16)),
+             (cc.CartesianGrid((0.0, 0.0, 0.0), (33, 9, 70), (0.03,) * 3),
+              cc.Sphere((0.5, 0.13, 1.05), 0.4)),
              (cc.CartesianIsoGrid((-0.6, -0.6), (0.6, 0.6), 0.04),
               cc.SmoothUnion(cc.Circle((0.1, 0.0), 0.3), cc.Box((-0.2, 0.1), (0.15, 0.2)),
                              cc.Subtraction(cc.Circle((0.0, -0.2), 0.3), cc.Circle((0.0, -0.3), 0.1)), k=0.05))]
