@@ -509,6 +509,57 @@ __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, con
   }
 }
 
+// calc_volume in 3D, marching z: persistent CTAs take FZ_X x FZ_Y x FZ_KZ columns and prune a union
+// of spheres once per slab of FIT_S slices, as the 3D fit pass does (the same fractions; the sum
+// is the same compensated accumulation, in another order).
+template <class T, bool MX>
+__global__ void __launch_bounds__(NT) calc_volume_z_kernel(const DevGrid<T> g, const DevTape tape, double* partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_count;
+  const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
+  __syncthreads();
+  constexpr int X = FZ_X, Y = FZ_Y;
+  const long long n[3] = {g.n[0], g.n[1], g.n[2]};
+  const unsigned ntx = unsigned((n[0] + X - 1) / X), nty = unsigned((n[1] + Y - 1) / Y);
+  const unsigned ncol = ntx * nty * unsigned((n[2] + FZ_KZ - 1) / FZ_KZ);
+  const int q = threadIdx.x;
+  KSum acc{0.0, 0.0};
+  for (unsigned col = blockIdx.x; col < ncol; col += gridDim.x) {
+    unsigned b = col;
+    const unsigned bx = b % ntx;
+    b /= ntx;
+    const unsigned by = b % nty;
+    b /= nty;
+    const long long i0 = (long long)bx * X, j0 = (long long)by * Y, k0 = (long long)b * FZ_KZ;
+    const long long k1 = k0 + FZ_KZ < n[2] ? k0 + FZ_KZ : n[2];
+    const long long ix = i0 + q % X, jy = j0 + q / X;
+    const bool inxy = ix < n[0] && jy < n[1];
+    for (long long ks = k0; ks < k1; ks += FIT_S) {
+      const long long first[3] = {i0, j0, ks};
+      const int ext[3] = {X, Y, FIT_S};
+      const STape<T> u = box_tape<T, 3>(t, tape, g, first, ext, smem, &s_count);
+      const long long ke = ks + FIT_S < k1 ? ks + FIT_S : k1;
+      if (inxy)
+        for (long long k = ks; k < ke; ++k) {
+          const long long idx[3] = {ix, jy, k};
+          acc.add(double(cell_plane<T, 3, MX>(u, g, idx).fraction));
+        }
+      __syncthreads();  // the next slab's pruning overwrites the ops this one read
+    }
+  }
+  __shared__ double ss[NT], sc[NT];
+  ss[threadIdx.x] = acc.s;
+  sc[threadIdx.x] = acc.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    KSum r{0.0, 0.0};
+    double cc = 0.0;
+    for (int i = 0; i < NT; ++i) { r.add(ss[i]); cc += sc[i]; }
+    partial[2 * blockIdx.x] = r.s;
+    partial[2 * blockIdx.x + 1] = r.c + cc;
+  }
+}
+
 __global__ void calc_volume_final(const double* partial, int nb, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   KSum b{0.0, 0.0};
@@ -693,14 +744,25 @@ template <class T, int D>
 cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double* partial, double* out,
                                cudaStream_t s, bool mixed) {
   const int sm = CentroidSmem::of(tape).bytes;
-  if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(calc_volume_kernel<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(calc_volume_kernel<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e != cudaSuccess) return e;
+  if constexpr (D == 3) {
+    if (sm > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(calc_volume_z_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(calc_volume_z_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e != cudaSuccess) return e;
+    }
+    if (mixed && sizeof(T) == 4) calc_volume_z_kernel<T, true><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+    else calc_volume_z_kernel<T, false><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+  } else {
+    if (sm > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(calc_volume_kernel<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(calc_volume_kernel<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e != cudaSuccess) return e;
+    }
+    if (mixed && sizeof(T) == 4) calc_volume_kernel<T, D, true><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
+    else calc_volume_kernel<T, D, false><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
   }
-  if (mixed && sizeof(T) == 4) calc_volume_kernel<T, D, true><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
-  else calc_volume_kernel<T, D, false><<<VOL_BLOCKS, NT, sm, s>>>(g, tape, partial);
   calc_volume_final<<<1, 32, 0, s>>>(partial, VOL_BLOCKS, out);
   return cudaGetLastError();
 }
