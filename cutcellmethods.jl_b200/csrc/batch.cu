@@ -114,8 +114,7 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
         }
         __syncthreads();
         const T cs[2] = {dx, dy};
-        for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) {
-          const int a = c % A.tx, b = c / A.tx;
+        auto cell = [&](int a, int b) {
           const long long i = i0 + a, j = j0 + b;
           if (i < n0 && j < n1) {
             const T xa = node_coord(gx0, dx, i), xb = node_coord(gx0, dx, i + 1);
@@ -125,6 +124,14 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
                              node[a + nxn * (b + 1)]};
             ms_cell<T, MX>(nd, ph, cs, I.cols, i + n0 * j);
           }
+        };
+        if (sizeof(T) == 4 && nt % A.tx == 0) {
+          // the block covers whole tile rows: a thread keeps its column and steps through rows
+          // (Float32 only: measured, the Float64 instantiation runs 6% slower this way)
+          const int a = threadIdx.x % A.tx, step = nt / A.tx;
+          for (int b = threadIdx.x / A.tx; b < A.ty; b += step) cell(a, b);
+        } else {
+          for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) cell(c % A.tx, c / A.tx);
         }
       } else {
         // one chunk of tree leaves, a leaf per thread (as ms_tree_kernel)
