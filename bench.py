@@ -165,6 +165,23 @@ def config(args):
             "l2": "each step writes >14 GB (outputs larger than L2), no flush needed"}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's x: a multi-GPU time is the slowest rank's. Every rank must call
+    it at the same point (it is a collective); alone, x itself."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, cells_per_rank: int, seconds: float) -> float:
+    """Whole-job cells/s: every rank updates its own replica of cells_per_rank cells (weak scaling),
+    in the slowest rank's time."""
+    return world * cells_per_rank / seconds
+
+
 def run_ours(args, rank, world, dist):
     import ctypes as C
     import torch
@@ -204,12 +221,9 @@ def run_ours(args, rank, world, dist):
     # clocks are sampled over every timed region (Float32, end to end, Float64, learned)
     clk = ClockSampler(dev.index, period_ms=100).__enter__()
     cache, total_ms, per = timed_updates(torch.float32)
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     ms = total_ms / args.steps
-    value = world * n ** 3 / (ms * 1e-3)
+    value = job_rate(world, n ** 3, ms * 1e-3)
     elem = 4
     bytes_per = cc.workloads.mc_bytes_per_update(n, elem)
     avg = statistics.mean(per)
@@ -224,19 +238,15 @@ def run_ours(args, rank, world, dist):
     for _ in range(args.steps):
         cc.update_cache(cache, body, g)  # flattens the host body and uploads it every step
         rep = cc.cut_cell_report(cache)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, dist, dev)
     ops_bytes = tape.ops.nbytes + tape.params.nbytes
 
     # Float64 and mixed precision at the same size, then every field's error against Float64
     cache64, total64, per64 = timed_updates(torch.float64)
-    ms64 = total64 / args.steps
+    ms64 = max_over_ranks(total64, dist, dev) / args.steps
     bytes64 = cc.workloads.mc_bytes_per_update(n, 8)
     cachem, totalm, perm = timed_updates(torch.float32, "mixed")
-    msm = totalm / args.steps
+    msm = max_over_ranks(totalm, dist, dev) / args.steps
     precision = {"reference": "the Float64 update of the same body and grid (bit-identical to the Float64 oracle)",
                  "float32": field_errors(cache, cache64), "mixed": field_errors(cachem, cache64)}
     del cache, cache64, cachem
@@ -261,13 +271,13 @@ def run_ours(args, rank, world, dist):
                          "algorithmic_bytes_per_launch": bytes_per,
                          "per": "one update (fill + cut-band launch), CUDA events",
                          "traffic_source": "ncu dram__bytes_read+write of fill and cut at 256^3, scaled by cells"},
-            "e2e": {"value": world * n ** 3 / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(ops_bytes),
+            "e2e": {"value": job_rate(world, n ** 3, e2e_s), "unit": "cells/s", "h2d_bytes_per_step": int(ops_bytes),
                     "d2h_bytes_per_step": 48},
             "gpu_launches": 2 * args.steps,  # per update: the fill kernel and the cut-band kernel
             "clocks": clocks,
-            "fp64": {"value": world * n ** 3 / (ms64 * 1e-3), "ms_per_step": ms64,
+            "fp64": {"value": job_rate(world, n ** 3, ms64 * 1e-3), "ms_per_step": ms64,
                      "roofline_frac": bytes64 / (statistics.mean(per64) * 1e-3) / 1e9 / peak},
-            "mixed": {"value": world * n ** 3 / (msm * 1e-3), "ms_per_step": msm,
+            "mixed": {"value": job_rate(world, n ** 3, msm * 1e-3), "ms_per_step": msm,
                       "roofline_frac": bytes_per / (statistics.mean(perm) * 1e-3) / 1e9 / peak},
             "precision": precision,
             "learned": learned,
