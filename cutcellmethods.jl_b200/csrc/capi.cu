@@ -322,6 +322,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->cut_count) cudaFree(h->cut_count);
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
   if (h->mesh_scan) cudaFree(h->mesh_scan);
+  if (h->mesh_list) cudaFree(h->mesh_list);
   if (h->prune) cudaFree(h->prune);
   cci::free_ms_mesh(h);
   cci::free_plic_mesh(h);

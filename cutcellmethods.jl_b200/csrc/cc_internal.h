@@ -135,6 +135,7 @@ struct MeshKey {
   cc_grid g{};
   int prec = -1;
   unsigned long long tot[3] = {0, 0, 0};
+  unsigned long long cut_nodes = 0, cut_cells = 0;  // lengths of the kept survivor lists
 };
 }  // namespace cci
 
@@ -157,6 +158,8 @@ struct cc_handle {
   size_t mesh_vbase_n = 0;
   unsigned long long* mesh_scan = nullptr;  // generate_mesh: per-block counts and offsets
   size_t mesh_scan_n = 0;
+  unsigned long long* mesh_list = nullptr;  // generate_mesh: cut nodes and cut cells in order
+  unsigned long long mesh_node_cap = 0, mesh_cell_cap = 0;
   void* prune = nullptr;  // marching cubes: per fill CTA pruned op lists of a union of spheres
   size_t prune_bytes = 0;
   void* ms_mesh = nullptr;  // marching squares: the last contour built (ms_mesh.cu)

@@ -72,25 +72,78 @@ __device__ __forceinline__ int compact(int* cand, Keep keep) {
   return (int)total;
 }
 
-// In-place exclusive scan of `n` per-block counts (`lanes` interleaved series, lanes <= 4) in one
-// CTA of MB threads; totals[l] receives series l's sum.
-template <int MB>
-__global__ void scan_series_kernel(unsigned long long* a, long long n, int lanes, unsigned long long* totals) {
-  __shared__ unsigned long long carry[4];
-  if (threadIdx.x < 4) carry[threadIdx.x] = 0;
-  __syncthreads();
-  for (int l = 0; l < lanes; ++l)
-    for (long long base = 0; base < n; base += MB) {
-      const long long q = base + threadIdx.x;
-      const unsigned long long x = q < n ? a[lanes * q + l] : 0ull;
-      unsigned long long t;
-      const unsigned long long pre = block_scan<MB>(x, &t);
-      if (q < n) a[lanes * q + l] = carry[l] + pre;
-      __syncthreads();
-      if (threadIdx.x == 0) carry[l] += t;
-      __syncthreads();
+// ---- word-parallel survivors -----------------------------------------------------------------
+// When the cheap test is a bit per item packed 32 to a word (a sign bitmap), a block owns MB * IPT
+// consecutive words, thread t taking word q*MB + t in round q, so block order is word order, and
+// round_prefix places each word's set bits among the block's.
+
+// Exclusive prefix, in block order (round, then thread), of one count per thread and round;
+// pre[q] receives this thread's and the block total is returned. The counts are 64-bit so that
+// several small counts packed in bit fields are placed by one call. Every thread of the block
+// calls it; its shared slots are free again when it returns.
+template <int MB, int IPT>
+__device__ __forceinline__ unsigned long long round_prefix(const unsigned long long (&cnt)[IPT],
+                                                           unsigned long long (&pre)[IPT]) {
+  static_assert(IPT * (MB / 32) <= MB, "one (round, warp) slot per thread");
+  constexpr int S = IPT * (MB / 32);
+  __shared__ unsigned long long slot[S];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    unsigned long long v = cnt[q];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
     }
-  if (threadIdx.x < lanes) totals[threadIdx.x] = carry[threadIdx.x];
+    pre[q] = v - cnt[q];
+    if (lane == 31) slot[q * (MB / 32) + w] = v;
+  }
+  __syncthreads();
+  unsigned long long total;
+  const unsigned long long first = block_scan<MB>(threadIdx.x < S ? slot[threadIdx.x] : 0ull, &total);
+  if (threadIdx.x < S) slot[threadIdx.x] = first;  // block_scan's closing barrier ordered the reads
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) pre[q] += slot[q * (MB / 32) + w];
+  __syncthreads();
+  return total;
+}
+
+// In-place exclusive scan of `n` per-block counts (LANES interleaved series) in one CTA of MB
+// threads, each thread taking E consecutive entries of every series per pass (all loads issued
+// before the scans); totals[l] receives series l's sum.
+template <int MB, int LANES>
+__global__ void __launch_bounds__(MB) scan_series_kernel(unsigned long long* a, long long n, unsigned long long* totals) {
+  constexpr int E = 8;
+  unsigned long long carry[LANES];  // the same in every thread
+#pragma unroll
+  for (int l = 0; l < LANES; ++l) carry[l] = 0;
+  for (long long base = 0; base < n; base += (long long)MB * E) {
+    const long long q0 = base + (long long)threadIdx.x * E;
+    unsigned long long x[LANES][E];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int l = 0; l < LANES; ++l) x[l][e] = q0 + e < n ? a[LANES * (q0 + e) + l] : 0ull;
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) {
+      unsigned long long sum = 0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) sum += x[l][e];
+      unsigned long long t;
+      unsigned long long run = carry[l] + block_scan<MB>(sum, &t);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        if (q0 + e < n) a[LANES * (q0 + e) + l] = run;
+        run += x[l][e];
+      }
+      carry[l] += t;
+    }
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int l = 0; l < LANES; ++l) totals[l] = carry[l];
 }
 
 }  // namespace cccompact

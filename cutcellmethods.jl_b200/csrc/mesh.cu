@@ -14,16 +14,21 @@
 // interior vertices, cells in linear order; triangles by cell in linear order, each cell's in
 // tile order.
 //
-// Two passes, edge vertices (nodes) and cells. Each counts per block of 8192 items, the block
-// counts are scanned, and an emit writes through in-block scans; both compact the thin band that
-// contributes (nodes with a cut edge, cut cells) per block before the long work, so it runs on
-// dense warps (compact.cuh). The count call keeps each block's survivors and the scanned offsets
-// on the handle, and an emit call that follows it for the same phi and grid, with no update in
-// between, starts from them. The edge pass keeps each surviving node's first vertex, so a cell's
-// triangles can name the vertices of edges other nodes own. Every write of an emit is checked
-// against the output capacities.
+// The surface lives in a thin band (about one node in a hundred at 512^3), so the passes first
+// find it cheaply. A sign pass reads phi once and writes one bit per node (outside or not); every
+// later test is word arithmetic on that bitmap, 32 nodes at a time: an edge crosses where its two
+// nodes' bits differ, a cell is cut where its corners' bits are not all equal. The count pass
+// sums the cut edges by popcount and runs the tile of each cut cell (triangles, interior vertex);
+// the per-block counts are scanned; the two emit passes (edge vertices, then cells) recompute the
+// block's cut bits, place them in order and hand them out to dense warps (compact.cuh), so the
+// long work -- edge crossings, tiles -- runs only on the band. The count call keeps the bitmap and
+// the scanned offsets on the handle, and an emit call that follows it for the same phi and grid,
+// with no update in between, starts from them. The edge pass keeps each surviving node's first
+// vertex, so a cell's triangles can name the vertices of edges other nodes own. Every write of an
+// emit is checked against the output capacities.
 #include <cstdint>
 #include <string>
+#include <tuple>
 #include <cuda_runtime.h>
 #include "../../include/cutcell_b200.h"
 #include "cc_device.cuh"
@@ -39,9 +44,8 @@ using cci::DevGrid;
 using cci::DevTable;
 
 constexpr int MB = 256;          // threads per block
-constexpr int IPT = 32;          // rounds per block
-constexpr int BLK = MB * IPT;    // nodes or cells per block
-constexpr int KEEP = 1024;       // survivors a block hands from the count to the emit pass
+constexpr int IPT = 4;           // rounds per block, one bitmap word per thread and round
+constexpr int BW = MB * IPT;     // bitmap words per block (32768 nodes)
 
 template <class T>
 __device__ __forceinline__ bool outside(T v) { return nudge(v) >= T(0); }
@@ -80,188 +84,88 @@ __device__ __forceinline__ void edge_vertex(const T* __restrict__ phi, const Dev
   for (int q = 0; q < 3; ++q) out[q] = fa >= T(0) ? xa[q] + s * (xb[q] - xa[q]) : xb[q] + s * (xa[q] - xb[q]);
 }
 
-// Walks item coordinates (i, j, k) over an n0 x n1 x * box from item `start + threadIdx.x` in steps
-// of MB (one 64-bit division at the start), carrying the item's node index b = i + sx j + sz k
-// (for the node box, b is the item itself; for the cell box, the cell's lower corner). Indices
-// are 32-bit: a mesh grid has fewer than 2^32 nodes. The steps are arithmetic only, so the loads
-// they address do not wait on one another.
-struct Walker {
-  unsigned v, b;
-  int i, j, k;
-  const int n0, n1;
-  const unsigned sx, sz;
-  __device__ Walker(long long start, long long n0_, long long n1_, long long sx_, long long sz_)
-      : n0(int(n0_)), n1(int(n1_)), sx(unsigned(sx_)), sz(unsigned(sz_)) {
-    const long long v64 = start + threadIdx.x;
-    v = unsigned(v64);
-    i = int(v64 % n0_);
-    j = int((v64 / n0_) % n1_);
-    k = int(v64 / (n0_ * n1_));
-    b = unsigned(i) + sx * unsigned(j) + sz * unsigned(k);
-  }
-  __device__ __forceinline__ void step() {
-    v += MB;
-    i += MB;
-    b += MB;
-    while (i >= n0) {
-      i -= n0;
-      b += sx - unsigned(n0);
-      if (++j == n1) {
-        j = 0;
-        ++k;
-        b += sz - sx * unsigned(n1);
-      }
-    }
-  }
-};
-
 // outside(v) without the nudge: |v| < eps reads as +eps, so v is outside exactly when v > -eps
 // (a NaN is neither).
 template <class T>
 __device__ __forceinline__ bool out_fast(T v) { return v > -Eps<T>::v(); }
 
-// The cheap tests, in groups of G rounds: each round's item is clamped to the box's last item
-// (past it the round answers false), and every load of the group is issued before any is tested.
-// A node has a cut edge when a neighbour along +x, +y or +z (inside the box) lies on the other side;
-// a cell is cut when its corners are not all on one side.
-template <class T, int G>
-__device__ __forceinline__ unsigned nodes_with_cut(const T* __restrict__ phi, Walker& w, unsigned nn, int m0, int m1,
-                                                   int m2, unsigned nx, unsigned nz, bool full) {
-  T p0[G], px[G], py[G], pz[G];
-  bool in[G];
-#pragma unroll
-  for (int u = 0; u < G; ++u) {
-    in[u] = full || w.v < nn;
-    const T* p = phi + (in[u] ? w.b : nn - 1);
-    p0[u] = p[0];
-    px[u] = p[in[u] && w.i < m0 ? 1u : 0u];
-    py[u] = p[in[u] && w.j < m1 ? nx : 0u];
-    pz[u] = p[in[u] && w.k < m2 ? nz : 0u];
-    w.step();
-  }
-  unsigned m = 0;
-#pragma unroll
-  for (int u = 0; u < G; ++u) {
-    const bool o = out_fast(p0[u]);
-    const bool cut = (out_fast(px[u]) != o) | (out_fast(py[u]) != o) | (out_fast(pz[u]) != o);
-    if (in[u] & cut) m |= 1u << u;
-  }
-  return m;
-}
-
-template <class T, int G>
-__device__ __forceinline__ unsigned cells_with_cut(const T* __restrict__ phi, Walker& w, unsigned nc, unsigned nx,
-                                                   unsigned nz, bool full) {
-  T c[G][8];
-  bool in[G];
-#pragma unroll
-  for (int u = 0; u < G; ++u) {
-    in[u] = full || w.v < nc;
-    const T* p = phi + (in[u] ? w.b : 0u);
-    c[u][0] = p[0]; c[u][1] = p[1]; c[u][2] = p[nx]; c[u][3] = p[nx + 1];
-    c[u][4] = p[nz]; c[u][5] = p[nz + 1]; c[u][6] = p[nz + nx]; c[u][7] = p[nz + nx + 1];
-    w.step();
-  }
-  unsigned m = 0;
-#pragma unroll
-  for (int u = 0; u < G; ++u) {
-    const bool o = out_fast(c[u][0]);
-    bool cut = false;
-#pragma unroll
-    for (int q = 1; q < 8; ++q) cut |= out_fast(c[u][q]) != o;
-    if (in[u] & cut) m |= 1u << u;
-  }
-  return m;
-}
-
-template <class T> struct Groups { static constexpr int node = 8, cell = 4; };
-template <> struct Groups<double> { static constexpr int node = 4, cell = 2; };
-
-// This block's survivors: from the count pass (kept_n >= 0) or compacted again (kept_n < 0,
-// more than KEEP). Returns their number (block-uniform).
-template <int G, class Keep>
-__device__ __forceinline__ int survivors(int* cand, const int* kept, const int* kept_n, Keep keep) {
-  int n = kept_n[blockIdx.x];
-  if (n == 0) return 0;
-  if (n > 0) {
-    for (int x = threadIdx.x; x < n; x += MB) cand[x] = kept[(size_t)blockIdx.x * KEEP + x];
-    __syncthreads();
-    return n;
-  }
-  return cccompact::compact<MB, IPT, G>(cand, keep);
-}
-
-__device__ __forceinline__ void keep_survivors(const int* cand, int n, int* kept, int* kept_n) {
-  if (threadIdx.x == 0) kept_n[blockIdx.x] = n <= KEEP ? n : -1;
-  if (n <= KEEP)
-    for (int x = threadIdx.x; x < n; x += MB) kept[(size_t)blockIdx.x * KEEP + x] = cand[x];
-}
-
-// ---- the edge vertices ----------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(MB, 4) node_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                           unsigned long long* bsum, int* kept, int* kept_n) {
-  __shared__ int cand[BLK];
-  const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
-  const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, nx, ny, nx, nx * ny);
-  const bool full = start + BLK <= nn;  // block-uniform: no item past the grid
-  const int n = cccompact::compact<MB, IPT, Groups<T>::node>(cand, [&](int) {
-    return nodes_with_cut<T, Groups<T>::node>(phi, w, unsigned(nn), int(g.n[0]), int(g.n[1]), int(g.n[2]),
-                                              unsigned(nx), unsigned(nx * ny), full);
-  });
-  keep_survivors(cand, n, kept, kept_n);
-  unsigned long long c = 0;
-  for (int x = threadIdx.x; x < n; x += MB) {
-    const long long v = start + cand[x];
-    c += __popc(node_edges(phi, v % nx, (v / nx) % ny, v / (nx * ny), g.n));
-  }
-  unsigned long long total;
-  cccompact::block_scan<MB>(c, &total);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
-}
-
-template <class T>
-__global__ void __launch_bounds__(MB, 4) node_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                          const unsigned long long* __restrict__ boff,
-                                                          const int* kept, const int* kept_n, unsigned* __restrict__ vbase,
-                                                          T* __restrict__ verts, unsigned long long vcap,
-                                                          unsigned long long* overflow) {
-  __shared__ int cand[BLK];
-  const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
-  const long long start = (long long)blockIdx.x * BLK;
-  Walker w(start, nx, ny, nx, nx * ny);
-  const bool full = start + BLK <= nn;  // block-uniform: no item past the grid
-  const int n = survivors<Groups<T>::node>(cand, kept, kept_n, [&](int) {
-    return nodes_with_cut<T, Groups<T>::node>(phi, w, unsigned(nn), int(g.n[0]), int(g.n[1]), int(g.n[2]),
-                                              unsigned(nx), unsigned(nx * ny), full);
-  });
-  unsigned long long run = boff[blockIdx.x];
-  for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
-    const int x = c0 + threadIdx.x;
-    const long long v = x < n ? start + cand[x] : 0;
-    const long long i = v % nx, j = (v / nx) % ny, k = v / (nx * ny);
-    const unsigned m = x < n ? node_edges(phi, i, j, k, g.n) : 0u;
-    unsigned long long total;
-    unsigned long long id = run + cccompact::block_scan<MB>((unsigned long long)__popc(m), &total);
-    run += total;
-    if (x >= n) continue;
-    if (id + __popc(m) > vcap) {
-      atomicOr(overflow, 1ull);
-      continue;
+// The sign bitmap. Node row r = j + ny k keeps its nx nodes in W 32-bit words, bit b of word w set
+// when node i = 32 w + b is outside (bits past nx stay clear); word u = r W + w. Rows are padded to
+// whole words so that every word lies in one row: its +y and +z neighbours are the words W and
+// W ny further on, and a 32-node test is a few word operations.
+// Quotient and remainder of a 32-bit value by a fixed divisor d >= 1 through one multiply-high
+// (division by invariant integers, Granlund and Montgomery 1994): with m = floor((2^32 - 1) / d),
+// umulhi(u, m) is floor(u / d) or one less, and a single correction step makes it exact.
+struct FastDiv {
+  unsigned d, m;
+  static FastDiv of(unsigned d) { return FastDiv{d, 0xffffffffu / d}; }
+  __device__ __forceinline__ unsigned div(unsigned u, unsigned& rem) const {
+    unsigned q = __umulhi(u, m), r = u - q * d;
+    if (r >= d) {
+      ++q;
+      r -= d;
     }
-    vbase[v] = unsigned(id);
-    for (int a = 0; a < 3; ++a) {
-      if (!(m >> a & 1u)) continue;
-      T p[3];
-      edge_vertex(phi, g, i, j, k, a, p);
-      verts[3 * id] = p[0]; verts[3 * id + 1] = p[1]; verts[3 * id + 2] = p[2];
-      ++id;
-    }
+    rem = r;
+    return q;
+  }
+};
+
+struct Signs {
+  unsigned* s;
+  unsigned W, ny, words;
+  int n0, n1, n2;
+  FastDiv byW, byny;
+};
+
+// One warp per node row: lane b tests node 32 w + b of each of the row's W words in turn and a
+// ballot forms the word. One load per lane in flight per warp, many warps per SM: on a 513^3
+// Float32 field this read 5.2 TB/s where batches of 4, 8 and 16 loads per lane read 4.8, 4.1 and
+// 3.5. No index needs a division.
+template <class T>
+__global__ void __launch_bounds__(256) sign_kernel(const T* __restrict__ phi, const Signs sg, unsigned nx,
+                                                   unsigned rows) {
+  const unsigned lane = threadIdx.x & 31u, r = blockIdx.x * 8u + (threadIdx.x >> 5);
+  if (r >= rows) return;  // warp-uniform
+  const T* __restrict__ row = phi + (size_t)nx * r;
+  unsigned* __restrict__ out = sg.s + (size_t)sg.W * r;
+  for (unsigned w = 0; w < sg.W; ++w) {
+    const unsigned i = 32u * w + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, i < nx && out_fast(row[i < nx ? i : 0u]));
+    if (lane == 0) out[w] = m;
   }
 }
 
-// ---- the cells: triangles and interior vertices ----------------------------------------------
+// The cuts of bitmap word u, one bit per node: its x, y and z edges to the next node that cross
+// the surface (ax, ay, az), and the cut cells it is the lower corner of (cell). All zero past the
+// last word. An edge crosses where its two nodes' bits differ; a cell is cut unless its eight
+// corners share node (i, j, k)'s bit, i.e. unless the (j, k) face corners agree at i and at i + 1
+// and bit i equals bit i + 1.
+struct Cuts {
+  unsigned ax, ay, az, cell;
+};
+__device__ __forceinline__ Cuts word_cuts(const Signs& sg, unsigned u) {
+  const bool in = u < sg.words;
+  const unsigned uc = in ? u : 0u;
+  unsigned w, j;
+  const unsigned r = sg.byW.div(uc, w), k = sg.byny.div(r, j);
+  const bool hx = w + 1u < sg.W, hy = int(j) < sg.n1, hz = int(k) < sg.n2;
+  const unsigned ox = hx ? 1u : 0u, oy = hy ? sg.W : 0u, oz = hz ? sg.W * sg.ny : 0u;
+  const unsigned* p = sg.s + uc;  // every address below stays inside the bitmap
+  const unsigned A = p[0], B = p[oy], C = p[oz], D = p[oy + oz];
+  unsigned An = p[ox], Bn = p[oy + ox], Cn = p[oz + ox], Dn = p[oy + oz + ox];
+  if (!hx) An = Bn = Cn = Dn = 0u;  // the row's last word: bit 31 is past n0 and masked below
+  const int lo = sg.n0 - int(32u * w);
+  const unsigned xm = lo >= 32 ? 0xffffffffu : lo <= 0 ? 0u : (1u << lo) - 1u;  // nodes with i < n0
+  Cuts c{0u, 0u, 0u, 0u};
+  if (!in) return c;
+  c.ax = (A ^ ((A >> 1) | (An << 31))) & xm;
+  c.ay = A ^ B;  // B is A itself on the last row along y, C on the last layer along z
+  c.az = A ^ C;
+  const unsigned d = (A ^ B) | (A ^ C) | (A ^ D), dn = (An ^ Bn) | (An ^ Cn) | (An ^ Dn);
+  c.cell = hy && hz ? (d | (d >> 1) | (dn << 31) | c.ax) & xm : 0u;
+  return c;
+}
+
 template <class T>
 __device__ __forceinline__ void corners(const T* __restrict__ phi, const long long n[3], long long i, long long j,
                                         long long k, T ph[8]) {
@@ -291,122 +195,215 @@ __device__ __forceinline__ int cell_tile(const T ph[8], const DevTable& tb, int&
   return tile;
 }
 
-template <class T, bool MX>
-__global__ void __launch_bounds__(MB, 4) cell_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                           const DevTable tb, unsigned long long* bsum, int* kept,
-                                                           int* kept_n) {
-  __shared__ int cand[BLK];
-  const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
-  const long long start = (long long)blockIdx.x * BLK;
-  const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
-  Walker w(start, n0, n1, nx, nz);
-  const bool full = start + BLK <= nc;  // block-uniform: no item past the grid
-  const int n = cccompact::compact<MB, IPT, Groups<T>::cell>(cand, [&](int) {
-    return cells_with_cut<T, Groups<T>::cell>(phi, w, unsigned(nc), unsigned(nx), unsigned(nz), full);
-  });
-  keep_survivors(cand, n, kept, kept_n);
-  unsigned long long t = 0, in = 0;
-  for (int x = threadIdx.x; x < n; x += MB) {
-    const long long c = start + cand[x];
-    T ph[8];
-    corners(phi, g.n, c % n0, (c / n0) % n1, c / (n0 * n1), ph);
-    int nt, it;
-    cell_tile<T, MX>(ph, tb, nt, it);
-    t += nt;
-    in += it;
+// ---- the band: per block of words, its cut nodes, their edge vertices and its cut cells -------
+__global__ void __launch_bounds__(MB) band_count_kernel(const Signs sg, unsigned long long* bsum) {
+  const unsigned u0 = blockIdx.x * unsigned(BW);
+  unsigned long long packed = 0;  // cut nodes | edge vertices << 21 | cut cells << 42, each < 2^21
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    const Cuts c = word_cuts(sg, u0 + q * MB + threadIdx.x);
+    packed += (unsigned long long)__popc(c.ax | c.ay | c.az) +
+              ((unsigned long long)(__popc(c.ax) + __popc(c.ay) + __popc(c.az)) << 21) +
+              ((unsigned long long)__popc(c.cell) << 42);
   }
-  unsigned long long tt, ti;
-  cccompact::block_scan<MB>(t, &tt);
-  cccompact::block_scan<MB>(in, &ti);
+  unsigned long long t;
+  cccompact::block_scan<MB>(packed, &t);
   if (threadIdx.x == 0) {
-    bsum[2 * blockIdx.x] = tt;
-    bsum[2 * blockIdx.x + 1] = ti;
+    bsum[3 * blockIdx.x] = t & 0x1fffffull;
+    bsum[3 * blockIdx.x + 1] = (t >> 21) & 0x1fffffull;
+    bsum[3 * blockIdx.x + 2] = t >> 42;
   }
 }
 
-template <class T, bool MX>
-__global__ void __launch_bounds__(MB, 4) cell_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
-                                                          const DevTable tb, const unsigned long long* __restrict__ boff,
-                                                          const int* kept, const int* kept_n,
-                                                          const unsigned* __restrict__ vbase,
-                                                          unsigned long long n_edge_verts, T* __restrict__ verts,
-                                                          unsigned long long vcap, int32_t* __restrict__ tris,
-                                                          unsigned long long tcap, int64_t* __restrict__ tri_cells,
-                                                          unsigned long long* overflow) {
-  __shared__ int cand[BLK];
-  const long long n0 = g.n[0], n1 = g.n[1], nc = n0 * n1 * g.n[2];
-  const long long start = (long long)blockIdx.x * BLK;
-  const long long nx = n0 + 1, nz = (n0 + 1) * (n1 + 1);
-  Walker w(start, n0, n1, nx, nz);
-  const bool full = start + BLK <= nc;  // block-uniform: no item past the grid
-  const int n = survivors<Groups<T>::cell>(cand, kept, kept_n, [&](int) {
-    return cells_with_cut<T, Groups<T>::cell>(phi, w, unsigned(nc), unsigned(nx), unsigned(nz), full);
-  });
-  unsigned long long run_t = boff[2 * blockIdx.x], run_i = n_edge_verts + boff[2 * blockIdx.x + 1];
-  for (int c0 = 0; c0 < n; c0 += MB) {  // block-uniform
-    const int x = c0 + threadIdx.x;
-    const long long c = x < n ? start + cand[x] : 0;
-    const long long i = c % n0, j = (c / n0) % n1, k = c / (n0 * n1);
-    T ph[8];
-    int nt = 0, it = 0, tile = -1;
-    if (x < n) {
-      corners(phi, g.n, i, j, k, ph);
-      tile = cell_tile<T, MX>(ph, tb, nt, it);
-    }
-    unsigned long long tot;
-    const unsigned long long pre =
-        cccompact::block_scan<MB>(((unsigned long long)nt << 32) | (unsigned long long)it, &tot);
-    unsigned long long tri_id = run_t + (pre >> 32), int_id = run_i + (pre & 0xffffffffull);
-    run_t += tot >> 32;
-    run_i += tot & 0xffffffffull;
-    if (tile < 0) continue;
-    if (tri_id + nt > tcap || (it && int_id >= vcap)) {
-      atomicOr(overflow, 1ull);
-      continue;
-    }
-    // the vertex of each of the cell's cut edges (code e + 1), from its lower node's numbering
-    unsigned vid[12];
+// Writes the block's cut nodes (node, first vertex, edge bits) and cut cells (lower node) at
+// their places in the two ordered lists, as far as the lists' capacities reach. Each word's owner
+// writes its own bits: the writes are short, and the long work runs later on the flat lists, one
+// survivor per thread.
+__global__ void __launch_bounds__(MB) band_list_kernel(const Signs sg, unsigned nx,
+                                                       const unsigned long long* __restrict__ boff,
+                                                       uint4* __restrict__ nodes, unsigned long long node_cap,
+                                                       unsigned* __restrict__ cells, unsigned long long cell_cap) {
+  const unsigned u0 = blockIdx.x * unsigned(BW);
+  const unsigned long long nb = boff[3 * blockIdx.x], vb = boff[3 * blockIdx.x + 1], cb = boff[3 * blockIdx.x + 2];
+  unsigned ax[IPT], ay[IPT], az[IPT], cm[IPT];
+  unsigned long long cnt[IPT], pre[IPT];  // cut nodes | edge vertices << 21 | cut cells << 42
 #pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    const Cuts c = word_cuts(sg, u0 + q * MB + threadIdx.x);
+    ax[q] = c.ax;
+    ay[q] = c.ay;
+    az[q] = c.az;
+    cm[q] = c.cell;
+    cnt[q] = (unsigned long long)__popc(c.ax | c.ay | c.az) +
+             ((unsigned long long)(__popc(c.ax) + __popc(c.ay) + __popc(c.az)) << 21) +
+             ((unsigned long long)__popc(c.cell) << 42);
+  }
+  cccompact::round_prefix<MB, IPT>(cnt, pre);
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    const unsigned u = u0 + q * MB + threadIdx.x;
+    if (u >= sg.words) continue;
+    unsigned w;
+    const unsigned r = sg.byW.div(u, w), v0 = 32u * w + nx * r;  // the node of bit 0
+    unsigned bits = ax[q] | ay[q] | az[q];
+    unsigned long long x = nb + (pre[q] & 0x1fffffull), vid = vb + ((pre[q] >> 21) & 0x1fffffull);
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1u;
+      const unsigned m = (ax[q] >> b & 1u) | (ay[q] >> b & 1u) << 1 | (az[q] >> b & 1u) << 2;
+      if (x < node_cap) nodes[x] = make_uint4(v0 + unsigned(b), unsigned(vid), m, 0u);
+      ++x;
+      vid += __popc(m);
+    }
+    bits = cm[q];
+    x = cb + (pre[q] >> 42);
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1u;
+      if (x < cell_cap) cells[x] = v0 + unsigned(b);
+      ++x;
+    }
+  }
+}
+
+struct NodeDiv {
+  FastDiv bynx, byny;
+};
+__device__ __forceinline__ void split_node(unsigned v, const NodeDiv& nd, long long& i, long long& j, long long& k) {
+  unsigned ri, rj;
+  const unsigned r = nd.bynx.div(v, ri), rk = nd.byny.div(r, rj);
+  i = ri;
+  j = rj;
+  k = rk;
+}
+
+// Per block of MB cut cells: its triangles and interior vertices. The list holds
+// min(*n_cells, cap) cells (the count is read on the device; blocks past it write zeros).
+template <class T, bool MX>
+__global__ void __launch_bounds__(MB) tile_count_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                        const NodeDiv nd, const DevTable tb,
+                                                        const unsigned* __restrict__ cells,
+                                                        const unsigned long long* __restrict__ n_cells,
+                                                        unsigned long long cap, unsigned long long* bsum) {
+  const unsigned long long n = *n_cells < cap ? *n_cells : cap;
+  const unsigned long long x = (unsigned long long)blockIdx.x * MB + threadIdx.x;
+  unsigned long long nt_it = 0;
+  if (x < n) {
+    long long i, j, k;
+    split_node(cells[x], nd, i, j, k);
+    T ph[8];
+    corners(phi, g.n, i, j, k, ph);
+    int nt, it;
+    cell_tile<T, MX>(ph, tb, nt, it);
+    nt_it = ((unsigned long long)nt << 32) | (unsigned long long)it;
+  }
+  unsigned long long t;
+  cccompact::block_scan<MB>(nt_it, &t);
+  if (threadIdx.x == 0) {
+    bsum[2 * blockIdx.x] = t >> 32;
+    bsum[2 * blockIdx.x + 1] = t & 0xffffffffull;
+  }
+}
+
+// ---- the edge vertices: one cut node per thread ----------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(MB) node_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                       const NodeDiv nd, const uint4* __restrict__ nodes, unsigned long long n,
+                                                       unsigned* __restrict__ vbase, T* __restrict__ verts,
+                                                       unsigned long long vcap, unsigned long long* overflow) {
+  const unsigned long long x = (unsigned long long)blockIdx.x * MB + threadIdx.x;
+  if (x >= n) return;
+  const uint4 e = nodes[x];
+  unsigned long long id = e.y;
+  long long i, j, k;
+  split_node(e.x, nd, i, j, k);
+  if (id + __popc(e.z) > vcap) {
+    atomicOr(overflow, 1ull);
+    return;
+  }
+  vbase[e.x] = unsigned(id);
+  for (int a = 0; a < 3; ++a) {
+    if (!(e.z >> a & 1u)) continue;
+    T p[3];
+    edge_vertex(phi, g, i, j, k, a, p);
+    verts[3 * id] = p[0]; verts[3 * id + 1] = p[1]; verts[3 * id + 2] = p[2];
+    ++id;
+  }
+}
+
+// ---- the cells: triangles and interior vertices, one cut cell per thread ----------------------
+template <class T, bool MX>
+__global__ void __launch_bounds__(MB) cell_emit_kernel(const T* __restrict__ phi, const DevGrid<T> g,
+                                                       const NodeDiv nd, const DevTable tb,
+                                                       const unsigned* __restrict__ cells, unsigned long long n,
+                                                       const unsigned long long* __restrict__ boff,
+                                                       const unsigned* __restrict__ vbase,
+                                                       unsigned long long n_edge_verts, T* __restrict__ verts,
+                                                       unsigned long long vcap, int32_t* __restrict__ tris,
+                                                       unsigned long long tcap, int64_t* __restrict__ tri_cells,
+                                                       unsigned long long* overflow) {
+  const unsigned long long x = (unsigned long long)blockIdx.x * MB + threadIdx.x;
+  const unsigned long long tri0 = boff[2 * blockIdx.x], int0 = n_edge_verts + boff[2 * blockIdx.x + 1];
+  long long i = 0, j = 0, k = 0;
+  T ph[8];
+  int nt = 0, it = 0, tile = -1;
+  if (x < n) {
+    split_node(cells[x], nd, i, j, k);
+    corners(phi, g.n, i, j, k, ph);
+    tile = cell_tile<T, MX>(ph, tb, nt, it);
+  }
+  unsigned long long tot;
+  const unsigned long long pre = cccompact::block_scan<MB>(((unsigned long long)nt << 32) | (unsigned long long)it, &tot);
+  unsigned long long tri_id = tri0 + (pre >> 32);
+  const unsigned long long int_id = int0 + (pre & 0xffffffffull);
+  if (tile < 0) return;
+  if (tri_id + nt > tcap || (it && int_id >= vcap)) {
+    atomicOr(overflow, 1ull);
+    return;
+  }
+  const long long c = i + g.n[0] * (j + g.n[1] * k);
+  // the vertex of each of the cell's cut edges (code e + 1), from its lower node's numbering
+  unsigned vid[12];
+#pragma unroll
+  for (int e = 0; e < 12; ++e) {
+    const int ca = edge_node(e, 0), cb = edge_node(e, 1);
+    vid[e] = 0;
+    if ((ph[ca] >= T(0)) == (ph[cb] >= T(0))) continue;
+    const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
+    const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
+    const long long li = i + cbit(lo, 0), lj = j + cbit(lo, 1), lk = k + cbit(lo, 2);
+    const unsigned m = node_edges(phi, li, lj, lk, g.n);
+    const long long v = li + (g.n[0] + 1) * (lj + (g.n[1] + 1) * lk);
+    vid[e] = vbase[v] + __popc(m & ((1u << a) - 1u));
+  }
+  unsigned centre = 0;
+  if (it) {
+    centre = unsigned(int_id);
+    T acc[3] = {T(0), T(0), T(0)};
+    int ncr = 0;
     for (int e = 0; e < 12; ++e) {
       const int ca = edge_node(e, 0), cb = edge_node(e, 1);
-      vid[e] = 0;
       if ((ph[ca] >= T(0)) == (ph[cb] >= T(0))) continue;
       const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
       const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
-      const long long li = i + cbit(lo, 0), lj = j + cbit(lo, 1), lk = k + cbit(lo, 2);
-      const unsigned m = node_edges(phi, li, lj, lk, g.n);
-      const long long v = li + (g.n[0] + 1) * (lj + (g.n[1] + 1) * lk);
-      vid[e] = vbase[v] + __popc(m & ((1u << a) - 1u));
+      T p[3];
+      edge_vertex(phi, g, i + cbit(lo, 0), j + cbit(lo, 1), k + cbit(lo, 2), a, p);
+      acc[0] = acc[0] + p[0]; acc[1] = acc[1] + p[1]; acc[2] = acc[2] + p[2];
+      ++ncr;
     }
-    unsigned centre = 0;
-    if (it) {
-      centre = unsigned(int_id);
-      T acc[3] = {T(0), T(0), T(0)};
-      int ncr = 0;
-      for (int e = 0; e < 12; ++e) {
-        const int ca = edge_node(e, 0), cb = edge_node(e, 1);
-        if ((ph[ca] >= T(0)) == (ph[cb] >= T(0))) continue;
-        const int a = cbit(ca, 0) != cbit(cb, 0) ? 0 : (cbit(ca, 1) != cbit(cb, 1) ? 1 : 2);
-        const int lo = cbit(ca, a) < cbit(cb, a) ? ca : cb;
-        T p[3];
-        edge_vertex(phi, g, i + cbit(lo, 0), j + cbit(lo, 1), k + cbit(lo, 2), a, p);
-        acc[0] = acc[0] + p[0]; acc[1] = acc[1] + p[1]; acc[2] = acc[2] + p[2];
-        ++ncr;
-      }
-      verts[3 * (long long)centre] = acc[0] / T(ncr);
-      verts[3 * (long long)centre + 1] = acc[1] / T(ncr);
-      verts[3 * (long long)centre + 2] = acc[2] / T(ncr);
-    }
-    const cc_mc_tile tl = tb.tiles[tile];
-    const uint8_t* codes = tb.codes + tl.code_off;
-    for (int r = 0; r < tl.ntris; ++r, ++tri_id) {
+    verts[3 * (long long)centre] = acc[0] / T(ncr);
+    verts[3 * (long long)centre + 1] = acc[1] / T(ncr);
+    verts[3 * (long long)centre + 2] = acc[2] / T(ncr);
+  }
+  const cc_mc_tile tl = tb.tiles[tile];
+  const uint8_t* codes = tb.codes + tl.code_off;
+  for (int r = 0; r < tl.ntris; ++r, ++tri_id) {
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int code = codes[3 * r + q];
-        tris[3 * tri_id + q] = int32_t(code == 13 ? centre : vid[code - 1]);
-      }
-      if (tri_cells) tri_cells[tri_id] = c;
+    for (int q = 0; q < 3; ++q) {
+      const int code = codes[3 * r + q];
+      tris[3 * tri_id + q] = int32_t(code == 13 ? centre : vid[code - 1]);
     }
+    if (tri_cells) tri_cells[tri_id] = c;
   }
 }
 
@@ -434,11 +431,12 @@ template <class T, bool MX>
 cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int64_t vcap, int32_t* tris, int64_t tcap,
                    int64_t* tri_cells, int64_t* nv, int64_t* nt, cudaStream_t s) {
   const DevGrid<T> g = grid_of<T>(gg);
-  const long long nn = (g.n[0] + 1) * (g.n[1] + 1) * (g.n[2] + 1);
-  const long long nc = g.n[0] * g.n[1] * g.n[2];
-  const long long nbn = (nn + BLK - 1) / BLK, nbc = (nc + BLK - 1) / BLK;
-  // 32-bit item indices, with room for the last block's rounds past the end
-  if (nn > 0xffffffffLL - BLK) return fail(CC_TOO_LARGE, "generate_mesh takes fewer than 2^32 - 8192 nodes");
+  const long long nx = g.n[0] + 1, ny = g.n[1] + 1, nn = nx * ny * (g.n[2] + 1);
+  const long long W = (nx + 31) / 32, words = W * ny * (g.n[2] + 1);
+  const long long nb = (words + BW - 1) / BW;
+  // 32-bit node and word indices, with room for the last block's words past the end
+  if (nn > 0xffffffffLL || words > 0xffffffffLL - BW)
+    return fail(CC_TOO_LARGE, "generate_mesh takes fewer than 2^32 nodes");
   cci::MeshKey& key = h->mesh_key;
   cudaError_t e = cudaSuccess;
   if (size_t(nn) > h->mesh_vbase_n) {
@@ -450,11 +448,11 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
       return cuda_fail(e, "generate_mesh scratch");
     h->mesh_vbase_n = size_t(nn);
   }
-  // 64-bit words: node block offsets, cell block offsets (tris, interior) interleaved, 3 totals,
-  // the overflow flag; then 32-bit: node kept_n, node kept, cell kept_n, cell kept
-  const size_t words = size_t(nbn + 2 * nbc + 4);
-  const size_t ints = size_t(nbn) * (KEEP + 1) + size_t(nbc) * (KEEP + 1);
-  const size_t scan_n = words + (ints + 1) / 2;
+  // 64-bit words: per word block (cut nodes, edge vertices, cut cells) interleaved, their 3
+  // totals, the 2 tile totals (triangles, interior vertices), the overflow flag; then the sign
+  // bitmap, 32-bit words
+  const size_t head = size_t(3 * nb + 6);
+  const size_t scan_n = head + size_t(words + 1) / 2;
   if (scan_n > h->mesh_scan_n) {
     if (h->mesh_scan) cudaFree(h->mesh_scan);
     h->mesh_scan = nullptr;
@@ -464,34 +462,89 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
       return cuda_fail(e, "generate_mesh scratch");
     h->mesh_scan_n = scan_n;
   }
-  unsigned long long* nb = h->mesh_scan;              // node blocks
-  unsigned long long* cb = nb + nbn;                  // cell blocks (tris, interior) interleaved
-  unsigned long long* tot = cb + 2 * nbc;             // edge vertices, tris, interior vertices
-  unsigned long long* overflow = tot + 3;
-  int* node_kept_n = reinterpret_cast<int*>(h->mesh_scan + words);
-  int* node_kept = node_kept_n + nbn;
-  int* cell_kept_n = node_kept + size_t(nbn) * KEEP;
-  int* cell_kept = cell_kept_n + nbc;
+  unsigned long long* bsum = h->mesh_scan;  // per word block, then scanned in place
+  unsigned long long* tot = bsum + 3 * nb;  // cut nodes, edge vertices, cut cells
+  unsigned long long* tot2 = tot + 3;       // triangles, interior vertices
+  unsigned long long* overflow = tot2 + 2;
+  Signs sg;
+  sg.s = reinterpret_cast<unsigned*>(h->mesh_scan + head);
+  sg.W = unsigned(W);
+  sg.ny = unsigned(ny);
+  sg.words = unsigned(words);
+  sg.n0 = int(g.n[0]);
+  sg.n1 = int(g.n[1]);
+  sg.n2 = int(g.n[2]);
+  sg.byW = FastDiv::of(unsigned(W));
+  sg.byny = FastDiv::of(unsigned(ny));
+  const NodeDiv nd{FastDiv::of(unsigned(nx)), FastDiv::of(unsigned(ny))};
   const bool emit = verts || tris;
   bool reuse = emit && key.valid && key.generation == h->generation && key.phi == phi && key.prec == h->prec;
   for (int a = 0; a < 3 && reuse; ++a)
     reuse = key.g.n[a] == gg->n[a] && key.g.x0[a] == gg->x0[a] && key.g.d[a] == gg->d[a];
   unsigned long long t[3] = {key.tot[0], key.tot[1], key.tot[2]};
+  unsigned long long n_nodes = key.cut_nodes, n_cells = key.cut_cells;
+  // the lists, at the capacities kept on the handle: cut nodes (16 B each), per tile block
+  // (triangles, interior vertices), cut cells (4 B each)
+  auto lists = [&]() {
+    const unsigned long long nc = h->mesh_node_cap, cc = h->mesh_cell_cap, ntb = (cc + MB - 1) / MB;
+    return std::make_tuple(reinterpret_cast<uint4*>(h->mesh_list), h->mesh_list + 2 * nc,
+                           reinterpret_cast<unsigned*>(h->mesh_list + 2 * nc + 2 * ntb), ntb);
+  };
   if (!reuse) {
     key.valid = false;
-    node_count_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, node_kept, node_kept_n);
-    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(nb, nbn, 1, tot);
-    cell_count_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, cell_kept, cell_kept_n);
-    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(cb, nbc, 2, tot + 1);
-    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(t, tot, sizeof t, cudaMemcpyDeviceToHost, s);
+    const long long rows = ny * (g.n[2] + 1);
+    sign_kernel<T><<<unsigned((rows + 7) / 8), 256, 0, s>>>(phi, sg, unsigned(nx), unsigned(rows));
+    band_count_kernel<<<unsigned(nb), MB, 0, s>>>(sg, bsum);
+    cccompact::scan_series_kernel<512, 3><<<1, 512, 0, s>>>(bsum, nb, tot);
+    // the list pass and the tile counts, into the lists as they are; run again below when the
+    // surface has outgrown them (the first call on a handle, or a larger surface)
+    auto list_pass = [&]() {
+      auto [nodes, tsum, cells, ntb] = lists();
+      band_list_kernel<<<unsigned(nb), MB, 0, s>>>(sg, unsigned(nx), bsum, nodes, h->mesh_node_cap, cells,
+                                                   h->mesh_cell_cap);
+      if (ntb > 0) {
+        tile_count_kernel<T, MX><<<unsigned(ntb), MB, 0, s>>>(phi, g, nd, h->tb, cells, tot + 2, h->mesh_cell_cap,
+                                                             tsum);
+        cccompact::scan_series_kernel<512, 2><<<1, 512, 0, s>>>(tsum, (long long)ntb, tot2);
+      } else {
+        cudaMemsetAsync(tot2, 0, 2 * sizeof(unsigned long long), s);
+      }
+    };
+    unsigned long long c5[5];  // cut nodes, edge vertices, cut cells, triangles, interior vertices
+    if (h->mesh_list) list_pass();
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(c5, tot, sizeof c5, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "generate_mesh count");
+    n_nodes = c5[0];
+    n_cells = c5[2];
+    if (!h->mesh_list || n_nodes > h->mesh_node_cap || n_cells > h->mesh_cell_cap) {
+      // grow with an eighth to spare, so that a slightly larger surface next time fits
+      const unsigned long long nc = n_nodes + n_nodes / 8 + 1024, cc = n_cells + n_cells / 8 + 1024;
+      const size_t list_n = size_t(2 * nc + 2 * ((cc + MB - 1) / MB) + (cc + 1) / 2);
+      if (h->mesh_list) cudaFree(h->mesh_list);
+      h->mesh_list = nullptr;
+      h->mesh_node_cap = h->mesh_cell_cap = 0;
+      if ((e = cudaMalloc(&h->mesh_list, list_n * sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(e, "generate_mesh scratch");
+      h->mesh_node_cap = nc;
+      h->mesh_cell_cap = cc;
+      list_pass();
+      if ((e = cudaGetLastError()) == cudaSuccess)
+        e = cudaMemcpyAsync(c5 + 3, tot2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return cuda_fail(e, "generate_mesh count");
+    }
+    t[0] = c5[1];
+    t[1] = c5[3];
+    t[2] = c5[4];
     key.valid = true;
     key.generation = h->generation;
     key.phi = phi;
     key.prec = h->prec;
     key.g = *gg;
     for (int q = 0; q < 3; ++q) key.tot[q] = t[q];
+    key.cut_nodes = n_nodes;
+    key.cut_cells = n_cells;
   }
   const long long n_vert = (long long)(t[0] + t[2]), n_tri = (long long)t[1];
   if (nv) *nv = n_vert;
@@ -500,16 +553,19 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
   if (!verts || !tris || vcap < n_vert || tcap < n_tri)
     return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
   if (n_vert > 0xffffffffLL) return fail(CC_TOO_LARGE, "generate_mesh numbers at most 2^32 - 1 vertices");
+  auto [nodes, tsum, cells, ntb_cap] = lists();
+  (void)ntb_cap;
+  const unsigned long long ntb = (n_cells + MB - 1) / MB;
   unsigned long long flag = 0;
   e = cudaMemsetAsync(overflow, 0, sizeof(unsigned long long), s);
-  if (e == cudaSuccess) {
-    node_emit_kernel<T><<<unsigned(nbn), MB, 0, s>>>(phi, g, nb, node_kept, node_kept_n, h->mesh_vbase, verts,
-                                                     (unsigned long long)vcap, overflow);
-    cell_emit_kernel<T, MX><<<unsigned(nbc), MB, 0, s>>>(phi, g, h->tb, cb, cell_kept, cell_kept_n, h->mesh_vbase, t[0],
-                                                         verts, (unsigned long long)vcap, tris,
-                                                         (unsigned long long)tcap, tri_cells, overflow);
-    e = cudaGetLastError();
-  }
+  if (e == cudaSuccess && n_nodes > 0)
+    node_emit_kernel<T><<<unsigned((n_nodes + MB - 1) / MB), MB, 0, s>>>(phi, g, nd, nodes, n_nodes, h->mesh_vbase, verts,
+                                                                        (unsigned long long)vcap, overflow);
+  if (e == cudaSuccess && n_cells > 0)
+    cell_emit_kernel<T, MX><<<unsigned(ntb), MB, 0, s>>>(phi, g, nd, h->tb, cells, n_cells, tsum, h->mesh_vbase, t[0],
+                                                        verts, (unsigned long long)vcap, tris, (unsigned long long)tcap,
+                                                        tri_cells, overflow);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, overflow, sizeof flag, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   key.valid = false;  // one emit per count

@@ -423,7 +423,7 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
   if (!reuse) {
     st->valid = false;
     plic_count_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, kept, kept_n);
-    cccompact::scan_series_kernel<MB><<<1, MB, 0, s>>>(bsum, nb, 2, bsum + 2 * nb);
+    cccompact::scan_series_kernel<MB, 2><<<1, MB, 0, s>>>(bsum, nb, bsum + 2 * nb);
     if ((e = cudaGetLastError()) == cudaSuccess)
       e = cudaMemcpyAsync(tot, bsum + 2 * nb, sizeof tot, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
