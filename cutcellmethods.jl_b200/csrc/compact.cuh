@@ -111,32 +111,30 @@ __device__ __forceinline__ unsigned long long round_prefix(const unsigned long l
 }
 
 // In-place exclusive scan of `n` per-block counts (LANES interleaved series) in one CTA of MB
-// threads, each thread taking E consecutive entries of every series per pass (all loads issued
-// before the scans); totals[l] receives series l's sum.
-template <int MB, int LANES>
+// threads, E * MB entries per pass taken round-major (entry base + e*MB + t in round e, so the
+// loads coalesce and are all issued before the scans) and placed by round_prefix; totals[l]
+// receives series l's sum.
+template <int MB, int LANES, int E = 8>
 __global__ void __launch_bounds__(MB) scan_series_kernel(unsigned long long* a, long long n, unsigned long long* totals) {
-  constexpr int E = 8;
   unsigned long long carry[LANES];  // the same in every thread
 #pragma unroll
   for (int l = 0; l < LANES; ++l) carry[l] = 0;
   for (long long base = 0; base < n; base += (long long)MB * E) {
-    const long long q0 = base + (long long)threadIdx.x * E;
     unsigned long long x[LANES][E];
 #pragma unroll
-    for (int e = 0; e < E; ++e)
+    for (int e = 0; e < E; ++e) {
+      const long long q = base + (long long)e * MB + threadIdx.x;
 #pragma unroll
-      for (int l = 0; l < LANES; ++l) x[l][e] = q0 + e < n ? a[LANES * (q0 + e) + l] : 0ull;
+      for (int l = 0; l < LANES; ++l) x[l][e] = q < n ? a[LANES * q + l] : 0ull;
+    }
 #pragma unroll
     for (int l = 0; l < LANES; ++l) {
-      unsigned long long sum = 0;
-#pragma unroll
-      for (int e = 0; e < E; ++e) sum += x[l][e];
-      unsigned long long t;
-      unsigned long long run = carry[l] + block_scan<MB>(sum, &t);
+      unsigned long long pre[E];
+      const unsigned long long t = round_prefix<MB, E>(x[l], pre);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        if (q0 + e < n) a[LANES * (q0 + e) + l] = run;
-        run += x[l][e];
+        const long long q = base + (long long)e * MB + threadIdx.x;
+        if (q < n) a[LANES * q + l] = carry[l] + pre[e];
       }
       carry[l] += t;
     }

@@ -19,10 +19,16 @@
 // geometry, so its vertex order may differ from that package's; the sort makes the polygon's
 // winding the same.
 //
-// Two passes over the entries (count, then emit at scanned offsets), so the output is in entry
+// Only a thin band of entries draws anything, and its clip (edge crossings, angle sort, fan) is long
+// and branchy, so the passes separate the streaming from the clipping. A filter pass reads every
+// plane once and writes a bitmap of the entries that may draw (a conservative plane-misses-cell
+// test) with per-block counts; after a scan, a list pass writes those entries in order; a clip
+// pass counts each listed entry's nodes and elements, one entry per thread, and after a second
+// scan the emit pass clips them again and writes at the scanned offsets. The output is in entry
 // order with no atomics.
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <cuda_runtime.h>
 #include "../../include/cutcell_b200.h"
 #include "cc_device.cuh"
@@ -34,9 +40,9 @@ namespace {
 using namespace ccd;
 
 constexpr int MB = 256;
-constexpr int IPT = 32;  // rounds per block: a block's one long clip pass is spread over MB * IPT entries
-constexpr int BLK = MB * IPT;
-constexpr int KEEP = 1024;  // compacted entries a block hands from the count to the emit pass
+constexpr int FR = 32;          // filter rounds per thread
+constexpr int FBLK = MB * FR;   // entries per filter block (256 bitmap words)
+constexpr int LW = 4;           // filter blocks per list block: bitmap words per thread of the list pass
 
 template <class T, int D>
 struct PlicIn {
@@ -210,18 +216,25 @@ __device__ __forceinline__ bool draws_nothing(const PlicIn<T, D>& P, T n0, T n1,
   return !ok || miss;
 }
 
-// A block's entries that may draw something, in entry order, into cand (compact.cuh): G rounds'
-// planes are loaded (the index clamped to the block's last entry) before any is tested.
+// ---- the filter: a bitmap of the entries that may draw something ------------------------------
+// Bit b of word w is set when entry 32 w + b may draw something (draws_nothing is false); bsum gets
+// each block's count. Thread t tests entry q*MB + t of its block in round q, so a warp's ballot is
+// one word; G rounds' planes are loaded (the index clamped to the block's last entry) before any
+// is tested. No clip runs here: the pass streams the planes once.
 template <class T, int D>
-__device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d, int* cand) {
-  constexpr int G = sizeof(T) == 4 ? 8 : 4;
-  const long long start = (long long)blockIdx.x * BLK;
+__global__ void __launch_bounds__(MB) plic_filter_kernel(const PlicIn<T, D> P, T min_d, unsigned* __restrict__ bits,
+                                                         unsigned long long* __restrict__ bsum) {
+  constexpr int G = 2;
+  const long long start = (long long)blockIdx.x * FBLK;
   // this block's entries, addressed by 32-bit offsets
-  const int here = P.count - start < BLK ? int(P.count - start) : BLK;
+  const int here = P.count - start < FBLK ? int(P.count - start) : FBLK;
   const T* nrm = P.normals + D * start;
   const T* icp = P.intercepts + start;
   const uint8_t* val = P.valid ? P.valid + start : nullptr;
-  return cccompact::compact<MB, IPT, G>(cand, [&](int q0) {
+  unsigned* wbits = bits + start / 32;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  unsigned long long cnt = 0;
+  for (int q0 = 0; q0 < FR; q0 += G) {
     T n0[G], n1[G], n2[G], a[G];
     bool ok[G];
 #pragma unroll
@@ -234,102 +247,136 @@ __device__ __forceinline__ int compact_candidates(const PlicIn<T, D>& P, T min_d
       a[u] = icp[rr];
       ok[u] = val ? val[rr] != 0 : true;
     }
-    unsigned m = 0;
 #pragma unroll
     for (int u = 0; u < G; ++u) {
       const int r = (q0 + u) * MB + threadIdx.x;
       const bool okk = val ? ok[u] : (n0[u] != T(0) || n1[u] != T(0) || n2[u] != T(0));
-      if (r < here && !draws_nothing<T, D>(P, n0[u], n1[u], n2[u], a[u], okk, min_d)) m |= 1u << u;
+      const unsigned m = __ballot_sync(0xffffffffu, r < here && !draws_nothing<T, D>(P, n0[u], n1[u], n2[u], a[u], okk, min_d));
+      const int first = (q0 + u) * MB + wp * 32;  // the word's first entry in the block
+      if (lane == 0 && first < here) {
+        wbits[first / 32] = m;
+        cnt += __popc(m);
+      }
     }
-    return m;
-  });
+  }
+  unsigned long long t;
+  cccompact::block_scan<MB>(cnt, &t);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = t;
 }
 
-// Node and element counts travel packed in one 64-bit word (nodes high, elements low; a block's
-// element count stays far below 2^32).
-// The count pass also saves each block's compacted entries (up to KEEP; -1 in kept_n when more),
-// so the emit pass clips them without testing every entry again.
+// Writes the surviving entries of LW consecutive filter blocks, in order, at their places in the
+// list (as far as its capacity reaches). Thread t takes word q*MB + t in round q, so round q is
+// filter block LW * blockIdx.x + q, and boff (the filter blocks' scanned counts) places the first.
+__global__ void __launch_bounds__(MB) plic_list_kernel(const unsigned* __restrict__ bits, long long nwords,
+                                                       const unsigned long long* __restrict__ boff,
+                                                       unsigned long long* __restrict__ list, unsigned long long cap) {
+  static_assert(FBLK / 32 == MB, "one filter block per round");
+  const unsigned long long off = boff[(long long)blockIdx.x * LW];
+  const long long w0 = (long long)blockIdx.x * (MB * LW) + threadIdx.x;
+  unsigned m[LW];
+  unsigned long long cnt[LW], pre[LW];
+#pragma unroll
+  for (int q = 0; q < LW; ++q) {
+    m[q] = w0 + q * MB < nwords ? bits[w0 + q * MB] : 0u;
+    cnt[q] = __popc(m[q]);
+  }
+  cccompact::round_prefix<MB, LW>(cnt, pre);
+#pragma unroll
+  for (int q = 0; q < LW; ++q) {
+    unsigned long long x = off + pre[q];
+    const unsigned long long e0 = 32ull * (unsigned long long)(w0 + q * MB);
+    while (m[q]) {
+      const int b = __ffs(m[q]) - 1;
+      m[q] &= m[q] - 1u;
+      if (x < cap) list[x] = e0 + unsigned(b);
+      ++x;
+    }
+  }
+}
+
+// A listed entry's clip, kept by the clip pass for the emit pass: its polygon, coordinate (v, q) at
+// poly[(3 v + q) * cap + x] (one plane per coordinate, so a warp's stores and loads coalesce), and
+// a packed word: vertex count m | nodes << 3 | elements << 6 | fan keep bits << 9.
+template <class T>
+struct Clips {
+  T* poly;
+  unsigned* info;
+  unsigned long long cap;
+};
+
+// Per block of MB listed entries: the nodes and elements they draw, packed (nodes high, elements
+// low), and each entry's clip kept for the emit. The list holds min(*n_list, cap) entries (the
+// count is read on the device; blocks past it write zeros).
 template <class T, int D>
-__global__ void __launch_bounds__(MB, sizeof(T) == 4 ? 5 : 4) plic_count_kernel(const PlicIn<T, D> P, T min_d, unsigned long long* bsum,
-                                                        int* kept, int* kept_n) {
-  __shared__ int cand[BLK];
-  const int ncand = compact_candidates<T, D>(P, min_d, cand);
-  const long long start = (long long)blockIdx.x * BLK;
-  if (threadIdx.x == 0) kept_n[blockIdx.x] = ncand <= KEEP ? ncand : -1;
-  if (ncand <= KEEP)
-    for (int i = threadIdx.x; i < ncand; i += MB) kept[(size_t)blockIdx.x * KEEP + i] = cand[i];
+__global__ void __launch_bounds__(MB) plic_clip_count_kernel(const PlicIn<T, D> P, T min_d,
+                                                             const unsigned long long* __restrict__ list,
+                                                             const unsigned long long* __restrict__ n_list,
+                                                             const Clips<T> C, unsigned long long* tsum) {
+  const unsigned long long n = *n_list < C.cap ? *n_list : C.cap;
+  const unsigned long long x = (unsigned long long)blockIdx.x * MB + threadIdx.x;
   unsigned long long packed = 0;
-  for (int i = threadIdx.x; i < ncand; i += MB) {
+  if (x < n) {
     T p[6][3];
-    const int m = clip_cell<T, D>(P, start + cand[i], p);
+    const int m = clip_cell<T, D>(P, (long long)list[x], p);
     int a, b;
     unsigned keep;
     cell_counts<T, D>(P, m, p, min_d, a, b, keep);
-    packed += ((unsigned long long)a << 32) | (unsigned long long)b;
+    packed = ((unsigned long long)a << 32) | (unsigned long long)b;
+    C.info[x] = unsigned(m) | unsigned(a) << 3 | unsigned(b) << 6 | keep << 9;
+    for (int v = 0; v < a; ++v)
+#pragma unroll
+      for (int q = 0; q < D; ++q) C.poly[(size_t)(3 * v + q) * C.cap + x] = p[v][q];
   }
   unsigned long long t;
   cccompact::block_scan<MB>(packed, &t);
-  if (threadIdx.x == 0) { bsum[2 * blockIdx.x] = t >> 32; bsum[2 * blockIdx.x + 1] = t & 0xffffffffull; }
+  if (threadIdx.x == 0) {
+    tsum[2 * blockIdx.x] = t >> 32;
+    tsum[2 * blockIdx.x + 1] = t & 0xffffffffull;
+  }
 }
 
-// The writes are checked against the output capacities: offsets from a count of other planes (a
+// One listed entry per thread: its kept clip written at the scanned offsets of its block. The
+// writes are checked against the output capacities: offsets from a count of other planes (a
 // caller that changed them between its two calls) raise *overflow instead of writing past the end.
 template <class T, int D>
-__global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, T min_d, const unsigned long long* boff,
-                                                       T* nodes, unsigned long long ncap, int32_t* elems,
-                                                       unsigned long long ecap, int64_t* cells,
-                                                       unsigned long long* overflow, const int* kept,
-                                                       const int* kept_n) {
-  __shared__ int cand[BLK];
-  int ncand = kept_n[blockIdx.x];  // block-uniform
-  if (ncand == 0) return;
-  if (ncand > 0) {
-    for (int i = threadIdx.x; i < ncand; i += MB) cand[i] = kept[(size_t)blockIdx.x * KEEP + i];
-    __syncthreads();
-  } else {
-    ncand = compact_candidates<T, D>(P, min_d, cand);
+__global__ void __launch_bounds__(MB) plic_emit_kernel(const PlicIn<T, D> P, const unsigned long long* __restrict__ list,
+                                                       unsigned long long n, const Clips<T> C,
+                                                       const unsigned long long* __restrict__ boff, T* nodes,
+                                                       unsigned long long ncap, int32_t* elems, unsigned long long ecap,
+                                                       int64_t* cells, unsigned long long* overflow) {
+  const unsigned long long x = (unsigned long long)blockIdx.x * MB + threadIdx.x;
+  const unsigned long long node0 = boff[2 * blockIdx.x], elem0 = boff[2 * blockIdx.x + 1];
+  const unsigned info = x < n ? C.info[x] : 0u;
+  const int m = int(info & 7u), a = int(info >> 3 & 7u), b = int(info >> 6 & 7u);
+  const unsigned keep = info >> 9;
+  unsigned long long t;
+  const unsigned long long pre = cccompact::block_scan<MB>(((unsigned long long)a << 32) | (unsigned long long)b, &t);
+  const unsigned long long vn = node0 + (pre >> 32);
+  unsigned long long ve = elem0 + (pre & 0xffffffffull);
+  if (a == 0) return;
+  if (vn + a > ncap || ve + b > ecap) {
+    atomicOr(overflow, 1ull);
+    return;
   }
-  const long long start = (long long)blockIdx.x * BLK;
-  unsigned long long run_n = boff[2 * blockIdx.x], run_e = boff[2 * blockIdx.x + 1];
-  for (int c0 = 0; c0 < ncand; c0 += MB) {  // block-uniform
-    const int i = c0 + threadIdx.x;
-    const long long k = i < ncand ? start + cand[i] : 0;
-    T p[6][3];
-    int m = 0, a = 0, b = 0;
-    unsigned keep = 0;
-    if (i < ncand) {
-      m = clip_cell<T, D>(P, k, p);
-      cell_counts<T, D>(P, m, p, min_d, a, b, keep);
-    }
-    unsigned long long t;
-    const unsigned long long pre = cccompact::block_scan<MB>(((unsigned long long)a << 32) | (unsigned long long)b, &t);
-    unsigned long long vn = run_n + (pre >> 32), ve = run_e + (pre & 0xffffffffull);
-    run_n += t >> 32;
-    run_e += t & 0xffffffffull;
-    if (a == 0) continue;
-    if (vn + a > ncap || ve + b > ecap) {
-      atomicOr(overflow, 1ull);
-      continue;
-    }
-    const long long ci = P.index ? (long long)P.index[k] : k;
-    for (int v = 0; v < a; ++v)
+  const long long k = (long long)list[x];
+  const long long ci = P.index ? (long long)P.index[k] : k;
+  for (int v = 0; v < a; ++v)
 #pragma unroll
-      for (int x = 0; x < D; ++x) nodes[D * (vn + v) + x] = p[v][x];
-    if (D == 2) {
-      if (b) {
-        elems[2 * ve] = int32_t(vn);
-        elems[2 * ve + 1] = int32_t(vn + 1);
-        cells[ve] = ci;
-      }
-    } else {
-      for (int v = 1; v < m - 1; ++v) {
-        if (!(keep >> v & 1u)) continue;
-        elems[3 * ve] = int32_t(vn);
-        elems[3 * ve + 1] = int32_t(vn + v);
-        elems[3 * ve + 2] = int32_t(vn + v + 1);
-        cells[ve] = ci;
-        ++ve;
-      }
+    for (int q = 0; q < D; ++q) nodes[D * (vn + v) + q] = C.poly[(size_t)(3 * v + q) * C.cap + x];
+  if (D == 2) {
+    if (b) {
+      elems[2 * ve] = int32_t(vn);
+      elems[2 * ve + 1] = int32_t(vn + 1);
+      cells[ve] = ci;
+    }
+  } else {
+    for (int v = 1; v < m - 1; ++v) {
+      if (!(keep >> v & 1u)) continue;
+      elems[3 * ve] = int32_t(vn);
+      elems[3 * ve + 1] = int32_t(vn + v);
+      elems[3 * ve + 2] = int32_t(vn + v + 1);
+      cells[ve] = ci;
+      ++ve;
     }
   }
 }
@@ -344,10 +391,14 @@ cc_status cuda_fail(cudaError_t e, const char* where) {
 }
 
 // A surface count kept on a handle between the count call and the emit call of generate_mesh:
-// the scanned block offsets and totals, and what they were counted from.
+// the bitmap, block counts and totals, the list of surviving entries with its per-block clip counts
+// (scanned), and what they were counted from. The list keeps its capacity across calls.
 struct Stored {
-  unsigned long long* bsum = nullptr;  // offsets, totals, overflow flag, the kept entries
-  size_t cap = 0;                      // entries of bsum
+  unsigned long long* bsum = nullptr;  // filter block counts, totals, overflow flag; then the bitmap
+  size_t cap = 0;                      // 64-bit words of bsum
+  // surviving entries; per list block (nodes, elements); the clips (18 coordinates, 1 info word each)
+  unsigned long long* list = nullptr;
+  unsigned long long list_cap = 0;     // entries the list holds
   bool valid = false;
   uint64_t generation = 0;
   const void *normals = nullptr, *intercepts = nullptr, *is_valid = nullptr;
@@ -355,6 +406,7 @@ struct Stored {
   double min_frac = 0.0;
   int prec = -1;
   unsigned long long tot[2] = {0, 0};
+  unsigned long long listed = 0;  // surviving entries of the kept count
   bool same(const cc_handle* h, const cc_grid* gg, const void* n, const void* i, const void* v, double f) const {
     if (!valid || generation != h->generation || normals != n || intercepts != i || is_valid != v ||
         prec != h->prec || min_frac != f || g.dim != gg->dim)
@@ -362,6 +414,13 @@ struct Stored {
     for (int a = 0; a < gg->dim; ++a)
       if (g.n[a] != gg->n[a] || g.x0[a] != gg->x0[a] || g.d[a] != gg->d[a]) return false;
     return true;
+  }
+  void release() {
+    if (bsum) cudaFree(bsum);
+    if (list) cudaFree(list);
+    bsum = list = nullptr;
+    cap = 0;
+    list_cap = 0;
   }
 };
 
@@ -389,48 +448,94 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
     if (n_elems) *n_elems = 0;
     return CC_OK;
   }
-  const long long nb = (nc + BLK - 1) / BLK;
-  // bsum: 2*nb block offsets, 2 totals, 1 overflow flag; then kept_n[nb] and kept[nb * KEEP]
-  const size_t words = 2 * size_t(nb) + 3;
-  const size_t need = words + (size_t(nb) * (KEEP + 1) + 1) / 2;
+  const long long nb = (nc + FBLK - 1) / FBLK, nwords = (nc + 31) / 32;
+  const long long nlb = (nb + LW - 1) / LW;  // list blocks
+  // bsum: nb filter block counts, their total, 2 clip totals (nodes, elements), the overflow flag;
+  // then the bitmap (FBLK / 32 32-bit words per block, LW blocks per list block)
+  const size_t head = size_t(nb) + 4;
+  const size_t need = head + size_t(nlb * LW) * (FBLK / 64);
   const bool emit = nodes || elems;
-  // With a handle the buffer is kept, and an emit call right after a count of the same planes
-  // (same update, arrays, grid and fraction) starts from that count's offsets.
+  // With a handle the buffers are kept, and an emit call right after a count of the same planes
+  // (same update, arrays, grid and fraction) starts from that count's list and offsets.
   Stored local;
   Stored* st = &local;
   if (h) {
     if (!h->plic_mesh) h->plic_mesh = new Stored();
     st = static_cast<Stored*>(h->plic_mesh);
   }
+  auto release = [&]() {
+    if (!h) local.release();
+  };
   cudaError_t e = cudaSuccess;
   if (st->cap < need) {
     if (st->bsum) cudaFree(st->bsum);
     st->bsum = nullptr;
     st->cap = 0;
     st->valid = false;
-    if ((e = cudaMalloc(&st->bsum, need * sizeof(unsigned long long))) != cudaSuccess)
+    if ((e = cudaMalloc(&st->bsum, need * sizeof(unsigned long long))) != cudaSuccess) {
+      release();
       return cuda_fail(e, "generate_mesh scratch");
+    }
     st->cap = need;
   }
   const bool reuse = h && emit && st->same(h, g, normals, intercepts, valid, min_frac);
   unsigned long long* bsum = st->bsum;
-  int* kept_n = reinterpret_cast<int*>(bsum + words);
-  int* kept = kept_n + nb;
-  auto release = [&]() {
-    if (!h && local.bsum) cudaFree(local.bsum);
+  unsigned long long* tot1 = bsum + nb;   // surviving entries
+  unsigned long long* tot2 = tot1 + 1;    // nodes, elements
+  unsigned long long* overflow = tot2 + 2;
+  unsigned* bits = reinterpret_cast<unsigned*>(bsum + head);
+  // the list: cap entries, 2 * ntb per-block counts, then the clips
+  auto ntb_of = [](unsigned long long cap) { return (cap + MB - 1) / MB; };
+  auto list_words = [&](unsigned long long cap) {
+    return size_t(cap + 2 * ntb_of(cap)) + (size_t(cap) * (18 * sizeof(T) + sizeof(unsigned)) + 7) / 8;
+  };
+  auto clips = [&]() {
+    Clips<T> c;
+    c.cap = st->list_cap;
+    c.poly = reinterpret_cast<T*>(st->list + c.cap + 2 * ntb_of(c.cap));
+    c.info = reinterpret_cast<unsigned*>(c.poly + 18 * c.cap);
+    return c;
   };
   unsigned long long tot[2] = {st->tot[0], st->tot[1]};
+  unsigned long long listed = st->listed;
   if (!reuse) {
     st->valid = false;
-    plic_count_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, kept, kept_n);
-    cccompact::scan_series_kernel<MB, 2><<<1, MB, 0, s>>>(bsum, nb, bsum + 2 * nb);
-    if ((e = cudaGetLastError()) == cudaSuccess)
-      e = cudaMemcpyAsync(tot, bsum + 2 * nb, sizeof tot, cudaMemcpyDeviceToHost, s);
+    plic_filter_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bits, bsum);
+    cccompact::scan_series_kernel<512, 1, 16><<<1, 512, 0, s>>>(bsum, nb, tot1);
+    // the list and its clip counts, into the list as it is; run again below when the surface has
+    // outgrown it (the first call on a handle, or a larger surface)
+    auto list_pass = [&]() {
+      const unsigned long long ntb = ntb_of(st->list_cap);
+      unsigned long long* tsum = st->list + st->list_cap;
+      plic_list_kernel<<<unsigned(nlb), MB, 0, s>>>(bits, nwords, bsum, st->list, st->list_cap);
+      plic_clip_count_kernel<T, D><<<unsigned(ntb), MB, 0, s>>>(P, min_d, st->list, tot1, clips(), tsum);
+      cccompact::scan_series_kernel<512, 2><<<1, 512, 0, s>>>(tsum, (long long)ntb, tot2);
+    };
+    unsigned long long c3[3];  // surviving entries, nodes, elements
+    if (st->list) list_pass();
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpyAsync(c3, tot1, sizeof c3, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && (!st->list || c3[0] > st->list_cap)) {
+      // grow with an eighth to spare, so that a slightly larger surface next time fits
+      const unsigned long long lc = c3[0] + c3[0] / 8 + 1024;
+      if (st->list) cudaFree(st->list);
+      st->list = nullptr;
+      st->list_cap = 0;
+      if ((e = cudaMalloc(&st->list, list_words(lc) * sizeof(unsigned long long))) == cudaSuccess) {
+        st->list_cap = lc;
+        list_pass();
+        if ((e = cudaGetLastError()) == cudaSuccess)
+          e = cudaMemcpyAsync(c3 + 1, tot2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      }
+    }
     if (e != cudaSuccess) {
       release();
       return cuda_fail(e, "generate_mesh count");
     }
+    listed = c3[0];
+    tot[0] = c3[1];
+    tot[1] = c3[2];
     if (h) {
       st->valid = true;
       st->generation = h->generation;
@@ -442,6 +547,7 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
       st->prec = h->prec;
       st->tot[0] = tot[0];
       st->tot[1] = tot[1];
+      st->listed = listed;
     }
   }
   if (n_nodes) *n_nodes = (int64_t)tot[0];
@@ -455,21 +561,21 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
       release();
       return fail(CC_BAD_ARG, "generate_mesh output smaller than the counted surface");
     }
-    unsigned long long overflow = 0;
+    unsigned long long flag = 0;
     if (tot[1] > 0) {
-      e = cudaMemsetAsync(bsum + 2 * nb + 2, 0, sizeof(unsigned long long), s);
+      const unsigned long long* tsum = st->list + st->list_cap;
+      e = cudaMemsetAsync(overflow, 0, sizeof(unsigned long long), s);
       if (e == cudaSuccess) {
-        plic_emit_kernel<T, D><<<unsigned(nb), MB, 0, s>>>(P, min_d, bsum, static_cast<T*>(nodes),
-                                                           (unsigned long long)ncap, elems, (unsigned long long)ecap,
-                                                           cells, bsum + 2 * nb + 2, kept, kept_n);
+        plic_emit_kernel<T, D><<<unsigned((listed + MB - 1) / MB), MB, 0, s>>>(
+            P, st->list, listed, clips(), tsum, static_cast<T*>(nodes), (unsigned long long)ncap, elems,
+            (unsigned long long)ecap, cells, overflow);
         e = cudaGetLastError();
       }
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&overflow, bsum + 2 * nb + 2, sizeof overflow, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, overflow, sizeof flag, cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     }
     if (h) st->valid = false;  // one emit per count
-    if (e == cudaSuccess && overflow) {
+    if (e == cudaSuccess && flag) {
       release();
       return fail(CC_BAD_ARG, "generate_mesh: the planes changed between the count and the emit call");
     }
@@ -498,7 +604,7 @@ namespace cci {
 void free_plic_mesh(cc_handle* h) {
   if (!h || !h->plic_mesh) return;
   Stored* st = static_cast<Stored*>(h->plic_mesh);
-  if (st->bsum) cudaFree(st->bsum);
+  st->release();
   delete st;
   h->plic_mesh = nullptr;
 }

@@ -329,10 +329,11 @@ cc_status cc_plic_surface(int prec, const cc_grid* g, const void* normals, const
 
 /* generate_mesh for a PLIC cache (src/plic/surface.jl:28-37): cc_plic_surface over every cell of the
  * cache's grid, from the cache's own normals / intercepts / is_valid (the grid is checked against
- * the cache's size). The handle keeps the counting call's block offsets: an emitting call that
- * follows it with the same arrays, grid and fraction, and no update in between, skips the second
- * count. The planes must not be written between the two calls; an emit that would then run past
- * the counted capacities writes nothing beyond them and returns CC_BAD_ARG. */
+ * the cache's size). The handle keeps what the counting call found -- the entries that draw, their
+ * clipped polygons and the scanned offsets: an emitting call that follows it with the same arrays,
+ * grid and fraction, and no update in between, writes that counted surface without clipping
+ * again. It is the surface of the planes as they were at the count, so planes written in place
+ * between the two calls do not reach the output. */
 cc_status cc_plic_mesh(cc_handle* h, const cc_grid* g, const void* normals, const void* intercepts,
                        const uint8_t* is_valid, double min_tri_area_fraction, void* nodes, int64_t node_capacity,
                        int32_t* elements, int64_t element_capacity, int64_t* element_cells, int64_t* n_nodes,

@@ -171,9 +171,10 @@ def test_large_grid_properties():
 
 
 def test_count_then_emit_reuse_and_changed_planes():
-    """The handle keeps the count for the emit call that follows it; planes written between the
-    two calls make the emit fail cleanly (its writes are checked against the counted capacities)
-    rather than run past the arrays, and the next generate_mesh counts afresh."""
+    """The handle keeps the count for the emit call that follows it -- the clipped polygons and
+    their offsets -- so the emit writes the surface as counted: planes written in place between
+    the two calls do not reach it (and cannot make it run past the counted arrays), and the next
+    generate_mesh counts the new planes afresh."""
     import ctypes as C
     L = __import__("cutcell_b200._lib", fromlist=["_lib"])
     cache_mod = __import__("cutcell_b200.cache", fromlist=["cache"])
@@ -200,7 +201,10 @@ def test_count_then_emit_reuse_and_changed_planes():
     c.is_valid.fill_(1)
     rc = lib.cc_plic_mesh(*head, nodes.data_ptr(), nn.value, elems.data_ptr(), ne.value, cells.data_ptr(),
                           C.byref(nn), C.byref(ne), s)
-    assert rc == L.CC_BAD_ARG
+    assert rc == L.CC_OK
+    assert torch.equal(nodes.to(first.nodes.dtype), first.nodes) and torch.equal(elems, first.elements.to(elems.dtype))
+    changed = S.generate_mesh(c, g)                     # a fresh count sees the new planes
+    assert changed.elements.shape[0] > first.elements.shape[0]
     c.normals.copy_(saved_n)
     c.intercepts.copy_(saved_i)
     c.is_valid.copy_(saved_v)
