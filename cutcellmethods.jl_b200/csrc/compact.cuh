@@ -110,38 +110,30 @@ __device__ __forceinline__ unsigned long long round_prefix(const unsigned long l
   return total;
 }
 
-// In-place exclusive scan of `n` per-block counts (LANES interleaved series) in one CTA of MB
-// threads, E * MB entries per pass taken round-major (entry base + e*MB + t in round e, so the
-// loads coalesce and are all issued before the scans) and placed by round_prefix; totals[l]
-// receives series l's sum.
+// In-place exclusive scan of `n` per-block counts (LANES interleaved series), one CTA of MB threads
+// per series (launch LANES CTAs; series l = blockIdx.x), E * MB entries per pass taken round-major
+// (entry base + e*MB + t in round e, so the loads coalesce and are all issued before the scan) and
+// placed by round_prefix; totals[l] receives series l's sum.
 template <int MB, int LANES, int E = 8>
 __global__ void __launch_bounds__(MB) scan_series_kernel(unsigned long long* a, long long n, unsigned long long* totals) {
-  unsigned long long carry[LANES];  // the same in every thread
-#pragma unroll
-  for (int l = 0; l < LANES; ++l) carry[l] = 0;
+  const int l = blockIdx.x;
+  unsigned long long carry = 0;  // the same in every thread
   for (long long base = 0; base < n; base += (long long)MB * E) {
-    unsigned long long x[LANES][E];
+    unsigned long long x[E], pre[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const long long q = base + (long long)e * MB + threadIdx.x;
-#pragma unroll
-      for (int l = 0; l < LANES; ++l) x[l][e] = q < n ? a[LANES * q + l] : 0ull;
+      x[e] = q < n ? a[LANES * q + l] : 0ull;
     }
+    const unsigned long long t = round_prefix<MB, E>(x, pre);
 #pragma unroll
-    for (int l = 0; l < LANES; ++l) {
-      unsigned long long pre[E];
-      const unsigned long long t = round_prefix<MB, E>(x[l], pre);
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const long long q = base + (long long)e * MB + threadIdx.x;
-        if (q < n) a[LANES * q + l] = carry[l] + pre[e];
-      }
-      carry[l] += t;
+    for (int e = 0; e < E; ++e) {
+      const long long q = base + (long long)e * MB + threadIdx.x;
+      if (q < n) a[LANES * q + l] = carry + pre[e];
     }
+    carry += t;
   }
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int l = 0; l < LANES; ++l) totals[l] = carry[l];
+  if (threadIdx.x == 0) totals[l] = carry;
 }
 
 }  // namespace cccompact

@@ -221,10 +221,14 @@ __global__ void __launch_bounds__(MB) band_count_kernel(const Signs sg, unsigned
 // survivor per thread.
 __global__ void __launch_bounds__(MB) band_list_kernel(const Signs sg, unsigned nx,
                                                        const unsigned long long* __restrict__ boff,
+                                                       const unsigned long long* __restrict__ tot,
                                                        uint4* __restrict__ nodes, unsigned long long node_cap,
                                                        unsigned* __restrict__ cells, unsigned long long cell_cap) {
   const unsigned u0 = blockIdx.x * unsigned(BW);
   const unsigned long long nb = boff[3 * blockIdx.x], vb = boff[3 * blockIdx.x + 1], cb = boff[3 * blockIdx.x + 2];
+  // the block's own counts, from the next block's offsets (the totals after the last block)
+  const unsigned long long* next = blockIdx.x + 1 < gridDim.x ? boff + 3 * (blockIdx.x + 1) : tot;
+  if (next[0] == nb && next[2] == cb) return;  // block-uniform: no cut node, no cut cell
   unsigned ax[IPT], ay[IPT], az[IPT], cm[IPT];
   unsigned long long cnt[IPT], pre[IPT];  // cut nodes | edge vertices << 21 | cut cells << 42
 #pragma unroll
@@ -495,17 +499,17 @@ cc_status run_mesh(cc_handle* h, const cc_grid* gg, const T* phi, T* verts, int6
     const long long rows = ny * (g.n[2] + 1);
     sign_kernel<T><<<unsigned((rows + 7) / 8), 256, 0, s>>>(phi, sg, unsigned(nx), unsigned(rows));
     band_count_kernel<<<unsigned(nb), MB, 0, s>>>(sg, bsum);
-    cccompact::scan_series_kernel<512, 3><<<1, 512, 0, s>>>(bsum, nb, tot);
+    cccompact::scan_series_kernel<512, 3><<<3, 512, 0, s>>>(bsum, nb, tot);
     // the list pass and the tile counts, into the lists as they are; run again below when the
     // surface has outgrown them (the first call on a handle, or a larger surface)
     auto list_pass = [&]() {
       auto [nodes, tsum, cells, ntb] = lists();
-      band_list_kernel<<<unsigned(nb), MB, 0, s>>>(sg, unsigned(nx), bsum, nodes, h->mesh_node_cap, cells,
+      band_list_kernel<<<unsigned(nb), MB, 0, s>>>(sg, unsigned(nx), bsum, tot, nodes, h->mesh_node_cap, cells,
                                                    h->mesh_cell_cap);
       if (ntb > 0) {
         tile_count_kernel<T, MX><<<unsigned(ntb), MB, 0, s>>>(phi, g, nd, h->tb, cells, tot + 2, h->mesh_cell_cap,
                                                              tsum);
-        cccompact::scan_series_kernel<512, 2><<<1, 512, 0, s>>>(tsum, (long long)ntb, tot2);
+        cccompact::scan_series_kernel<512, 2><<<2, 512, 0, s>>>(tsum, (long long)ntb, tot2);
       } else {
         cudaMemsetAsync(tot2, 0, 2 * sizeof(unsigned long long), s);
       }

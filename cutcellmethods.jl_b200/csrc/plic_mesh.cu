@@ -268,10 +268,14 @@ __global__ void __launch_bounds__(MB) plic_filter_kernel(const PlicIn<T, D> P, T
 // list (as far as its capacity reaches). Thread t takes word q*MB + t in round q, so round q is
 // filter block LW * blockIdx.x + q, and boff (the filter blocks' scanned counts) places the first.
 __global__ void __launch_bounds__(MB) plic_list_kernel(const unsigned* __restrict__ bits, long long nwords,
-                                                       const unsigned long long* __restrict__ boff,
+                                                       const unsigned long long* __restrict__ boff, long long nb,
+                                                       const unsigned long long* __restrict__ total,
                                                        unsigned long long* __restrict__ list, unsigned long long cap) {
   static_assert(FBLK / 32 == MB, "one filter block per round");
   const unsigned long long off = boff[(long long)blockIdx.x * LW];
+  // the block's own count, from the next list block's offset (the total after the last)
+  const long long nxt = (long long)(blockIdx.x + 1) * LW;
+  if ((nxt < nb ? boff[nxt] : *total) == off) return;  // block-uniform: no surviving entry
   const long long w0 = (long long)blockIdx.x * (MB * LW) + threadIdx.x;
   unsigned m[LW];
   unsigned long long cnt[LW], pre[LW];
@@ -507,9 +511,9 @@ cc_status run(const cc_grid* g, const void* normals, const void* intercepts, con
     auto list_pass = [&]() {
       const unsigned long long ntb = ntb_of(st->list_cap);
       unsigned long long* tsum = st->list + st->list_cap;
-      plic_list_kernel<<<unsigned(nlb), MB, 0, s>>>(bits, nwords, bsum, st->list, st->list_cap);
+      plic_list_kernel<<<unsigned(nlb), MB, 0, s>>>(bits, nwords, bsum, nb, tot1, st->list, st->list_cap);
       plic_clip_count_kernel<T, D><<<unsigned(ntb), MB, 0, s>>>(P, min_d, st->list, tot1, clips(), tsum);
-      cccompact::scan_series_kernel<512, 2><<<1, 512, 0, s>>>(tsum, (long long)ntb, tot2);
+      cccompact::scan_series_kernel<512, 2><<<2, 512, 0, s>>>(tsum, (long long)ntb, tot2);
     };
     unsigned long long c3[3];  // surviving entries, nodes, elements
     if (st->list) list_pass();
