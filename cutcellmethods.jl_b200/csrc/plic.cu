@@ -181,6 +181,22 @@ __device__ __forceinline__ T face_area(const T* n, T a, T frac, bool valid, cons
   }
 }
 
+// Whether a valid 3D plane misses its cell by more than rounding, and on which side: -1 when
+// every face's face_area is 0, +1 when it is the face's full area U V, 0 when it must be computed.
+// Over the unit cube n . xi spans [lo, hi] = [sum min(n_i, 0), sum max(n_i, 0)]. If a - hi exceeds
+// 64 u (|n|_1 + |a|) (u the unit roundoff of T), every face has n_p x + n_q y < a - n_c s with that
+// margin, so gvf2 (whose rounding error is a few u of the same scale, in T or, mixed, in FP64
+// from T's base) reaches its alpha >= s return, 1, and the area is (U V) (1 - 1) = 0; if lo - a
+// exceeds it, gvf2 returns 0 and the area is U V. A NaN or infinite plane fails both tests.
+template <class T>
+__device__ __forceinline__ int plane_side(const T n[3], T a) {
+  const T zero = T(0);
+  const T lo = (fmin(n[0], zero) + fmin(n[1], zero)) + fmin(n[2], zero);
+  const T hi = (fmax(n[0], zero) + fmax(n[1], zero)) + fmax(n[2], zero);
+  const T tol = (sizeof(T) == 4 ? T(0x1p-18) : T(0x1p-47)) * (((fabs(n[0]) + fabs(n[1])) + fabs(n[2])) + fabs(a));
+  return a - hi > tol ? -1 : (lo - a > tol ? 1 : 0);
+}
+
 __host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
 
 // m / full for a face area m of a face of area full > 0, bit for bit: an area of exactly 0 or
@@ -344,6 +360,15 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
     const T nrm[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
     const T a = intercepts[ci], fr = vf[ci];
     const bool ok = valid[ci] != 0;
+    const int side = ok ? plane_side<T>(nrm, a) : 0;
+    if (side != 0) {  // the values face_area gives a plane that misses the cell, without its arithmetic
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const int c = f >> 1;
+        buf[f][q] = side > 0 ? cs[c == 0 ? 1 : 0] * cs[c == 2 ? 1 : 2] : T(0);
+      }
+      return;
+    }
 #pragma unroll
     for (int f = 0; f < NF; ++f) buf[f][q] = face_area<T, 3, MX>(nrm, a, fr, ok, cs, f);
   };
