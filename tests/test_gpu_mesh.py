@@ -56,6 +56,35 @@ def test_mesh_of_a_nodal_field_and_cell_indices():
     assert (ci == own).mean() > 0.99
 
 
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_mesh_bitmap_word_edges(prec):
+    """The sign bitmap pads each node row to 32-node words: rows of exactly 32, 33, 64 and 65 nodes,
+    rows shorter than a word, one-cell and one-layer grids, under dense random fields (cuts in most
+    words, across row and word boundaries) -- bit for bit the oracle's mesh."""
+    rng = XorShift(2024)
+    for n in ((31, 3, 4), (32, 4, 3), (63, 2, 2), (64, 3, 2), (1, 1, 1), (2, 9, 7), (5, 1, 12), (95, 2, 1)):
+        g = cc.CartesianGrid((0.0, 0.0, 0.0), n, (1.0, 1.0, 1.0))
+        vals = np.array([rng.randn() for _ in range((n[0] + 1) * (n[1] + 1) * (n[2] + 1))])
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=DT[prec],
+                                  precision="mixed" if prec == 2 else "plain")
+        cc.update_cache(cache, cc.NodalField(torch.as_tensor(vals)), g)
+        check_against_oracle(cache, g, prec)
+
+
+def test_mesh_list_capacity_carries_over():
+    """The cut-node and cut-cell lists keep their capacity on the handle between calls: a surface
+    that outgrows them (counted again into larger lists), then a smaller one (counted into the
+    kept lists in one pass), each bit for bit the oracle's."""
+    g = cc.grid3(40)
+    cache = cc.allocate_cache(g, cc.MarchingCubesCutCell())
+    rng = XorShift(77)
+    vals = np.array([rng.randn() for _ in range(41 ** 3)])
+    for geo in (cc.Sphere((0.01, 0.02, -0.03), 0.3), cc.NodalField(torch.as_tensor(vals)),
+                cc.Sphere((0.01, 0.02, -0.03), 0.3), cc.Sphere((-0.02, 0.0, 0.05), 1.2)):
+        cc.update_cache(cache, geo, g)
+        check_against_oracle(cache, g, 1)
+
+
 def test_mesh_edge_cases():
     g = cc.grid3(16)
     empty = cache_for(g, cc.Sphere((5.0, 5.0, 5.0), 0.5), 1)

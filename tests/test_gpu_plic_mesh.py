@@ -150,6 +150,23 @@ def test_random_and_degenerate_planes(dim, prec):
     assert empty.elements.shape[0] == 0
 
 
+@pytest.mark.parametrize("prec", [1, 0])
+def test_dense_planes_across_blocks(prec):
+    """Random planes in every cell of a 41 x 37 x 29 grid (43,993 entries): the survivor bitmap,
+    its per-block counts and the ordered list cross several 8192-entry filter blocks and a
+    32768-entry list block with most entries surviving -- bit for bit the oracle's surface."""
+    n = (41, 37, 29)
+    g = cc.CartesianGrid((-0.2, 0.1, -0.4), n, (0.03, 0.04, 0.05))
+    nc = g.ncell
+    rng = XorShift(5151 + 2 * prec)  # the generator forces the seed odd
+    normals, icpt, valid = planes(3, nc, rng, np.float64 if prec == 1 else np.float32)
+    dev = torch.device("cuda", 0)
+    tn, ti, tv = (torch.from_numpy(normals).to(dev), torch.from_numpy(icpt).to(dev), torch.from_numpy(valid).to(dev))
+    ref = po.plic_mesh(g, normals, icpt, valid, 1 if prec == 1 else 0, 1e-4)
+    assert ref[1].shape[0] > nc // 2
+    same(S.extract_surface_plic(tn, ti, torch.arange(nc, device=dev), g, 1e-4, is_valid=tv), ref)
+
+
 def test_large_grid_properties():
     """256^3 Float32 sphere: every node inside its own cell and on its plane; the area is the
     sphere's."""
