@@ -170,6 +170,20 @@ __global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, c
   if (threadIdx.x == 0) count[blockIdx.x] = m;
 }
 
+// An uncut cell whose staging slot held an uncut cell of the same kind at the slot's previous use
+// (two slices earlier, in the same column): kind, flag, fraction, face fractions and the x, y
+// parts are the same values, so only what depends on the slice is written -- the centroid's and
+// interface centroid's z and the face centroids' half-height entries (slots 1, 3, 5, 7, written
+// with their neighbours as two 16-byte vectors). The slot then holds exactly what put_cell leaves.
+// 512^3 CSG body: Float32 update 2.78 -> 2.74 ms.
+__device__ __forceinline__ void put_uncut_z(const Stage<float>& st, int lc, float cz, float hx, float hy, float hz) {
+  st.c[3 * lc + 2] = cz;
+  st.ic[3 * lc + 2] = cz;
+  float4* d4 = reinterpret_cast<float4*>(st.fcl + 12 * lc);
+  d4[0] = make_float4(hy, hz, hy, hz);
+  d4[1] = make_float4(hx, hz, hx, hz);
+}
+
 template <class T, bool SAMPLE, bool PRUNED>
 __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
                                                                             const __grid_constant__ ColumnMaps maps) {
@@ -284,6 +298,9 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
                             reinterpret_cast<unsigned char*>(A.cols.ff), reinterpret_cast<unsigned char*>(A.cols.fcl),
                             reinterpret_cast<unsigned char*>(A.cols.ic)};
 
+  // What this thread's slot of each staging buffer holds: 0 not known (first use, or a cut cell,
+  // whose slot the fill leaves alone), 1 an uncut cell outside, 2 inside (2 bits per buffer).
+  int slots = 0;
   for (long long k = k0; k < k1; ++k) {
     const int sb = (int)((k - k0) & 1);
     unsigned char* sbase = smem + sb * L::stage_bytes;
@@ -304,16 +321,23 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
       int nout = 0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) nout += ph[q] > neps ? 1 : 0;
-      if (nout == 0 || nout == 8) {
+      const int state = nout == 8 ? 2 : (nout == 0 ? 1 : 0);
+      if (state != 0) {
         const T hz = T(0.5) * (zb - za);
         const T one = nout == 8 ? T(1) : T(0);
         const T cen[3] = {cx, cy, za + T(0.5) * dz};
-        const T ff[6] = {one, one, one, one, one, one};
-        const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
-        put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+        // (Float32 only: at Float64 the split cost more than the stores it saved, 4.91 vs 4.76 ms)
+        if (sizeof(T) == 4 && ((slots >> (2 * sb)) & 3) == state) {
+          if constexpr (sizeof(T) == 4) put_uncut_z(stage_at<T>(sbase), lc, cen[2], hx, hy, hz);
+        } else {
+          const T ff[6] = {one, one, one, one, one, one};
+          const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
+          put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+        }
       } else {
         is_cut = true;
       }
+      slots = (slots & ~(3 << (2 * sb))) | (state << (2 * sb));
     }
     // Warp-ballot compaction of the cut band into the global work list. A cut cell's staged slot
     // is left as it is: the span is copied out whole and the cut kernel, which runs after this
