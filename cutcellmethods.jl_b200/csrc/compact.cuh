@@ -1,14 +1,13 @@
-// compact.cuh -- in-order block compaction for the surface extractors (mesh.cu, plic_mesh.cu).
+// compact.cuh -- in-order placement and block-sum scans for the surface extractors (mesh.cu,
+// plic_mesh.cu).
 //
 // A surface pass visits every node or cell, but only a thin band (about one in a hundred at
-// 512^3) contributes anything, and that band's work (a clip, a tile, an edge walk) is long and
-// branchy. Run in place, it would leave 31 lanes of most warps waiting on one. So a block owns
-// BLK = MB * IPT consecutive items, taken round-major (round q covers items q*MB + [0, MB), one
-// per thread, so loads coalesce), tests them all cheaply with no barrier in between (their loads
-// overlap), and places the survivors' local indices in item order -- round, warp, lane -- into
-// shared memory, through warp ballots and one block scan of the per-(round, warp) counts. The
-// long work then runs over the survivors on dense warps, MB at a time, and an in-block scan per
-// chunk keeps the output in item order with no atomics.
+// 512^3) contributes anything. The extractors test every item cheaply into a bitmap (one bit per
+// item, 32 to a word), count the set bits per block, scan the block counts, and write the
+// survivors in item order into flat lists; the long work (a clip, a tile, an edge walk) then runs
+// over the lists one survivor per thread. This header holds the pieces those passes share: a
+// block scan, round_prefix (the place of each word's set bits among a block's, in word order)
+// and the block-sum scan.
 #pragma once
 #include <cstdint>
 
@@ -37,45 +36,9 @@ __device__ __forceinline__ unsigned long long block_scan(unsigned long long x, u
   return base + v - x;
 }
 
-// Places in cand[0 .. n) (n returned, block-uniform) the local indices r = q*MB + threadIdx.x of
-// this block's items that are kept, in increasing order. keep(q0) is called by every thread for
-// q0 = 0, G, 2G, .. in order and returns the kept bits of rounds q0 .. q0+G-1 (bit u for round
-// q0+u), answering 0 past the block's last item. A group is the unit of memory-level parallelism:
-// keep should issue all of its G rounds' loads (from clamped, always valid addresses) before
-// testing any, so a round does not wait on the one before it.
-template <int MB, int IPT, int G, class Keep>
-__device__ __forceinline__ int compact(int* cand, Keep keep) {
-  static_assert(IPT <= 32 && IPT * (MB / 32) == MB, "one bit per round; one (round, warp) slot per thread");
-  static_assert(IPT % G == 0, "whole groups");
-  __shared__ int slot[MB];  // per (round, warp): its count, then its first position
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned bits = 0;
-#pragma unroll 2
-  for (int q0 = 0; q0 < IPT; q0 += G) bits |= keep(q0) << q0;
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q) {
-    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if (lane == 0) slot[q * (MB / 32) + w] = __popc(bal);
-  }
-  __syncthreads();
-  unsigned long long total;
-  const unsigned long long first = block_scan<MB>((unsigned long long)slot[threadIdx.x], &total);
-  slot[threadIdx.x] = (int)first;  // block_scan's closing barrier ordered every read before this
-  __syncthreads();
-  const unsigned below = (1u << lane) - 1u;
-#pragma unroll 8
-  for (int q = 0; q < IPT; ++q) {
-    const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-    if ((bits >> q) & 1u) cand[slot[q * (MB / 32) + w] + __popc(bal & below)] = q * MB + threadIdx.x;
-  }
-  __syncthreads();
-  return (int)total;
-}
-
-// ---- word-parallel survivors -----------------------------------------------------------------
-// When the cheap test is a bit per item packed 32 to a word (a sign bitmap), a block owns MB * IPT
-// consecutive words, thread t taking word q*MB + t in round q, so block order is word order, and
-// round_prefix places each word's set bits among the block's.
+// ---- placing a block's set bits ----------------------------------------------------------------
+// A block owns MB * IPT consecutive bitmap words, thread t taking word q*MB + t in round q, so
+// block order is word order, and round_prefix places each word's set bits among the block's.
 
 // Exclusive prefix, in block order (round, then thread), of one count per thread and round;
 // pre[q] receives this thread's and the block total is returned. The counts are 64-bit so that

@@ -17,15 +17,17 @@
 // The surface lives in a thin band (about one node in a hundred at 512^3), so the passes first
 // find it cheaply. A sign pass reads phi once and writes one bit per node (outside or not); every
 // later test is word arithmetic on that bitmap, 32 nodes at a time: an edge crosses where its two
-// nodes' bits differ, a cell is cut where its corners' bits are not all equal. The count pass
-// sums the cut edges by popcount and runs the tile of each cut cell (triangles, interior vertex);
-// the per-block counts are scanned; the two emit passes (edge vertices, then cells) recompute the
-// block's cut bits, place them in order and hand them out to dense warps (compact.cuh), so the
-// long work -- edge crossings, tiles -- runs only on the band. The count call keeps the bitmap and
-// the scanned offsets on the handle, and an emit call that follows it for the same phi and grid,
-// with no update in between, starts from them. The edge pass keeps each surviving node's first
-// vertex, so a cell's triangles can name the vertices of edges other nodes own. Every write of an
-// emit is checked against the output capacities.
+// nodes' bits differ, a cell is cut where its corners' bits are not all equal. A band count pass
+// sums, per block of words, the cut nodes, their edge vertices (popcounts) and the cut cells; the
+// block counts are scanned; a band list pass writes the cut nodes (with their first vertex and
+// edge bits) and the cut cells in order into two flat lists. The long work -- each cut cell's
+// tile for the triangle counts, the edge crossings, the triangles -- then runs over the lists one
+// survivor per thread, so a block that a grid-aligned face fills with cut cells is no tail. The
+// count call keeps the bitmap, the lists (whose capacity carries over between calls) and the
+// scanned offsets on the handle, and an emit call that follows it for the same phi and grid, with
+// no update in between, starts from them. The node emit stores each cut node's first vertex, so
+// a cell's triangles can name the vertices of edges other nodes own. Every write of an emit is
+// checked against the output capacities.
 #include <cstdint>
 #include <string>
 #include <tuple>
