@@ -318,11 +318,13 @@ __global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, co
 }
 
 // The resolved faces in 3D, marching z: a CTA owns a column of FZ_X x FZ_Y cells and FZ_KZ slices.
-// Per slice it computes the next slice's one-sided areas (whose -z face is this slice's +z
-// neighbour), this slice's x and y halo, then resolves the slice and writes its rows; this
-// slice's +z areas are kept as the next slice's -z neighbours. So every plane is read once (the
-// column's first slice also reads the plane below it), with no z-halo, in two barriers per slice.
-// The areas and the resolve expression are plic_face_kernel's, so the faces are the same bits.
+// Per slice it computes the next slice's one-sided fractions (area / full face, frac_of; whose
+// -z face is this slice's +z neighbour), this slice's x and y halo, then resolves the slice and
+// writes its rows; this slice's +z fractions are kept as the next slice's -z neighbours. So every
+// plane is read once (the column's first slice also reads the plane below it), with no z-halo,
+// in two barriers per slice, and each one-sided fraction is formed once rather than by both
+// cells of its face. The areas, fractions and resolve expression are plic_face_kernel's, so the
+// faces are the same bits.
 constexpr int FZ_X = 32, FZ_Y = 8, FZ_KZ = 32;
 
 template <class T, bool MX>
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
   constexpr int X = FZ_X, Y = FZ_Y, NF = 6;
   static_assert(X * Y == NT, "one cell of the slice per thread");
   __shared__ T bufA[NF][NT], bufB[NF][NT];
-  __shared__ T prev5[NT];                   // the slice below's +z areas
+  __shared__ T prev5[NT];                   // the slice below's +z fractions
   __shared__ T hx[2][Y], hy[2][X];          // this slice's x and y halo
   __shared__ __align__(16) T res[NT * NF];  // resolved fractions, cell-major as in the column
   const long long n[3] = {g.n[0], g.n[1], g.n[2]};
@@ -351,42 +353,44 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
   const int q = threadIdx.x, lx = q % X, ly = q / X;
   const long long ix = i0 + lx, jy = j0 + ly;
   const bool inxy = ix < n[0] && jy < n[1];
-  auto area_of = [&](long long ci, int f) {
-    return face_area<T, 3, MX>(normals + 3 * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, f);
+  // the full area of a face of direction f, and the fraction m / full of an area m (frac_of)
+  auto full_of = [&](int f) {
+    const int c = f >> 1;
+    return (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
   };
-  auto own6 = [&](T (*buf)[NT], long long k) {  // this thread's cell of slice k, all six faces
+  auto frac_at = [&](long long ci, int f) {  // the one-sided fraction of cell ci's face f
+    return frac_of(face_area<T, 3, MX>(normals + 3 * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, f), full_of(f));
+  };
+  auto own6 = [&](T (*buf)[NT], long long k) {  // this thread's cell of slice k: six one-sided fractions
     if (!inxy) return;
     const long long ci = ix + n[0] * (jy + n[1] * k);
     const T nrm[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
     const T a = intercepts[ci], fr = vf[ci];
     const bool ok = valid[ci] != 0;
     const int side = ok ? plane_side<T>(nrm, a) : 0;
-    if (side != 0) {  // the values face_area gives a plane that misses the cell, without its arithmetic
+    if (side != 0) {  // a plane that misses the cell: every area 0 or the full face, so 0 or 1
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        const int c = f >> 1;
-        buf[f][q] = side > 0 ? cs[c == 0 ? 1 : 0] * cs[c == 2 ? 1 : 2] : T(0);
-      }
+      for (int f = 0; f < NF; ++f) buf[f][q] = side > 0 ? T(1) : T(0);
       return;
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f) buf[f][q] = face_area<T, 3, MX>(nrm, a, fr, ok, cs, f);
+    for (int f = 0; f < NF; ++f) buf[f][q] = frac_of(face_area<T, 3, MX>(nrm, a, fr, ok, cs, f), full_of(f));
   };
   T (*cur)[NT] = bufA;
   T (*nxt)[NT] = bufB;
   own6(cur, k0);
-  if (inxy && k0 >= 1) prev5[q] = area_of(ix + n[0] * (jy + n[1] * (k0 - 1)), 5);
+  if (inxy && k0 >= 1) prev5[q] = frac_at(ix + n[0] * (jy + n[1] * (k0 - 1)), 5);
   for (long long k = k0; k < k1; ++k) {
     if (k + 1 < n[2]) own6(nxt, k + 1);
     for (int h = q; h < 2 * Y + 2 * X; h += NT) {
       if (h < 2 * Y) {
         const int side = h / Y, y = h % Y;
         const long long ii = side == 0 ? i0 - 1 : i0 + X, jj = j0 + y;
-        if (ii >= 0 && ii < n[0] && jj < n[1]) hx[side][y] = area_of(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
+        if (ii >= 0 && ii < n[0] && jj < n[1]) hx[side][y] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
       } else {
         const int side = (h - 2 * Y) / X, x = (h - 2 * Y) % X;
         const long long ii = i0 + x, jj = side == 0 ? j0 - 1 : j0 + Y;
-        if (jj >= 0 && jj < n[1] && ii < n[0]) hy[side][x] = area_of(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
+        if (jj >= 0 && jj < n[1] && ii < n[0]) hy[side][x] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
       }
     }
     __syncthreads();
@@ -395,8 +399,6 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
         const int c = f >> 1;
-        const int o1 = c == 0 ? 1 : 0, o2 = c == 2 ? 1 : 2;
-        const T full = (T(1) * cs[o1]) * cs[o2];
         const T mine = cur[f][q];
         T r;
         if ((f & 1) == 0) {
@@ -404,13 +406,13 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
           T below = T(0);
           if (has) below = c == 0 ? (lx > 0 ? cur[1][q - 1] : hx[0][ly])
                                   : c == 1 ? (ly > 0 ? cur[3][q - X] : hy[0][lx]) : prev5[q];
-          r = has ? (frac_of(below, full) + frac_of(mine, full)) * T(0.5) : frac_of(mine, full);
+          r = has ? (below + mine) * T(0.5) : mine;
         } else {
           const bool has = idx[c] <= n[c] - 2;
           T above = T(0);
           if (has) above = c == 0 ? (lx < X - 1 ? cur[0][q + 1] : hx[1][ly])
                                   : c == 1 ? (ly < Y - 1 ? cur[2][q + X] : hy[1][lx]) : nxt[4][q];
-          r = has ? (frac_of(mine, full) + frac_of(above, full)) * T(0.5) : frac_of(mine, full);
+          r = has ? (mine + above) * T(0.5) : mine;
         }
         res[q * NF + f] = r;
       }
