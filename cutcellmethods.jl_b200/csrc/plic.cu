@@ -334,10 +334,11 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
                                                             const uint8_t* __restrict__ valid) {
   constexpr int X = FZ_X, Y = FZ_Y, NF = 6;
   static_assert(X * Y == NT, "one cell of the slice per thread");
-  __shared__ T bufA[NF][NT], bufB[NF][NT];
-  __shared__ T prev5[NT];                   // the slice below's +z fractions
-  __shared__ T hx[2][Y], hy[2][X];          // this slice's x and y halo
-  __shared__ __align__(16) T res[NT * NF];  // resolved fractions, cell-major as in the column
+  // One-sided fractions of the slices k % 3, warp-blocked: row w (one warp) keeps its six faces
+  // over its 32 lanes, [w][f][lane], so a warp's own writes stay in its own block.
+  __shared__ __align__(16) T bufs[3][Y][NF][X];
+  __shared__ T prev5[NT];                    // the slice below's +z fractions (own slot only)
+  __shared__ T hx[2][2][Y], hy[2][2][X];     // the x and y halo of slices of each parity
   const long long n[3] = {g.n[0], g.n[1], g.n[2]};
   const T* vf = static_cast<const T*>(cols.vf);
   T* ff = static_cast<T*>(cols.ff);
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
   auto frac_at = [&](long long ci, int f) {  // the one-sided fraction of cell ci's face f
     return frac_of(face_area<T, 3, MX>(normals + 3 * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, f), full_of(f));
   };
-  auto own6 = [&](T (*buf)[NT], long long k) {  // this thread's cell of slice k: six one-sided fractions
+  auto own6 = [&](T (*buf)[NF][X], long long k) {  // this thread's cell of slice k: six one-sided fractions
     if (!inxy) return;
     const long long ci = ix + n[0] * (jy + n[1] * k);
     const T nrm[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
@@ -370,27 +371,40 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
     const int side = ok ? plane_side<T>(nrm, a) : 0;
     if (side != 0) {  // a plane that misses the cell: every area 0 or the full face, so 0 or 1
 #pragma unroll
-      for (int f = 0; f < NF; ++f) buf[f][q] = side > 0 ? T(1) : T(0);
+      for (int f = 0; f < NF; ++f) buf[ly][f][lx] = side > 0 ? T(1) : T(0);
       return;
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f) buf[f][q] = frac_of(face_area<T, 3, MX>(nrm, a, fr, ok, cs, f), full_of(f));
+    for (int f = 0; f < NF; ++f) buf[ly][f][lx] = frac_of(face_area<T, 3, MX>(nrm, a, fr, ok, cs, f), full_of(f));
   };
-  T (*cur)[NT] = bufA;
-  T (*nxt)[NT] = bufB;
-  own6(cur, k0);
+  // One barrier per slice. Slice k's fractions live in bufs[(k - k0) % 3]: the next slice's are
+  // written (own slots) while this one's are read, and the buffer they overwrite was last read in
+  // slice k - 2, whose readers all passed the previous barrier. The halo alternates by slice
+  // parity on the same argument. The third buffer, free during slice k (it was slice k - 1's and
+  // becomes slice k + 2's), takes each warp's resolved row in the warp's own block: only that
+  // warp writes or reads its block until it fills it with slice k + 2's fractions itself, and it
+  // copies the row out in between.
+  own6(bufs[0], k0);
   if (inxy && k0 >= 1) prev5[q] = frac_at(ix + n[0] * (jy + n[1] * (k0 - 1)), 5);
+  const int lane = q & 31, wrow = q >> 5;
+  static_assert(X == 32, "a warp is one row of the slice");
   for (long long k = k0; k < k1; ++k) {
+    const int r3 = int((k - k0) % 3), par = int((k - k0) & 1);
+    T (*cur)[NF][X] = bufs[r3];
+    T (*nxt)[NF][X] = bufs[r3 == 2 ? 0 : r3 + 1];
+    T* const res = &bufs[r3 == 0 ? 2 : r3 - 1][wrow][0][0];  // this warp's row, cell-major
+    T (*hxp)[Y] = hx[par];
+    T (*hyp)[X] = hy[par];
     if (k + 1 < n[2]) own6(nxt, k + 1);
     for (int h = q; h < 2 * Y + 2 * X; h += NT) {
       if (h < 2 * Y) {
         const int side = h / Y, y = h % Y;
         const long long ii = side == 0 ? i0 - 1 : i0 + X, jj = j0 + y;
-        if (ii >= 0 && ii < n[0] && jj < n[1]) hx[side][y] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
+        if (ii >= 0 && ii < n[0] && jj < n[1]) hxp[side][y] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
       } else {
         const int side = (h - 2 * Y) / X, x = (h - 2 * Y) % X;
         const long long ii = i0 + x, jj = side == 0 ? j0 - 1 : j0 + Y;
-        if (jj >= 0 && jj < n[1] && ii < n[0]) hy[side][x] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
+        if (jj >= 0 && jj < n[1] && ii < n[0]) hyp[side][x] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
       }
     }
     __syncthreads();
@@ -399,45 +413,41 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
         const int c = f >> 1;
-        const T mine = cur[f][q];
+        const T mine = cur[ly][f][lx];
         T r;
         if ((f & 1) == 0) {
           const bool has = idx[c] >= 1;
           T below = T(0);
-          if (has) below = c == 0 ? (lx > 0 ? cur[1][q - 1] : hx[0][ly])
-                                  : c == 1 ? (ly > 0 ? cur[3][q - X] : hy[0][lx]) : prev5[q];
+          if (has) below = c == 0 ? (lx > 0 ? cur[ly][1][lx - 1] : hxp[0][ly])
+                                  : c == 1 ? (ly > 0 ? cur[ly - 1][3][lx] : hyp[0][lx]) : prev5[q];
           r = has ? (below + mine) * T(0.5) : mine;
         } else {
           const bool has = idx[c] <= n[c] - 2;
           T above = T(0);
-          if (has) above = c == 0 ? (lx < X - 1 ? cur[0][q + 1] : hx[1][ly])
-                                  : c == 1 ? (ly < Y - 1 ? cur[2][q + X] : hy[1][lx]) : nxt[4][q];
+          if (has) above = c == 0 ? (lx < X - 1 ? cur[ly][0][lx + 1] : hxp[1][ly])
+                                  : c == 1 ? (ly < Y - 1 ? cur[ly + 1][2][lx] : hyp[1][lx]) : nxt[ly][4][lx];
           r = has ? (mine + above) * T(0.5) : mine;
         }
-        res[q * NF + f] = r;
+        res[lx * NF + f] = r;
       }
     }
-    __syncthreads();
-    // the slice's rows leave whole (16-byte vectors where the row is full and aligned)
-    const int rowcells = (int)(n[0] - i0 < X ? n[0] - i0 : X);
-    constexpr int RV = X * NF * int(sizeof(T)) / 16;
-    for (int w = q; w < Y * RV; w += NT) {
-      const int row = w / RV, v = w - row * RV;
-      const long long j = j0 + row;
-      if (j >= n[1]) continue;
+    __syncwarp();
+    // the warp's row leaves whole (16-byte vectors where the row is full and aligned)
+    const long long j = jy;
+    if (j < n[1]) {
+      const int rowcells = (int)(n[0] - i0 < X ? n[0] - i0 : X);
+      constexpr int RV = X * NF * int(sizeof(T)) / 16;
       const long long c0 = i0 + n[0] * (j + n[1] * k);
+      const T* src = res;
       if (rowcells == X && (reinterpret_cast<uintptr_t>(ff + NF * c0) & 15u) == 0) {
-        reinterpret_cast<uint4*>(ff + NF * c0)[v] = reinterpret_cast<const uint4*>(res + row * X * NF)[v];
+        for (int v = lane; v < RV; v += 32)
+          reinterpret_cast<uint4*>(ff + NF * c0)[v] = reinterpret_cast<const uint4*>(src)[v];
       } else {
-        constexpr int PER = 16 / int(sizeof(T));
-        for (int e = v * PER; e < (v + 1) * PER; ++e)
-          if (e < rowcells * NF) ff[NF * c0 + e] = res[row * X * NF + e];
+        for (int e = lane; e < rowcells * NF; e += 32) ff[NF * c0 + e] = src[e];
       }
     }
-    if (inxy) prev5[q] = cur[5][q];
-    T (*t)[NT] = cur;
-    cur = nxt;
-    nxt = t;
+    if (inxy) prev5[q] = cur[ly][5][lx];
+    __syncwarp();  // every lane has copied the row out before any writes the next slice's fractions here
   }
 }
 
