@@ -632,27 +632,40 @@ __global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_
   unsigned long long cut = 0, ins = 0, out = 0, am = 0;
   T vmin = T(1);
   const long long nvec = vec_ok ? ncell / 16 : 0;
-  for (long long g = blockIdx.x * (long long)NT + threadIdx.x; g < nvec; g += (long long)gridDim.x * NT) {
-    const uint4 kk = reinterpret_cast<const uint4*>(kind)[g];
-    const uint4 aa = reinterpret_cast<const uint4*>(amb)[g];
+  const uint4* kind4 = reinterpret_cast<const uint4*>(kind);
+  const uint4* amb4 = reinterpret_cast<const uint4*>(amb);
+  // sixteen cells: the bytes of each word equal to 2 (cut), 0 (inside), 1 (outside), and the
+  // nonzero ambiguous bytes, counted exactly whatever the byte values; the fraction is only read
+  // for cut cells, which are few
+  auto sixteen = [&](const uint4 kk, const uint4 aa, long long g) {
     const unsigned kw[4] = {kk.x, kk.y, kk.z, kk.w};
     const unsigned aw[4] = {aa.x, aa.y, aa.z, aa.w};
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
-      // four cells at once: the bytes of a word equal to 2 (cut), 0 (inside), 1 (outside), and
-      // the nonzero ambiguous bytes, counted exactly whatever the byte values
       const unsigned cutm = zero_bytes(kw[w] ^ 0x02020202u);
       cut += __popc(cutm);
       ins += __popc(zero_bytes(kw[w]));
       out += __popc(zero_bytes(kw[w] ^ 0x01010101u));
       am += 4 - __popc(zero_bytes(aw[w]));
-      // the fraction is only read for cut cells, which are few
       for (unsigned m = cutm; m; m &= m - 1) {
         const T v = vf[16 * g + 4 * w + ((__ffs(m) - 1) >> 3)];
         if (v > T(0) && v < vmin) vmin = v;
       }
     }
+  };
+  const long long stride = (long long)gridDim.x * NT;
+  long long g = blockIdx.x * (long long)NT + threadIdx.x;
+  for (; g + 3 * stride < nvec; g += 4 * stride) {  // four strides' loads in flight before any test
+    uint4 kk[4], aa[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      kk[u] = kind4[g + u * stride];
+      aa[u] = amb4[g + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) sixteen(kk[u], aa[u], g + u * stride);
   }
+  for (; g < nvec; g += stride) sixteen(kind4[g], amb4[g], g);
   for (long long i = 16 * nvec + blockIdx.x * (long long)NT + threadIdx.x; i < ncell; i += (long long)gridDim.x * NT)
     report_cell<T>(kind[i], amb[i], kind[i] == 2 ? vf[i] : T(1), cut, ins, out, am, vmin);
 #pragma unroll
@@ -806,7 +819,9 @@ cudaError_t launch_calc_volume(const DevGrid<T>& g, const DevTape& tape, double*
 
 cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* amb, const void* vf, int is_f64,
                           unsigned long long* counts, double* vmin, cudaStream_t s) {
-  const int nb = blocks_for((ncell + 15) / 16, 8);
+  // four CTAs of 256 per SM (the unrolled loop's registers), each thread with eight 16-byte
+  // loads in flight: 128 KB per SM
+  const int nb = blocks_for((ncell + 15) / 16, 4);
   unsigned long long* vb = reinterpret_cast<unsigned long long*>(vmin);
   const int vec_ok = ((reinterpret_cast<uintptr_t>(kind) | reinterpret_cast<uintptr_t>(amb)) & 15u) == 0;
   if (is_f64)
