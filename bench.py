@@ -109,8 +109,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def slab_range(n, slab=8):
+    """The middle z-slab of cell layers the CPU legs sample: layers k0..k0+slab-1 of the n^3 grid."""
+    k0 = max(n // 2 - slab // 2, 0)
+    return k0, min(k0 + slab, n)
+
+
 def cpu_port_rate(n, prec, seconds=8.0, slab=8):
-    """Oracle throughput (cells/s) on a slab of the workload with every host thread."""
+    """Oracle throughput (cells/s) on the middle slab of the workload with every host thread; the
+    slab is evaluated with the full grid's node coordinates, so its output is the whole-grid
+    oracle's for those layers. Returns (rate, threads, sample, (phi, columns) of the last run)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     from __graft_entry__ import load_package
@@ -118,21 +126,44 @@ def cpu_port_rate(n, prec, seconds=8.0, slab=8):
     threads = os.cpu_count() or 1
     po.set_threads(threads)
     g = cc.workloads.csg_grid(n)
-    # a slab through the middle of the body: n x n x slab cells
-    sub = cc.CartesianGrid((g.x0[0], g.x0[1], -slab / 2 * g.d[2]), (n, n, slab), g.d)
+    k0, k1 = slab_range(n, slab)
     tape = cc.flatten(cc.workloads.csg_body(0), 3)
     table = cc.mc_tables.project_table()
     t0 = time.perf_counter()
     cells = 0
     reps = 0
     while True:
-        po.mc_update(sub, tape, table, prec)
-        cells += sub.ncell
+        out = po.mc_update_slab(g, tape, table, prec, k0, k1)
+        cells += n * n * (k1 - k0)
         reps += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    return cells / dt, threads, f"{reps} x oracle mc_update of a {n}x{n}x{slab} slab of the workload ({dt:.1f} s)"
+    sample = (f"{reps} x oracle mc_update of cell layers {k0}..{k1 - 1} of the {n}^3 workload ({n}x{n}x{k1 - k0} "
+              f"cells, full-grid node coordinates, {dt:.1f} s); cells/s of that sample, extrapolated to the "
+              f"whole grid only in ms_per_step")
+    return cells / dt, threads, sample, out
+
+
+def slab_of_cache(cache, n, slab=8):
+    """Host copies of the middle slab's phi (node layers k0..k1) and columns (cell layers k0..k1-1)."""
+    k0, k1 = slab_range(n, slab)
+    lay, nlay = n * n, (n + 1) * (n + 1)
+    cols = {f: getattr(cache.cells, f)[lay * k0:lay * k1].cpu().numpy() for f in CELL_FIELDS}
+    return cache.phi[nlay * k0:nlay * (k1 + 1)].cpu().numpy(), cols
+
+
+CELL_FIELDS = ("kind", "ambiguous", "volume_fraction", "centroid", "face_fraction", "face_centroid_local",
+               "interface_centroid")
+
+
+def same_bits(dev, ref):
+    """Device slab (phi, columns) equal to the oracle's bit for bit."""
+    import numpy as np
+
+    def eq(a, b):
+        return np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+    return bool(eq(dev[0], ref[0]) and all(eq(dev[1][f], ref[1][f]) for f in CELL_FIELDS))
 
 
 def run_reference(args, rank, world):
@@ -143,7 +174,7 @@ def run_reference(args, rank, world):
     for _ in range(args.warmup):
         cpu_port_rate(args.n, prec, seconds=0.5)
     for _ in range(args.steps):
-        r, threads, sample = cpu_port_rate(args.n, prec, seconds=2.0)
+        r, threads, sample, _ = cpu_port_rate(args.n, prec, seconds=2.0)
         rates.append(r)
     v = statistics.median(rates)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cells/s", "n_gpus": args.gpus,
@@ -247,8 +278,10 @@ def run_ours(args, rank, world, dist):
     bytes64 = cc.workloads.mc_bytes_per_update(n, 8)
     cachem, totalm, perm = timed_updates(torch.float32, "mixed")
     msm = max_over_ranks(totalm, dist, dev) / args.steps
-    precision = {"reference": "the Float64 update of the same body and grid (bit-identical to the Float64 oracle)",
-                 "float32": field_errors(cache, cache64), "mixed": field_errors(cachem, cache64)}
+    precision = precision_report(cc, g, cache, cache64, cachem, dev)
+    # the middle slab of each cache, for the oracle check of the CPU-baseline leg below
+    slabs = {"float32": slab_of_cache(cache, n), "float64": slab_of_cache(cache64, n),
+             "mixed": slab_of_cache(cachem, n)} if (not args.no_cpu and world == 1) else None
     del cache, cache64, cachem
     torch.cuda.empty_cache()
     precision["degenerate_deciders"] = degenerate_decider_errors(cc, dev)
@@ -272,7 +305,10 @@ def run_ours(args, rank, world, dist):
                          "per": "one update (fill + cut-band launch), CUDA events",
                          "traffic_source": "ncu dram__bytes_read+write of fill and cut at 256^3, scaled by cells"},
             "e2e": {"value": job_rate(world, n ** 3, e2e_s), "unit": "cells/s", "h2d_bytes_per_step": int(ops_bytes),
-                    "d2h_bytes_per_step": 48},
+                    "d2h_bytes_per_step": 48,
+                    "note": "per step: the host body flattened and uploaded, a blocking update_cache, the cut-cell "
+                            "report read back; the columns stay on the device, as the reference's CuArray cache "
+                            "does"},
             "gpu_launches": 2 * args.steps,  # per update: the fill kernel and the cut-band kernel
             "clocks": clocks,
             "fp64": {"value": job_rate(world, n ** 3, ms64 * 1e-3), "ms_per_step": ms64,
@@ -285,18 +321,31 @@ def run_ours(args, rank, world, dist):
             "mesh": mesh,
             "plic": plic,
             "report": rep}
-    if not args.no_cpu and world == 1:
-        v, threads, sample = cpu_port_rate(n, 0)
+    if slabs is not None:
+        v, threads, sample, ref32 = cpu_port_rate(n, 0)
         line["cpu_baseline"] = {"value": v, "unit": "cells/s", "cores": threads, "kind": "port", "sample": sample}
+        # the timed oracle's own output checks the device's Float32 slab; one more oracle run each
+        # checks the Float64 and mixed slabs
+        _, _, _, ref64 = cpu_port_rate(n, 1, seconds=0.0)
+        _, _, _, refm = cpu_port_rate(n, 2, seconds=0.0)
+        k0, k1 = slab_range(n)
+        precision["oracle_check"] = {
+            "slab": f"cell layers {k0}..{k1 - 1} of {n}^3 ({n * n * (k1 - k0)} cells), every column and phi",
+            "float32_bitwise": same_bits(slabs["float32"], ref32),
+            "float64_bitwise": same_bits(slabs["float64"], ref64),
+            "mixed_bitwise": same_bits(slabs["mixed"], refm)}
+    else:
+        precision["oracle_check"] = "not run (--no-cpu or more than one rank)"
     print(json.dumps(line), flush=True)
 
 
-def field_errors(c, ref, chunk=1 << 23):
+def field_errors(c, ref, chunk=1 << 23, keep=None):
     """Max and mean absolute error of every column of cache ``c`` against cache ``ref`` (same
     grid), over all cells and over the cells whose eight corner values classify the same in both
     (marching cubes' nudged signs, phi > -eps(T): there the difference is the arithmetic's;
     elsewhere a value within eps(Float32) of zero, or a sampled value near zero, flipped side),
-    and the cells whose kind or ambiguous flag differ. Computed on the device in chunks."""
+    and the cells whose kind or ambiguous flag differ. ``keep`` (a bool per cell) restricts the
+    "same signs" statistics further. Computed on the device in chunks."""
     import torch
     import torch.nn.functional as F
     n = c.cells.kind.numel()
@@ -307,10 +356,13 @@ def field_errors(c, ref, chunk=1 << 23):
     same = (F.max_pool3d(flip, 2, stride=1) == 0).reshape(-1)
     del flip
     out = {"cells_with_a_flipped_corner_sign": int(n - same.sum().item())}
+    if keep is not None:
+        same &= keep
+    out["cells_in_same_signs_stats"] = int(same.sum().item())
     for f in ("volume_fraction", "centroid", "face_fraction", "face_centroid_local", "interface_centroid"):
         a = getattr(c.cells, f).reshape(n, -1)
         b = getattr(ref.cells, f).reshape(n, -1)
-        mx = sm = mxs = 0.0
+        mx = sm = mxs = sms = 0.0
         for s0 in range(0, n, chunk):
             d = (a[s0:s0 + chunk].double() - b[s0:s0 + chunk]).abs()
             mx = max(mx, d.max().item())
@@ -318,12 +370,56 @@ def field_errors(c, ref, chunk=1 << 23):
             ds = d[same[s0:s0 + chunk]]
             if ds.numel():
                 mxs = max(mxs, ds.max().item())
-        out[f] = {"max": mx, "mean": sm / a.numel(), "max_same_signs": mxs}
+                sms += ds.sum().item()
+        out[f] = {"max": mx, "mean": sm / a.numel(), "max_same_signs": mxs,
+                  "mean_same_signs": sms / max(int(same.sum().item()) * a.shape[1], 1)}
     d = (c.phi.double() - ref.phi).abs()
     out["phi"] = {"max": d.max().item(), "mean": d.mean().item()}
     del d
     out["kind_mismatch"] = int((c.cells.kind != ref.cells.kind).sum().item())
     out["ambiguous_mismatch"] = int((c.cells.ambiguous != ref.cells.ambiguous).sum().item())
+    return out
+
+
+def cells_differ(a, b, chunk=1 << 23):
+    """Per cell: does any column of cache ``a`` differ from cache ``b`` (same dtype) bit for bit."""
+    import torch
+    n = a.cells.kind.numel()
+    out = torch.zeros(n, dtype=torch.bool, device=a.cells.kind.device)
+    for f in ("kind", "ambiguous", "volume_fraction", "centroid", "face_fraction", "face_centroid_local",
+              "interface_centroid"):
+        x = getattr(a.cells, f).reshape(n, -1)
+        y = getattr(b.cells, f).reshape(n, -1)
+        iv = torch.int8 if x.element_size() == 1 else (torch.int32 if x.element_size() == 4 else torch.int64)
+        for s0 in range(0, n, chunk):
+            out[s0:s0 + chunk] |= (x[s0:s0 + chunk].view(iv) != y[s0:s0 + chunk].view(iv)).any(dim=1)
+    return out
+
+
+def precision_report(cc, g, c32, c64, cm, dev):
+    """Every column's error of the Float32 and mixed updates against Float64, split into its
+    sources. ``c64_on_32`` is the Float64 cell construction run on the Float32 update's phi: against
+    the Float64 update it isolates the error of sampling phi in Float32 (corner signs and the
+    deciders' inputs move); against it, the Float32 and mixed updates show their arithmetic alone.
+    Float32 differs from mixed only where a Float32 decider (or a tiny edge root) decides otherwise
+    than Float64 on the same values: those cells are counted, and the Float32 arithmetic-only
+    statistics leave them out."""
+    import torch
+    c64on32 = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float64, device=dev)
+    cc.update_cache(c64on32, cc.NodalField(c32.phi.double()), g)
+    flips = cells_differ(c32, cm)
+    out = {"reference": "the Float64 update of the same body and grid",
+           "float32": field_errors(c32, c64), "mixed": field_errors(cm, c64),
+           "input_rounding": {"what": "Float64 cells from the Float32 phi, against the Float64 update",
+                              **field_errors(c64on32, c64)},
+           "float32_decider_flip_cells": int(flips.sum().item()),
+           "float32_arithmetic": {"what": "Float32 against Float64 cells on the same Float32 phi, cells where "
+                                          "Float32 and mixed agree (same decisions)",
+                                  **field_errors(c32, c64on32, keep=~flips)},
+           "mixed_arithmetic": {"what": "mixed against Float64 cells on the same Float32 phi",
+                                **field_errors(cm, c64on32)}}
+    del c64on32, flips
+    torch.cuda.empty_cache()
     return out
 
 

@@ -867,33 +867,42 @@ Tape<T> make_tape(const cc_optape* t) {
   return r;
 }
 
-// _sample_nodes_kernel!, src/marching_squares/cache.jl:67-70
+// _sample_nodes_kernel!, src/marching_squares/cache.jl:67-70, over the node layers kn0..kn1
+// (inclusive; 3D) of the full grid: every node's coordinates are get_node's expression with its
+// global index, and phi holds the layers from kn0 on.
 template <class T, int D>
-void sample_nodes(const cc_grid& g, const Tape<T>& tp, T* phi) {
-  const int64_t nx = g.n[0] + 1, ny = g.n[1] + 1, nz = D == 3 ? g.n[2] + 1 : 1;
+void sample_nodes_range(const cc_grid& g, const Tape<T>& tp, T* phi, int64_t kn0, int64_t kn1) {
+  const int64_t nx = g.n[0] + 1, ny = g.n[1] + 1, nz = D == 3 ? kn1 - kn0 + 1 : 1;
   const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
   const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
   parallel_for(ny * nz, [&](int64_t row) {
-    const int64_t j = row % ny, k = row / ny;
+    const int64_t j = row % ny, kl = row / ny;
     for (int64_t i = 0; i < nx; ++i) {
       T x[3];
       x[0] = node_coord(x0[0], d[0], i);
       x[1] = node_coord(x0[1], d[1], j);
-      x[2] = node_coord(x0[2], d[2], k);
-      phi[i + nx * (j + ny * k)] = eval_tape<T, D, T>(tp, x);
+      x[2] = node_coord(x0[2], d[2], D == 3 ? kn0 + kl : kl);
+      phi[i + nx * (j + ny * kl)] = eval_tape<T, D, T>(tp, x);
     }
   });
 }
 
-// _nodal_cells_kernel!, src/marching_squares/cache.jl:75-78, 3D
+template <class T, int D>
+void sample_nodes(const cc_grid& g, const Tape<T>& tp, T* phi) {
+  sample_nodes_range<T, D>(g, tp, phi, 0, D == 3 ? g.n[2] : 0);
+}
+
+// _nodal_cells_kernel!, src/marching_squares/cache.jl:75-78, 3D, over the cell layers k0..k1-1
+// of the full grid: phi holds the node layers k0..k1 and the columns the cell layers from k0 on;
+// node coordinates use the global indices.
 template <class T>
-void mc_cells(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells& c) {
-  const int64_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+void mc_cells_range(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells& c, int64_t k0, int64_t k1) {
+  const int64_t n0 = g.n[0], n1 = g.n[1];
   const int64_t nx = n0 + 1, ny = n1 + 1;
   const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
   const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
-  parallel_for(n1 * n2, [&](int64_t row) {
-    const int64_t j = row % n1, k = row / n1;
+  parallel_for(n1 * (k1 - k0), [&](int64_t row) {
+    const int64_t j = row % n1, kl = row / n1, k = k0 + kl;
     for (int64_t i = 0; i < n0; ++i) {
         T nodes[8][3], ph[8];
         for (int q = 0; q < 8; ++q) {
@@ -901,13 +910,18 @@ void mc_cells(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells&
           nodes[q][0] = node_coord(x0[0], d[0], ii);
           nodes[q][1] = node_coord(x0[1], d[1], jj);
           nodes[q][2] = node_coord(x0[2], d[2], kk);
-          ph[q] = phi[ii + nx * (jj + ny * kk)];
+          ph[q] = phi[ii + nx * (jj + ny * (kk - k0))];
         }
         CellOut<T, 3> o;
         mc_moments(tb, nodes, ph, d, o);
-        store<T, 3>(c, i + n0 * (j + n1 * k), o);
+        store<T, 3>(c, i + n0 * (j + n1 * kl), o);
     }
   });
+}
+
+template <class T>
+void mc_cells(const cc_grid& g, const McTable& tb, const T* phi, const cc_cells& c) {
+  mc_cells_range<T>(g, tb, phi, c, 0, g.n[2]);
 }
 
 // generate_mesh (src/marching_cubes/surface.jl:82-112) restated for the project's device mesh:
@@ -1209,27 +1223,44 @@ inline T face_area(const T* n, T a, T frac, bool valid, const T* cs, int k /*0-b
   }
 }
 
+// _plic_fit_kernel! + _plic_face_fraction_kernel! (src/plic/cache.jl:96-162) over the cell layers
+// k0..k1-1 of the full grid (3D; 2D takes the whole grid): the planes of the layers k0-1..k1 (those
+// inside the grid) are fitted, so the slab's faces resolve against the same neighbours as in the
+// whole-grid update. The columns, normals, intercepts and flags hold the slab's cells from k0 on.
 template <class T, int D>
-void plic_update(const cc_grid& g, const Tape<T>& tp, const cc_cells& c, T* normals, T* intercepts,
-                 uint8_t* is_valid) {
+void plic_update_range(const cc_grid& g, const Tape<T>& tp, const cc_cells& c, T* normals, T* intercepts,
+                       uint8_t* is_valid, int64_t k0, int64_t k1) {
   const int64_t n[3] = {g.n[0], g.n[1], D == 3 ? g.n[2] : 1};
   const T x0[3] = {T(g.x0[0]), T(g.x0[1]), T(g.x0[2])};
   const T d[3] = {T(g.d[0]), T(g.d[1]), T(g.d[2])};
-  const int64_t ncell = n[0] * n[1] * n[2];
-  T* vf = static_cast<T*>(c.volume_fraction);
-  parallel_for(ncell, [&](int64_t ci) {
+  if (D == 2) { k0 = 0; k1 = 1; }
+  const int64_t h0 = k0 > 0 ? k0 - 1 : 0, h1 = k1 < n[2] ? k1 + 1 : n[2];  // fitted layers [h0, h1)
+  const int64_t nlay = n[0] * n[1];
+  const int64_t nfit = nlay * (h1 - h0);
+  std::vector<T> hn(size_t(nfit) * D), ha(nfit), hvf(nfit);
+  std::vector<uint8_t> hv(nfit);
+  parallel_for(nfit, [&](int64_t li) {
+    const int64_t ci = li + nlay * h0;
     const int64_t idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
     Plane<T, D> pl = cell_plane<T, D>(tp, x0, d, idx);
-    const T frac = T(1) - pl.fraction;
-    for (int a = 0; a < D; ++a) normals[D * ci + a] = pl.n[a];
-    intercepts[ci] = pl.a;
-    is_valid[ci] = pl.valid ? 1 : 0;
-    vf[ci] = frac;
-    c.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+    for (int a = 0; a < D; ++a) hn[D * li + a] = pl.n[a];
+    ha[li] = pl.a;
+    hv[li] = pl.valid ? 1 : 0;
+    hvf[li] = T(1) - pl.fraction;
   });
+  T* vf = static_cast<T*>(c.volume_fraction);
   T* ff = static_cast<T*>(c.face_fraction);
-  parallel_for(ncell, [&](int64_t ci) {
+  const int64_t nout = nlay * (k1 - k0);
+  parallel_for(nout, [&](int64_t oi) {
+    const int64_t ci = oi + nlay * k0;  // global cell index
+    const int64_t li = ci - nlay * h0;  // index among the fitted layers
     const int64_t idx[3] = {ci % n[0], (ci / n[0]) % n[1], ci / (n[0] * n[1])};
+    const T frac = hvf[li];
+    for (int a = 0; a < D; ++a) normals[D * oi + a] = hn[D * li + a];
+    intercepts[oi] = ha[li];
+    is_valid[oi] = hv[li];
+    vf[oi] = frac;
+    c.kind[oi] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
     for (int k = 0; k < 2 * D; ++k) {
       const int cax = k >> 1;
       int64_t stride = 1;
@@ -1237,23 +1268,29 @@ void plic_update(const cc_grid& g, const Tape<T>& tp, const cc_cells& c, T* norm
       T full;
       if (D == 2) full = d[1 - cax];
       else full = full_face_area3(d, k);
-      auto area_of = [&](int64_t cj, int kk) {
-        return face_area<T, D>(normals + D * cj, intercepts[cj], vf[cj], is_valid[cj] != 0, d, kk);
+      auto area_of = [&](int64_t lj, int kk) {
+        return face_area<T, D>(hn.data() + D * lj, ha[lj], hvf[lj], hv[lj] != 0, d, kk);
       };
-      const T own = area_of(ci, k);
+      const T own = area_of(li, k);
       T r;
       if ((k & 1) == 0) {
         const bool has = idx[cax] >= 1;
-        const T below = area_of(has ? ci - stride : ci, k + 1);
+        const T below = area_of(has ? li - stride : li, k + 1);
         r = has ? (below / full + own / full) / T(2) : own / full;
       } else {
         const bool has = idx[cax] <= n[cax] - 2;
-        const T above = area_of(has ? ci + stride : ci, k - 1);
+        const T above = area_of(has ? li + stride : li, k - 1);
         r = has ? (own / full + above / full) / T(2) : own / full;
       }
-      ff[2 * D * ci + k] = r;
+      ff[2 * D * oi + k] = r;
     }
   });
+}
+
+template <class T, int D>
+void plic_update(const cc_grid& g, const Tape<T>& tp, const cc_cells& c, T* normals, T* intercepts,
+                 uint8_t* is_valid) {
+  plic_update_range<T, D>(g, tp, c, normals, intercepts, is_valid, 0, D == 3 ? g.n[2] : 1);
 }
 
 template <class T, int D>
@@ -1461,6 +1498,39 @@ int oc_mc_cells_from_phi(int prec, const cc_grid* g, const uint8_t* table, const
   if (!tb.parse(table)) return CC_BAD_TABLE;
   if (prec == 1) oc::mc_cells<double>(*g, tb, (const double*)phi, *c);
   else oc::mc_cells<float>(*g, tb, (const float*)phi, *c);
+  return 0;
+}
+
+// Marching cubes over the cell layers k0..k1-1 of the full grid g: phi receives the node layers
+// k0..k1 and the columns the slab's cells, each computed with its global indices.
+int oc_mc_update_slab(int prec, const cc_grid* g, const cc_optape* t, const uint8_t* table, int64_t k0,
+                      int64_t k1, void* phi, const cc_cells* c) {
+  if (g->dim != 3 || k0 < 0 || k1 > g->n[2] || k0 >= k1) return CC_BAD_ARG;
+  oc::MixedScope mixed(prec == 2);
+  oc::McTable tb;
+  if (!tb.parse(table)) return CC_BAD_TABLE;
+  if (prec == 1) {
+    oc::sample_nodes_range<double, 3>(*g, oc::make_tape<double>(t), (double*)phi, k0, k1);
+    oc::mc_cells_range<double>(*g, tb, (const double*)phi, *c, k0, k1);
+  } else {
+    oc::sample_nodes_range<float, 3>(*g, oc::make_tape<float>(t), (float*)phi, k0, k1);
+    oc::mc_cells_range<float>(*g, tb, (const float*)phi, *c, k0, k1);
+  }
+  return 0;
+}
+
+// PLIC over the cell layers k0..k1-1 of the full 3D grid g (the layers either side fitted too, so
+// the faces resolve as in the whole-grid update); outputs hold the slab's cells.
+int oc_plic_update_slab(int prec, const cc_grid* g, const cc_optape* t, int64_t k0, int64_t k1, const cc_cells* c,
+                        void* normals, void* intercepts, uint8_t* is_valid) {
+  if (g->dim != 3 || k0 < 0 || k1 > g->n[2] || k0 >= k1) return CC_BAD_ARG;
+  oc::MixedScope mixed(prec == 2);
+  if (prec == 1)
+    oc::plic_update_range<double, 3>(*g, oc::make_tape<double>(t), *c, (double*)normals, (double*)intercepts,
+                                     is_valid, k0, k1);
+  else
+    oc::plic_update_range<float, 3>(*g, oc::make_tape<float>(t), *c, (float*)normals, (float*)intercepts,
+                                    is_valid, k0, k1);
   return 0;
 }
 

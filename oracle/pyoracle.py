@@ -61,6 +61,10 @@ def lib():
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_plic_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_mc_update_slab.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,
+                                        C.c_void_p, C.c_void_p]
+        L.oc_plic_update_slab.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_mc_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -202,6 +206,39 @@ def plic_mesh(g, normals, intercepts, valid, prec, min_frac=1e-4):
 def mc_update(g, tape, table: bytes, prec):
     phi = sample_nodes(g, tape, prec)
     return phi, mc_cells_from_phi(g, phi, table, prec)
+
+
+def mc_update_slab(g, tape, table: bytes, prec, k0, k1):
+    """Marching cubes over the cell layers k0..k1-1 of the full 3D grid g, every node at its global
+    get_node coordinates: (phi of the node layers k0..k1, columns of the slab's cells)."""
+    T = dtype_of(prec)
+    nx, ny = g.n[0] + 1, g.n[1] + 1
+    phi = np.zeros(nx * ny * (k1 - k0 + 1), T)
+    cols = alloc_cells(g.n[0] * g.n[1] * (k1 - k0), 3, prec)
+    t, keep = tape_struct(tape)
+    tb = np.frombuffer(table, np.uint8).copy()
+    rc = lib().oc_mc_update_slab(prec, C.byref(grid_struct(g)), C.byref(t), _ptr(tb), C.c_int64(k0), C.c_int64(k1),
+                                 _ptr(phi), C.byref(cells_struct(cols)))
+    assert rc == 0, rc
+    return phi, cols
+
+
+def plic_update_slab(g, tape, prec, k0, k1):
+    """PLIC over the cell layers k0..k1-1 of the full 3D grid g (the neighbouring layers fitted too):
+    (columns, normals, intercepts, is_valid) of the slab's cells."""
+    T = dtype_of(prec)
+    m = g.n[0] * g.n[1] * (k1 - k0)
+    cols = alloc_cells(m, 3, prec)
+    for k in ("centroid", "face_centroid_local", "interface_centroid"):
+        cols[k][...] = np.nan
+    normals = np.zeros((m, 3), T)
+    intercepts = np.zeros(m, T)
+    valid = np.zeros(m, np.uint8)
+    t, keep = tape_struct(tape)
+    rc = lib().oc_plic_update_slab(prec, C.byref(grid_struct(g)), C.byref(t), C.c_int64(k0), C.c_int64(k1),
+                                   C.byref(cells_struct(cols)), _ptr(normals), _ptr(intercepts), _ptr(valid))
+    assert rc == 0, rc
+    return cols, normals, intercepts, valid
 
 
 def ms_cells_from_phi(g, phi, prec):
