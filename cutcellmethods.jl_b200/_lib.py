@@ -47,6 +47,8 @@ EXPORTS = {
     "cc_handle_create": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
     "cc_handle_destroy": [C.c_void_p],
     "cc_handle_set_mc_table": [C.c_void_p, C.c_void_p, C.c_size_t],
+    "cc_handle_status": [C.c_void_p],
+    "cc_set_wait_limit": [C.c_int64],
     "cc_mc_update": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_mc_cells_from_phi": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_ms_update": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
@@ -121,7 +123,8 @@ def load(build_if_stale: bool = True):
             for name, args in EXPORTS.items():
                 fn = getattr(L, name)
                 fn.argtypes = args
-                fn.restype = C.c_char_p if name in ("cc_version", "cc_last_error") else C.c_int
+                fn.restype = (C.c_char_p if name in ("cc_version", "cc_last_error")
+                              else C.c_int64 if name == "cc_set_wait_limit" else C.c_int)
             _lib = L
         return _lib
 

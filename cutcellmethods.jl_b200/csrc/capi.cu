@@ -98,6 +98,57 @@ struct DeviceGuard {
 
 namespace cci {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// Every index a kernel takes from a tiling table blob is checked here, once, on the host: lookup
+// entries (test count, Lewiner case, face codes, outcome range), outcomes (interior-test kind,
+// edge, tiles) and tiles (triangle count, code range, codes 1..13).
+bool check_mc_table(const unsigned char* b, size_t nbytes, TableLayout* out, std::string* why) {
+  auto no = [&](const char* m) { if (why) *why = m; return false; };
+  if (!b) return no("null table");
+  if (nbytes < sizeof(cc_mc_table_header) + 256 * sizeof(cc_mc_lut)) return no("table too short");
+  cc_mc_table_header hd;
+  std::memcpy(&hd, b, sizeof hd);
+  if (hd.magic != CC_MC_TABLE_MAGIC || hd.version != 1) return no("not a tiling table");
+  const size_t need = sizeof(cc_mc_table_header) + 256 * sizeof(cc_mc_lut) + hd.n_outcomes * sizeof(cc_mc_outcome) +
+                      hd.n_tiles * sizeof(cc_mc_tile) + hd.n_codes;
+  if (need > nbytes || hd.total_bytes != nbytes || hd.n_outcomes > 65535 || hd.n_tiles > 65535)
+    return no("table sizes inconsistent");
+  const cc_mc_lut* luts = reinterpret_cast<const cc_mc_lut*>(b + sizeof hd);
+  const cc_mc_outcome* outs = reinterpret_cast<const cc_mc_outcome*>(luts + 256);
+  const cc_mc_tile* tiles = reinterpret_cast<const cc_mc_tile*>(outs + hd.n_outcomes);
+  const uint8_t* codes = reinterpret_cast<const uint8_t*>(tiles + hd.n_tiles);
+  for (int l = 0; l < 256; ++l) {
+    const cc_mc_lut& e = luts[l];
+    if (e.ntests > 6 || e.lcase < 1 || e.lcase > 15) return no("bad lookup entry");
+    if (size_t(e.outcome_base) + (size_t(1) << e.ntests) > hd.n_outcomes) return no("outcome out of range");
+    for (int i = 0; i < e.ntests; ++i)
+      if (e.face[i] == 0 || e.face[i] > 6 || e.face[i] < -6) return no("bad face code");
+  }
+  for (uint32_t o = 0; o < hd.n_outcomes; ++o) {
+    const cc_mc_outcome& oc = outs[o];
+    if (oc.itype > CC_MC_INTERIOR_EDGE || oc.edge > 11 || oc.tile_true >= hd.n_tiles || oc.tile_false >= hd.n_tiles)
+      return no("bad outcome");
+  }
+  for (uint32_t t = 0; t < hd.n_tiles; ++t) {
+    if (tiles[t].ntris > 16 || size_t(tiles[t].code_off) + 3u * tiles[t].ntris > hd.n_codes) return no("bad tile");
+    for (int c = 0; c < 3 * tiles[t].ntris; ++c)
+      if (codes[tiles[t].code_off + c] < 1 || codes[tiles[t].code_off + c] > 13) return no("bad edge code");
+  }
+  if (out) {
+    out->n_outcomes = hd.n_outcomes;
+    out->n_tiles = hd.n_tiles;
+  }
+  return true;
+}
+
+DevTable TableLayout::at(const unsigned char* dev) const {
+  DevTable tb;
+  tb.luts = reinterpret_cast<const cc_mc_lut*>(dev + sizeof(cc_mc_table_header));
+  tb.outs = reinterpret_cast<const cc_mc_outcome*>(tb.luts + 256);
+  tb.tiles = reinterpret_cast<const cc_mc_tile*>(tb.outs + n_outcomes);
+  tb.codes = reinterpret_cast<const uint8_t*>(tb.tiles + n_tiles);
+  return tb;
+}
 }  // namespace cci
 
 
@@ -268,6 +319,19 @@ extern "C" {
 const char* cc_version(void) { return "cutcell_b200 0.1.0 (sm_100a)"; }
 const char* cc_last_error(void) { return g_last_error.c_str(); }
 
+cc_status cc_handle_status(cc_handle* h) {
+  if (!h) return fail(CC_BAD_ARG, "null handle");
+  if (h->status_host && *reinterpret_cast<volatile unsigned*>(h->status_host)) {
+    *reinterpret_cast<volatile unsigned*>(h->status_host) = 0;
+    return fail(CC_DEVICE_TIMEOUT,
+                "a marching-cubes fill CTA gave up waiting on its staging mbarriers; that update's columns are "
+                "not valid");
+  }
+  return CC_OK;
+}
+
+int64_t cc_set_wait_limit(int64_t polls) { return cci::set_wait_limit(polls); }
+
 cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t prec, const int64_t n[3],
                            cc_handle** out) {
   if (!out || !n) return fail(CC_BAD_ARG, "null argument");
@@ -296,6 +360,11 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->tape_copied, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&h->vol_scratch, (2 * cci::calc_volume_blocks() + 2) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->rep_scratch, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaHostAlloc(&h->status_host, sizeof(unsigned), cudaHostAllocMapped);
+  if (e == cudaSuccess) {
+    *h->status_host = 0;
+    e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->status_dev), h->status_host, 0);
+  }
   if (e == cudaSuccess && method == CC_MARCHING_CUBES) {
     const int64_t ncell = h->n[0] * h->n[1] * h->n[2];
     e = cudaMalloc(&h->cut_list, size_t(ncell) * sizeof(unsigned));
@@ -318,6 +387,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->table_dev) cudaFree(h->table_dev);
   if (h->vol_scratch) cudaFree(h->vol_scratch);
   if (h->rep_scratch) cudaFree(h->rep_scratch);
+  if (h->status_host) cudaFreeHost(h->status_host);
   if (h->cut_list) cudaFree(h->cut_list);
   if (h->cut_count) cudaFree(h->cut_count);
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
@@ -332,37 +402,9 @@ cc_status cc_handle_destroy(cc_handle* h) {
 
 cc_status cc_handle_set_mc_table(cc_handle* h, const void* blob, size_t nbytes) {
   if (!h || !blob) return fail(CC_BAD_ARG, "null argument");
-  if (nbytes < sizeof(cc_mc_table_header) + 256 * sizeof(cc_mc_lut)) return fail(CC_BAD_TABLE, "table too short");
-  const unsigned char* b = static_cast<const unsigned char*>(blob);
-  cc_mc_table_header hd;
-  std::memcpy(&hd, b, sizeof hd);
-  if (hd.magic != CC_MC_TABLE_MAGIC || hd.version != 1) return fail(CC_BAD_TABLE, "not a tiling table");
-  const size_t need = sizeof(cc_mc_table_header) + 256 * sizeof(cc_mc_lut) + hd.n_outcomes * sizeof(cc_mc_outcome) +
-                      hd.n_tiles * sizeof(cc_mc_tile) + hd.n_codes;
-  if (need > nbytes || hd.total_bytes != nbytes || hd.n_outcomes > 65535 || hd.n_tiles > 65535)
-    return fail(CC_BAD_TABLE, "table sizes inconsistent");
-  const cc_mc_lut* luts = reinterpret_cast<const cc_mc_lut*>(b + sizeof hd);
-  const cc_mc_outcome* outs = reinterpret_cast<const cc_mc_outcome*>(luts + 256);
-  const cc_mc_tile* tiles = reinterpret_cast<const cc_mc_tile*>(outs + hd.n_outcomes);
-  const uint8_t* codes = reinterpret_cast<const uint8_t*>(tiles + hd.n_tiles);
-  for (int l = 0; l < 256; ++l) {
-    const cc_mc_lut& e = luts[l];
-    if (e.ntests > 6 || e.lcase < 1 || e.lcase > 15) return fail(CC_BAD_TABLE, "bad lookup entry");
-    if (size_t(e.outcome_base) + (size_t(1) << e.ntests) > hd.n_outcomes) return fail(CC_BAD_TABLE, "outcome out of range");
-    for (int i = 0; i < e.ntests; ++i)
-      if (e.face[i] == 0 || e.face[i] > 6 || e.face[i] < -6) return fail(CC_BAD_TABLE, "bad face code");
-  }
-  for (uint32_t o = 0; o < hd.n_outcomes; ++o) {
-    const cc_mc_outcome& oc = outs[o];
-    if (oc.itype > CC_MC_INTERIOR_EDGE || oc.edge > 11 || oc.tile_true >= hd.n_tiles || oc.tile_false >= hd.n_tiles)
-      return fail(CC_BAD_TABLE, "bad outcome");
-  }
-  for (uint32_t t = 0; t < hd.n_tiles; ++t) {
-    if (tiles[t].ntris > 16 || size_t(tiles[t].code_off) + 3u * tiles[t].ntris > hd.n_codes)
-      return fail(CC_BAD_TABLE, "bad tile");
-    for (int c = 0; c < 3 * tiles[t].ntris; ++c)
-      if (codes[tiles[t].code_off + c] < 1 || codes[tiles[t].code_off + c] > 13) return fail(CC_BAD_TABLE, "bad edge code");
-  }
+  std::string why;
+  cci::TableLayout lay;
+  if (!cci::check_mc_table(static_cast<const unsigned char*>(blob), nbytes, &lay, &why)) return fail(CC_BAD_TABLE, why);
   DeviceGuard dg(h->device);
   if (h->table_dev) { cudaFree(h->table_dev); h->table_dev = nullptr; }
   cudaError_t e = cudaMalloc(&h->table_dev, nbytes);
@@ -370,11 +412,7 @@ cc_status cc_handle_set_mc_table(cc_handle* h, const void* blob, size_t nbytes) 
   e = cudaMemcpy(h->table_dev, blob, nbytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "table upload");
   h->table_bytes = nbytes;
-  unsigned char* base = h->table_dev;
-  h->tb.luts = reinterpret_cast<const cc_mc_lut*>(base + sizeof hd);
-  h->tb.outs = reinterpret_cast<const cc_mc_outcome*>(h->tb.luts + 256);
-  h->tb.tiles = reinterpret_cast<const cc_mc_tile*>(h->tb.outs + hd.n_outcomes);
-  h->tb.codes = reinterpret_cast<const uint8_t*>(h->tb.tiles + hd.n_tiles);
+  h->tb = lay.at(h->table_dev);
   return CC_OK;
 }
 
@@ -398,15 +436,15 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dev_grid<double>(g), tape, static_cast<const double*>(phi_in),
-                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s,
-                               true, false, ps, ps ? pb : 0);
+                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count,
+                               h->status_dev, s, true, false, ps, ps ? pb : 0);
   } else {
     if (body && (st = upload_tape<float>(h, body, 3, s, &tape)) != CC_OK) return st;
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
-                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s, true,
-                              h->prec == CC_MIXED, ps, ps ? pb : 0);
+                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count,
+                              h->status_dev, s, true, h->prec == CC_MIXED, ps, ps ? pb : 0);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching cubes launch");
   return CC_OK;

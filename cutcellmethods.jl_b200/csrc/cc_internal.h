@@ -17,6 +17,15 @@ struct DevTable {
   const uint8_t* codes;
 };
 
+// Where a validated tiling table's parts sit once the blob is at device address `dev`.
+struct TableLayout {
+  uint32_t n_outcomes = 0, n_tiles = 0;
+  DevTable at(const unsigned char* dev) const;
+};
+// Validate a tiling table blob on the host (every index a kernel reads from it); on failure
+// `why` (if not null) receives the reason.
+bool check_mc_table(const unsigned char* blob, size_t nbytes, TableLayout* out, std::string* why);
+
 // Grid narrowed to T on the host (convert(CartesianGrid{D,T}, grid)).
 template <class T>
 struct DevGrid {
@@ -47,13 +56,18 @@ struct Cols {
 // Marching cubes: sample (if phi_in == nullptr: sample from the tape into phi_out) and build
 // every cell. Returns the CUDA launch status.
 // `cut_list` (one slot per cell) and `cut_count` are scratch: the fill pass lists the cut band
-// there and the cut pass reads it back.
+// there and the cut pass reads it back. `status` (host-mapped or device memory) is set to 1 by a
+// fill CTA whose bounded mbarrier wait ran out; the launch never clears it.
 // With with_cut false only the fill pass runs (the cut band is listed, not built).
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      cudaStream_t s, bool with_cut = true, bool mixed = false, void* prune_scratch = nullptr,
-                      size_t prune_bytes = 0);
+                      unsigned* status, cudaStream_t s, bool with_cut = true, bool mixed = false,
+                      void* prune_scratch = nullptr, size_t prune_bytes = 0);
+// The mbarrier poll limit of the fill and learned kernels (cc_set_wait_limit): set returns the old
+// value; a negative argument restores the default.
+long long set_wait_limit(long long polls);
+long long wait_limit();
 // Scratch launch_mc needs to prune a union-of-spheres tape per fill CTA (n_ops ops per CTA).
 size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool f64);
 // The handle's pruning scratch, grown to at least `bytes` (null on failure).
@@ -152,6 +166,8 @@ struct cc_handle {
   cci::DevTable tb{};
   unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
   unsigned* cut_count = nullptr;
+  unsigned* status_host = nullptr;  // pinned, mapped: set by a kernel whose bounded wait ran out
+  unsigned* status_dev = nullptr;   // the device's view of status_host
   double* vol_scratch = nullptr;  // calc_volume partials + result
   unsigned long long* rep_scratch = nullptr;  // report counters + min
   unsigned* mesh_vbase = nullptr;  // generate_mesh: first vertex of each node's cut edges

@@ -21,56 +21,57 @@ namespace {
 // Largest grid the static work list can serve: 2^23 cells (for example 203^3, or 512 x 128 x 128).
 constexpr long long kMaxCells = 8388608;
 constexpr size_t kTableBytes = 64 * 1024;    // the tiling table's device copy
-constexpr size_t kCountOffset = kTableBytes;  // the work list's counter
+constexpr size_t kCountOffset = kTableBytes;  // the work list's counter, then the fill's wait-limit flag
 constexpr size_t kListOffset = kTableBytes + 256;
 constexpr size_t kScratchBytes = kListOffset + size_t(kMaxCells) * sizeof(unsigned);  // 32 MiB + 64.25 KiB
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// The array's device address per device, looked up once with that device current. In host code
-// the symbol g_noalloc_scratch is only a host-side stand-in for the array, never its address.
+// What each device's table slot holds: the context it was uploaded in (a reset device gets a new
+// one, with the array's contents lost) and the blob's size and FNV-1a-64 hash. A call whose table is
+// already there skips the upload, so repeated calls copy nothing from the host.
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
+struct Resident {
+  unsigned long long ctx = 0, hash = 0;
+  size_t bytes = 0;
+};
+Resident g_resident[kMaxDevices];
 std::mutex g_scratch_mutex;
+
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+// The current context's unique id (0 when the driver cannot say: the table is then re-uploaded).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+unsigned long long fnv1a64(const unsigned char* b, size_t n) {
+  unsigned long long h = 0xcbf29ce484222325ull;
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
 
 cc_status fail(cc_status s, const std::string& m) {
   cci::set_last_error(m);  // read back through cc_last_error()
   return s;
-}
-
-bool table_ok(const unsigned char* b, size_t nbytes, cci::DevTable* tb, unsigned char* dev_base) {
-  if (nbytes < sizeof(cc_mc_table_header) + 256 * sizeof(cc_mc_lut)) return false;
-  cc_mc_table_header hd;
-  std::memcpy(&hd, b, sizeof hd);
-  if (hd.magic != CC_MC_TABLE_MAGIC || hd.version != 1 || hd.total_bytes != nbytes) return false;
-  const size_t need = sizeof hd + 256 * sizeof(cc_mc_lut) + hd.n_outcomes * sizeof(cc_mc_outcome) +
-                      hd.n_tiles * sizeof(cc_mc_tile) + hd.n_codes;
-  if (need > nbytes || hd.n_outcomes > 65535 || hd.n_tiles > 65535) return false;
-  const cc_mc_lut* luts = reinterpret_cast<const cc_mc_lut*>(b + sizeof hd);
-  const cc_mc_outcome* outs = reinterpret_cast<const cc_mc_outcome*>(luts + 256);
-  const cc_mc_tile* tiles = reinterpret_cast<const cc_mc_tile*>(outs + hd.n_outcomes);
-  const uint8_t* codes = reinterpret_cast<const uint8_t*>(tiles + hd.n_tiles);
-  for (int l = 0; l < 256; ++l) {
-    const cc_mc_lut& e = luts[l];
-    if (e.ntests > 6 || e.lcase < 1 || e.lcase > 15) return false;
-    if (size_t(e.outcome_base) + (size_t(1) << e.ntests) > hd.n_outcomes) return false;
-    for (int i = 0; i < e.ntests; ++i)
-      if (e.face[i] == 0 || e.face[i] > 6 || e.face[i] < -6) return false;
-  }
-  for (uint32_t o = 0; o < hd.n_outcomes; ++o)
-    if (outs[o].itype > CC_MC_INTERIOR_EDGE || outs[o].edge > 11 || outs[o].tile_true >= hd.n_tiles ||
-        outs[o].tile_false >= hd.n_tiles)
-      return false;
-  for (uint32_t t = 0; t < hd.n_tiles; ++t) {
-    if (tiles[t].ntris > 16 || size_t(tiles[t].code_off) + 3u * tiles[t].ntris > hd.n_codes) return false;
-    for (int c = 0; c < 3 * tiles[t].ntris; ++c)
-      if (codes[tiles[t].code_off + c] < 1 || codes[tiles[t].code_off + c] > 13) return false;
-  }
-  tb->luts = reinterpret_cast<const cc_mc_lut*>(dev_base + sizeof hd);
-  tb->outs = reinterpret_cast<const cc_mc_outcome*>(tb->luts + 256);
-  tb->tiles = reinterpret_cast<const cc_mc_tile*>(tb->outs + hd.n_outcomes);
-  tb->codes = reinterpret_cast<const uint8_t*>(tb->tiles + hd.n_tiles);
-  return true;
 }
 
 }  // namespace
@@ -96,49 +97,57 @@ extern "C" cc_status cc_mc_cells_from_phi_noalloc(int32_t device, int32_t prec, 
     return fail(CC_TOO_LARGE, buf);
   }
   if (table_bytes > kTableBytes) return fail(CC_BAD_TABLE, "tiling table larger than the 64 KiB table slot");
+  const unsigned char* blob = static_cast<const unsigned char*>(table);
+  std::string why;
+  cci::TableLayout lay;
+  if (!cci::check_mc_table(blob, table_bytes, &lay, &why)) return fail(CC_BAD_TABLE, "not a valid tiling table: " + why);
 
   int old = -1;
   cudaGetDevice(&old);
   if (old != device && cudaSetDevice(device) != cudaSuccess) return fail(CC_CUDA_ERR, "cudaSetDevice failed");
   cc_status status = CC_OK;
   do {
+    // The array's device address, looked up on every call with this device current (cheap once
+    // the module is loaded; a device reset can move it). In host code the symbol itself is only a
+    // host-side stand-in for the array, never its address.
     void* base = nullptr;
-    {
-      std::lock_guard<std::mutex> lk(g_scratch_mutex);
-      if (!g_scratch_addr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-          status = fail(CC_CUDA_ERR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-          break;
-        }
-        g_scratch_addr[device] = p;
-      }
-      base = g_scratch_addr[device];
-    }
-    unsigned char* b = static_cast<unsigned char*>(base);
-    cci::DevTable tb{};
-    if (!table_ok(static_cast<const unsigned char*>(table), table_bytes, &tb, b)) {
-      status = fail(CC_BAD_TABLE, "not a valid tiling table");
+    cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      status = fail(CC_CUDA_ERR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       break;
     }
+    unsigned char* b = static_cast<unsigned char*>(base);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemcpyAsync(b, table, table_bytes, cudaMemcpyHostToDevice, s);
+    {
+      std::lock_guard<std::mutex> lk(g_scratch_mutex);
+      Resident& r = g_resident[device];
+      const unsigned long long ctx = current_context_id();
+      const unsigned long long h = fnv1a64(blob, table_bytes);
+      if (ctx == 0 || r.ctx != ctx || r.hash != h || r.bytes != table_bytes) {
+        r = Resident{};
+        e = cudaMemcpyAsync(b, blob, table_bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) r = Resident{ctx, h, table_bytes};
+      }
+    }
     if (e == cudaSuccess) {
-      // the launch clears the work list's counter on the stream before the fill pass
+      // the launch clears the work list's counter on the stream before the fill pass; the word
+      // after it takes the fill's wait-limit flag, which this entry point does not report
       unsigned* count = reinterpret_cast<unsigned*>(b + kCountOffset);
       unsigned* list = reinterpret_cast<unsigned*>(b + kListOffset);
+      const cci::DevTable tb = lay.at(b);
       cci::Cols cols{cells->kind, cells->ambiguous, cells->volume_fraction, cells->centroid, cells->face_fraction,
                      cells->face_centroid_local, cells->interface_centroid};
       cci::DevTape none{nullptr, 0, 0, 0};
       if (prec == CC_F64) {
         cci::DevGrid<double> dg;
         for (int a = 0; a < 3; ++a) { dg.x0[a] = g->x0[a]; dg.d[a] = g->d[a]; dg.n[a] = g->n[a]; }
-        e = cci::launch_mc<double>(dg, none, static_cast<const double*>(phi), nullptr, cols, tb, list, count, s);
+        e = cci::launch_mc<double>(dg, none, static_cast<const double*>(phi), nullptr, cols, tb, list, count,
+                                   count + 1, s);
       } else {
         cci::DevGrid<float> dg;
         for (int a = 0; a < 3; ++a) { dg.x0[a] = float(g->x0[a]); dg.d[a] = float(g->d[a]); dg.n[a] = g->n[a]; }
-        e = cci::launch_mc<float>(dg, none, static_cast<const float*>(phi), nullptr, cols, tb, list, count, s);
+        e = cci::launch_mc<float>(dg, none, static_cast<const float*>(phi), nullptr, cols, tb, list, count,
+                                  count + 1, s);
       }
     }
     if (e != cudaSuccess) status = fail(CC_CUDA_ERR, std::string("marching cubes launch: ") + cudaGetErrorString(e));
