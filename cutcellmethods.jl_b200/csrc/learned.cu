@@ -74,7 +74,7 @@ constexpr int P_B3 = P_W3 + 64;
 constexpr int NPARAM = P_B3 + 1;   // 4801
 static_assert(NPARAM == CC_MLP_NPARAM, "parameter layout");
 
-constexpr long long WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a tile gives up
+constexpr long long WAIT_LIMIT = 1ll << 22;  // default mbarrier polls before a tile gives up
 
 // ---------------------------------------------------------------------------------------------
 // tcgen05 / mbarrier primitives
@@ -128,10 +128,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait on an MMA commit: false if the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
-  for (long long i = 0; i < WAIT_LIMIT; ++i)
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait on an MMA commit: false after `limit` polls or about one second.
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, long long limit) {
+  const unsigned long long t0 = limit > 0 ? global_ns() : 0;
+  for (long long i = 0; i < limit; ++i) {
     if (mbar_try_wait(m, parity)) return true;
+    if ((i & 255) == 255 && global_ns() - t0 > 1000000000ull) return false;
+  }
   return false;
 }
 // 16 consecutive FP32 accumulator columns of this thread's TMEM lane, waited for before use.
@@ -232,11 +240,13 @@ struct MlpShared {
   float* red;  // training only
   uint64_t* mbar;
   uint32_t* tmem;
+  long long limit;  // mbarrier polls before an MMA wait gives up (cc_set_wait_limit)
 };
 
-__device__ __forceinline__ MlpShared mlp_shared(unsigned char* smem, bool train) {
+__device__ __forceinline__ MlpShared mlp_shared(unsigned char* smem, bool train, long long limit) {
   MlpShared s;
   s.base = smem;
+  s.limit = limit;
   const int par = train ? MlpLayout::TRAIN_PAR : MlpLayout::INFER_BYTES;
   s.par = reinterpret_cast<float*>(smem + par);
   s.red = s.par + MlpLayout::PAR_FLOATS;
@@ -271,10 +281,17 @@ __device__ void stage_weights(const float* __restrict__ P, const MlpShared& s, b
 
 // Wait for the MMAs committed to the CTA's mbarrier; false on every thread if any thread's wait
 // ran out.
+// Before the caller gives up (and frees the TMEM the MMAs write), thread 0 waits once more, with
+// the default limit, for the MMAs already committed, so none is still in flight when the CTA
+// releases its TMEM.
 __device__ __forceinline__ bool mma_done(const MlpShared& s, uint32_t& phase) {
-  const bool ok = mbar_wait(s.mbar, phase);
+  const bool ok = mbar_wait(s.mbar, phase, s.limit);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) mbar_wait(s.mbar, phase, WAIT_LIMIT);
+    __syncthreads();
+    return false;
+  }
   phase ^= 1u;
-  if (__syncthreads_or(!ok)) return false;
   tc_fence_after();
   return true;
 }
@@ -429,9 +446,9 @@ __global__ void __launch_bounds__(TILE, 1)
     mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ feats, const float* __restrict__ labels,
                      const float* __restrict__ plain, const float* __restrict__ weights, long long n,
                      unsigned long long seed, int step, int augment, float inv_batch, float* __restrict__ grad,
-                     float* __restrict__ loss, int* __restrict__ err) {
+                     float* __restrict__ loss, int* __restrict__ err, long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const MlpShared s = mlp_shared(smem, true);
+  const MlpShared s = mlp_shared(smem, true, wait_limit);
   const int t = threadIdx.x, warp = t / 32, lane = t & 31;
   unsigned char* b = s.base;
   stage_weights(P, s, true);
@@ -597,9 +614,9 @@ __global__ void mlp_adam_kernel(float* __restrict__ P, float* __restrict__ m, fl
 // `correction` the correction s CORR (2p - 1) of the homogenized features.
 __global__ void __launch_bounds__(TILE)
     mlp_predict_kernel(const float* __restrict__ P, const float* __restrict__ feats, long long n, int correction,
-                       float* __restrict__ out, int* __restrict__ err) {
+                       float* __restrict__ out, int* __restrict__ err, long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const MlpShared s = mlp_shared(smem, false);
+  const MlpShared s = mlp_shared(smem, false, wait_limit);
   const int t = threadIdx.x;
   stage_weights(P, s, false);
   if (t == 0) mbar_init(s.mbar, 1);
@@ -652,12 +669,13 @@ struct LearnedArgs {
   float bound;
   unsigned long long* fallback;
   int* err;
+  long long wait_limit;
 };
 
 template <class T>
 __global__ void __launch_bounds__(TILE) mc_cut_learned_kernel(const LearnedArgs<T> A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const MlpShared s = mlp_shared(smem, false);
+  const MlpShared s = mlp_shared(smem, false, A.wait_limit);
   const int t = threadIdx.x;
   stage_weights(A.P, s, false);
   if (t == 0) mbar_init(s.mbar, 1);
@@ -728,8 +746,12 @@ __global__ void __launch_bounds__(TILE) mc_cut_learned_kernel(const LearnedArgs<
 
 // ---------------------------------------------------------------------------------------------
 // Training samples: for each listed cut cell, its features (8 corner phi / h), its plain volume
-// fraction, its linear index and the label -- the fluid fraction marching cubes gives it at 8x sub-refinement, the
-// body resampled at the 9^3 sub-nodes (Float64, on the global refined lattice x0 + m d/8).
+// fraction, its linear index and the label -- the fluid fraction marching cubes gives it at 8x
+// sub-refinement: update_cache! on the one-cell grid CartesianGrid(get_node(g, cell), (8,8,8), d/8)
+// (the idiom of test/test_mc_moments.jl:67-69,91-98), in Float64, its 512 fractions averaged. A
+// sub-node is get_node of that grid, (x0 + T(i) d) + T(a) d/8. The sum runs in a fixed order:
+// each thread's four sub-cells t, t+128, t+256, t+384, then a butterfly within each warp, then
+// (w0 + w1) + (w2 + w3).
 constexpr int LBL_NT = 128;
 constexpr int LBL_SUB_BYTES = ((729 * 8 + 15) / 16) * 16;  // staged columns then start 16-byte aligned
 __global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, const DevTape tape, const float* __restrict__ phi,
@@ -759,10 +781,13 @@ __global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, 
   for (long long q = blockIdx.x; q < n; q += gridDim.x) {
     const long long ci = list[q];
     const long long i = ci % n0, j = (ci / n0) % n1, k = ci / (n0 * n1);
+    // the one-cell grid's origin: the cell's first node
+    const double cx0[3] = {node_coord(g.x0[0], g.d[0], i), node_coord(g.x0[1], g.d[1], j),
+                           node_coord(g.x0[2], g.d[2], k)};
     for (int v = threadIdx.x; v < 729; v += LBL_NT) {
       const int a = v % 9, b = (v / 9) % 9, c = v / 81;
-      const double xyz[3] = {node_coord(g.x0[0], sd[0], 8 * i + a), node_coord(g.x0[1], sd[1], 8 * j + b),
-                             node_coord(g.x0[2], sd[2], 8 * k + c)};
+      const double xyz[3] = {node_coord(cx0[0], sd[0], a), node_coord(cx0[1], sd[1], b),
+                             node_coord(cx0[2], sd[2], c)};
       sub[v] = tape_eval<double, 3, double>(t, xyz);
     }
     __syncthreads();
@@ -777,11 +802,10 @@ __global__ void __launch_bounds__(LBL_NT) label_kernel(const DevGrid<double> g, 
       for (int e = 0; e < 8; ++e) nout += nudge(ph[e]) >= 0.0 ? 1 : 0;
       if (nout == 8) acc += 1.0;
       else if (nout > 0) {
-        const double org[3] = {node_coord(g.x0[0], sd[0], 8 * i + a), node_coord(g.x0[1], sd[1], 8 * j + b),
-                               node_coord(g.x0[2], sd[2], 8 * k + c)};
-        const double l[3] = {node_coord(g.x0[0], sd[0], 8 * i + a + 1) - org[0],
-                             node_coord(g.x0[1], sd[1], 8 * j + b + 1) - org[1],
-                             node_coord(g.x0[2], sd[2], 8 * k + c + 1) - org[2]};
+        const double org[3] = {node_coord(cx0[0], sd[0], a), node_coord(cx0[1], sd[1], b),
+                               node_coord(cx0[2], sd[2], c)};
+        const double l[3] = {node_coord(cx0[0], sd[0], a + 1) - org[0], node_coord(cx0[1], sd[1], b + 1) - org[1],
+                             node_coord(cx0[2], sd[2], c + 1) - org[2]};
         mc_cut_cell<double>(ph, l, org, sd, tb, st, threadIdx.x);
         acc += st.vf[threadIdx.x];
       }
@@ -816,7 +840,7 @@ template <class T>
 cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
                                   const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
                                   unsigned long long* fallback, int* err, cudaStream_t s) {
-  LearnedArgs<T> a{g, phi, cols, tb, cut_list, cut_count, P, bound, fallback, err};
+  LearnedArgs<T> a{g, phi, cols, tb, cut_list, cut_count, P, bound, fallback, err, wait_limit()};
   const int sm = MlpLayout::INFER_SMEM;
   cudaError_t e = cudaFuncSetAttribute(mc_cut_learned_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
@@ -839,7 +863,7 @@ cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* la
   cudaError_t e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   mlp_train_kernel<<<tiles, TILE, sm, s>>>(P, feats, labels, plain, weights, n, seed, step, augment ? 1 : 0,
-                                           1.0f / float(tiles * TILE), grad, loss, err);
+                                           1.0f / float(tiles * TILE), grad, loss, err, wait_limit());
   return cudaGetLastError();
 }
 
@@ -856,7 +880,7 @@ cudaError_t launch_mlp_predict(const float* P, const float* feats, long long n, 
   if (e != cudaSuccess) return e;
   long long tiles = (n + TILE - 1) / TILE;
   const int grid = (int)(tiles < 148 * 3 ? (tiles < 1 ? 1 : tiles) : 148 * 3);
-  mlp_predict_kernel<<<grid, TILE, sm, s>>>(P, feats, n, correction ? 1 : 0, out, err);
+  mlp_predict_kernel<<<grid, TILE, sm, s>>>(P, feats, n, correction ? 1 : 0, out, err, wait_limit());
   return cudaGetLastError();
 }
 

@@ -1501,6 +1501,56 @@ int oc_mc_cells_from_phi(int prec, const cc_grid* g, const uint8_t* table, const
   return 0;
 }
 
+// The learned correction's label of cut cell `ci` of the 3D grid g: the fluid volume fraction of
+// update_cache! on the one-cell grid CartesianGrid(get_node(g, ci), (8,8,8), g.d/8) in Float64 (the
+// idiom of test/test_mc_moments.jl:67-69,91-98), its 512 fractions summed in the order the device
+// sums them: four sub-cells per thread (t, t+128, t+256, t+384), a butterfly over each warp's 32
+// threads, then (w0 + w1) + (w2 + w3); divided by 512.
+int oc_mc_labels(const cc_grid* g, const cc_optape* t, const uint8_t* table, const int64_t* cells, int64_t n,
+                 double* out) {
+  if (g->dim != 3) return CC_BAD_ARG;
+  oc::McTable tb;
+  if (!tb.parse(table)) return CC_BAD_TABLE;
+  const oc::Tape<double> tp = oc::make_tape<double>(t);
+  for (int64_t q = 0; q < n; ++q) {
+    const int64_t ci = cells[q];
+    const int64_t idx[3] = {ci % g->n[0], (ci / g->n[0]) % g->n[1], ci / (g->n[0] * g->n[1])};
+    cc_grid sub{};
+    sub.dim = 3;
+    for (int a = 0; a < 3; ++a) {
+      sub.x0[a] = oc::node_coord(g->x0[a], g->d[a], idx[a]);
+      sub.d[a] = g->d[a] / 8.0;
+      sub.n[a] = 8;
+    }
+    std::vector<double> phi(729);
+    oc::sample_nodes_range<double, 3>(sub, tp, phi.data(), 0, 8);
+    std::vector<int8_t> kind(512);
+    std::vector<uint8_t> amb(512);
+    std::vector<double> vf(512), c(512 * 3), ff(512 * 6), fcl(512 * 12), ic(512 * 3);
+    const cc_cells cols{kind.data(), amb.data(), vf.data(), c.data(), ff.data(), fcl.data(), ic.data()};
+    oc::mc_cells_range<double>(sub, tb, phi.data(), cols, 0, 8);
+    double lane[128];
+    for (int th = 0; th < 128; ++th) {
+      double acc = 0.0;
+      for (int r = 0; r < 4; ++r) acc = acc + vf[th + 128 * r];
+      lane[th] = acc;
+    }
+    double red[4];
+    for (int w = 0; w < 4; ++w) {
+      double b[32];
+      for (int l = 0; l < 32; ++l) b[l] = lane[32 * w + l];
+      for (int o = 16; o > 0; o >>= 1) {
+        double nb[32];
+        for (int l = 0; l < 32; ++l) nb[l] = b[l] + b[l ^ o];
+        for (int l = 0; l < 32; ++l) b[l] = nb[l];
+      }
+      red[w] = b[0];
+    }
+    out[q] = ((red[0] + red[1]) + (red[2] + red[3])) / 512.0;
+  }
+  return 0;
+}
+
 // Marching cubes over the cell layers k0..k1-1 of the full grid g: phi receives the node layers
 // k0..k1 and the columns the slab's cells, each computed with its global indices.
 int oc_mc_update_slab(int prec, const cc_grid* g, const cc_optape* t, const uint8_t* table, int64_t k0,

@@ -65,6 +65,7 @@ def lib():
                                         C.c_void_p, C.c_void_p]
         L.oc_plic_update_slab.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_mc_labels.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
         L.oc_mc_mesh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
@@ -221,6 +222,18 @@ def mc_update_slab(g, tape, table: bytes, prec, k0, k1):
                                  _ptr(phi), C.byref(cells_struct(cols)))
     assert rc == 0, rc
     return phi, cols
+
+
+def mc_labels(g, tape, table: bytes, cells):
+    """The learned correction's labels (Float64) of the listed cells of the 3D grid g: each cell's
+    fluid fraction by marching cubes on its own one-cell grid at 8x sub-refinement."""
+    cells = np.ascontiguousarray(cells, np.int64)
+    out = np.zeros(len(cells), np.float64)
+    t, keep = tape_struct(tape)
+    tb = np.frombuffer(table, np.uint8).copy()
+    rc = lib().oc_mc_labels(C.byref(grid_struct(g)), C.byref(t), _ptr(tb), _ptr(cells), len(cells), _ptr(out))
+    assert rc == 0, rc
+    return out
 
 
 def plic_update_slab(g, tape, prec, k0, k1):

@@ -185,6 +185,33 @@ def test_samples_and_learned_update_invariants():
     assert nfb == int((~ok).sum())
 
 
+@pytest.mark.parametrize("n,seed", [(48, 11), (96, 12)])
+def test_label_kernel_matches_oracle_one_cell_grids(n, seed):
+    """Every label the device gives a cut cell is the oracle's: marching cubes in Float64 on that
+    cell's own one-cell grid at 8x sub-refinement, CartesianGrid(get_node(g, cell), (8,8,8), d/8)
+    (the idiom of test/test_mc_moments.jl:67-69,91-98), the 512 fractions summed in the device's
+    order and averaged. Bitwise: the Float64 sums agree exactly, so their Float32 roundings do."""
+    g = cc.workloads.unit_grid(n)
+    body = cc.workloads.smooth_blob(seed)
+    cache = cc.update_cache(cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32), body, g)
+    feats, labels, plain, index = L.make_samples(cache, body, g, with_index=True)
+    idx = index.cpu().numpy()
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(len(idx), size=min(400, len(idx)), replace=False)
+    ref = po.mc_labels(g, cc.flatten(body, 3), cc.mc_tables.project_table(), idx[pick])
+    got = labels.cpu().numpy()[pick]
+    assert np.array_equal(bits(got), bits(ref.astype(np.float32))), \
+        f"{int(np.sum(got != ref.astype(np.float32)))} of {len(pick)} labels differ"
+    # the features are the cell's Float32 corner values over h, in MC_NODE_BITS order
+    ph = cache.phi.cpu().numpy()
+    nx = n + 1
+    i, j, k = idx[pick] % n, (idx[pick] // n) % n, idx[pick] // (n * n)
+    b0 = i + nx * (j + nx * k)
+    offs = [0, 1, nx + 1, nx, nx * nx, nx * nx + 1, nx * nx + nx + 1, nx * nx + nx]
+    want = np.stack([ph[b0 + o] for o in offs], axis=1) * np.float32(1.0 / np.float32(g.d[0]))
+    assert np.array_equal(bits(feats.cpu().numpy()[pick]), bits(want.astype(np.float32)))
+
+
 def test_training_from_scratch_gains_over_plain_marching_cubes():
     # a small training set (24 bodies on 64^3 .. 160^3), a short schedule, an unseen body at 256^3
     data = L.training_set(range(1000, 1024), [64, 96, 128, 160])
