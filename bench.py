@@ -286,6 +286,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.empty_cache()
     precision["degenerate_deciders"] = degenerate_decider_errors(cc, dev)
 
+    sizes = sizes_block(args, dev, cc)
     learned = None if args.no_learned else learned_block(args, dev, cc)
     batched = None if args.no_batch else batch_block(args, dev, cc, k=args.batch_updates)
     mesh = mesh_block(args, dev, cc)
@@ -316,6 +317,7 @@ def run_ours(args, rank, world, dist):
             "mixed": {"value": job_rate(world, n ** 3, msm * 1e-3), "ms_per_step": msm,
                       "roofline_frac": bytes_per / (statistics.mean(perm) * 1e-3) / 1e9 / peak},
             "precision": precision,
+            "sizes": sizes,
             "learned": learned,
             "batch": batched,
             "mesh": mesh,
@@ -445,6 +447,39 @@ def degenerate_decider_errors(cc, dev, n=128, seed=7):
     for name in ("float32", "mixed"):
         e = field_errors(caches[name], caches["f64"])
         out[name] = {k: e[k] for k in ("volume_fraction", "face_fraction", "kind_mismatch", "ambiguous_mismatch")}
+    return out
+
+
+def sizes_block(args, dev, cc, sizes=(256, 200, 500)):
+    """The Float32 update of the same CSG body at other sizes: 256^3 (a configuration of its own) and
+    two grids whose x extent is not a multiple of 16 cells (200^3, the reference README's example
+    size, and 500^3), whose kind/ambiguous rows TMA cannot address. CUDA events, the roofline
+    fraction of each against the measured copy bandwidth."""
+    import torch
+    peak = measured_peak()[0]
+    out = {}
+    for m in sizes:
+        g = cc.workloads.csg_grid(m)
+        tape = cc.flatten(cc.workloads.csg_body(0), 3)
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32, device=dev)
+        s = torch.cuda.current_stream(dev)
+        for _ in range(max(args.warmup, 3)):
+            cc.update_cache(cache, tape, g, sync=False)
+        torch.cuda.synchronize(dev)
+        reps = max(args.steps, 10)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            cc.update_cache(cache, tape, g, sync=False)
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        ms = a.elapsed_time(b) / reps
+        byts = cc.workloads.mc_bytes_per_update(m, 4)
+        out[f"{m}^3"] = {"ms": ms, "cells_per_s": m ** 3 / (ms * 1e-3), "algorithmic_bytes": byts,
+                         "roofline_frac": byts / (ms * 1e-3) / 1e9 / peak,
+                         "x_multiple_of_16": m % 16 == 0}
+        del cache
+        torch.cuda.empty_cache()
     return out
 
 
@@ -710,13 +745,35 @@ def learned_block(args, dev, cc):
 
 
 def run_only(args):
-    """One block alone: the marching-cubes mesh of the Float32 CSG cache or the PLIC surface of the
-    Float32 64-sphere cache at --n, or the batched marching-squares workloads (--batch-updates)."""
+    """One block alone: the marching-cubes update of the CSG body at --n and --prec, the
+    marching-cubes mesh of the Float32 CSG cache or the PLIC surface of the Float32 64-sphere cache
+    at --n, or the batched marching-squares workloads (--batch-updates)."""
     import torch
     from __graft_entry__ import load_package
     cc = load_package()
     dev = torch.device("cuda", 0)
-    if args.only == "mesh":
+    if args.only == "update":
+        # the marching-cubes update alone (CSG body, --n, --prec), --warmup then --steps launches
+        # of the fill and cut-band kernels: the bounded command to profile
+        dtype = torch.float32 if args.prec == "f32" else torch.float64
+        g = cc.workloads.csg_grid(args.n)
+        tape = cc.flatten(cc.workloads.csg_body(0), 3)
+        cache = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=dtype, device=dev)
+        s = torch.cuda.current_stream(dev)
+        for _ in range(args.warmup):
+            cc.update_cache(cache, tape, g, sync=False)
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(args.steps):
+            cc.update_cache(cache, tape, g, sync=False)
+        b.record(s)
+        torch.cuda.synchronize(dev)
+        ms = a.elapsed_time(b) / max(args.steps, 1)
+        byts = cc.workloads.mc_bytes_per_update(args.n, 4 if args.prec == "f32" else 8)
+        out = {"grid": f"{args.n}^3 CSG body, {args.prec}", "ms": ms, "cells_per_s": args.n ** 3 / (ms * 1e-3),
+               "roofline_frac": byts / (ms * 1e-3) / 1e9 / measured_peak()[0]}
+    elif args.only == "mesh":
         args.no_cpu = True
         out = mesh_block(args, dev, cc)
     elif args.only == "batch":
@@ -742,7 +799,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-plic", action="store_true")
     ap.add_argument("--batch-updates", type=int, default=256, help="updates in the batched marching-squares block")
-    ap.add_argument("--only", choices=["mesh", "plic-surface", "batch"],
+    ap.add_argument("--only", choices=["update", "mesh", "plic-surface", "batch"],
                     help="run one block alone at --n and print its JSON (for profiling)")
     args = ap.parse_args()
     if args.only:
