@@ -398,29 +398,46 @@ def cells_differ(a, b, chunk=1 << 23):
     return out
 
 
+def near_zero_cells(c):
+    """Per cell: does a corner of cache ``c``'s phi lie within eps(T) of zero, where nudge_zeros
+    replaces it by eps(T) (src/marching_cubes/marching_cubes.jl:240-243)."""
+    import torch
+    import torch.nn.functional as F
+    nn = [x + 1 for x in c.n]
+    near = (c.phi.abs() < torch.finfo(c.phi.dtype).eps).reshape(1, 1, nn[2], nn[1], nn[0]).float()
+    return (F.max_pool3d(near, 2, stride=1) > 0).reshape(-1)
+
+
 def precision_report(cc, g, c32, c64, cm, dev):
     """Every column's error of the Float32 and mixed updates against Float64, split into its
     sources. ``c64_on_32`` is the Float64 cell construction run on the Float32 update's phi: against
     the Float64 update it isolates the error of sampling phi in Float32 (corner signs and the
-    deciders' inputs move); against it, the Float32 and mixed updates show their arithmetic alone.
-    Float32 differs from mixed only where a Float32 decider (or a tiny edge root) decides otherwise
-    than Float64 on the same values: those cells are counted, and the Float32 arithmetic-only
-    statistics leave them out."""
+    deciders' inputs move). On the same phi, two things still differ before any arithmetic:
+    nudge_zeros lifts a corner within eps(Float32) of zero to eps(Float32) in Float32 but leaves it
+    in Float64 (near-zero cells), and a Float32 decider can decide otherwise than Float64 (the cells
+    where Float32 and mixed differ, mixed's deciders being Float64). The arithmetic-only
+    statistics leave both out."""
     import torch
     c64on32 = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float64, device=dev)
     cc.update_cache(c64on32, cc.NodalField(c32.phi.double()), g)
     flips = cells_differ(c32, cm)
+    near = near_zero_cells(c32)
     out = {"reference": "the Float64 update of the same body and grid",
            "float32": field_errors(c32, c64), "mixed": field_errors(cm, c64),
            "input_rounding": {"what": "Float64 cells from the Float32 phi, against the Float64 update",
                               **field_errors(c64on32, c64)},
            "float32_decider_flip_cells": int(flips.sum().item()),
-           "float32_arithmetic": {"what": "Float32 against Float64 cells on the same Float32 phi, cells where "
-                                          "Float32 and mixed agree (same decisions)",
-                                  **field_errors(c32, c64on32, keep=~flips)},
-           "mixed_arithmetic": {"what": "mixed against Float64 cells on the same Float32 phi",
-                                **field_errors(cm, c64on32)}}
-    del c64on32, flips
+           "near_zero_corner_cells": int(near.sum().item()),
+           "near_zero": {"what": "Float32 against Float64 cells on the same Float32 phi, cells with a corner "
+                                 "within eps(Float32) of zero (nudged in Float32 only)",
+                         **field_errors(c32, c64on32, keep=near)},
+           "float32_arithmetic": {"what": "Float32 against Float64 cells on the same Float32 phi, cells with the "
+                                          "same decisions as mixed and no corner within eps(Float32) of zero",
+                                  **field_errors(c32, c64on32, keep=~flips & ~near)},
+           "mixed_arithmetic": {"what": "mixed against Float64 cells on the same Float32 phi, no corner within "
+                                        "eps(Float32) of zero",
+                                **field_errors(cm, c64on32, keep=~near)}}
+    del c64on32, flips, near
     torch.cuda.empty_cache()
     return out
 
