@@ -133,12 +133,16 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait on an MMA commit: false after `limit` polls or about one second.
+// Bounded wait on an MMA commit: false after `limit` polls or about one second (the clock starts
+// after 256 polls).
 __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, long long limit) {
-  const unsigned long long t0 = limit > 0 ? global_ns() : 0;
+  unsigned long long t0 = 0;
   for (long long i = 0; i < limit; ++i) {
     if (mbar_try_wait(m, parity)) return true;
-    if ((i & 255) == 255 && global_ns() - t0 > 1000000000ull) return false;
+    if ((i & 255) == 255) {
+      if (t0 == 0) t0 = global_ns();
+      else if (global_ns() - t0 > 1000000000ull) return false;
+    }
   }
   return false;
 }

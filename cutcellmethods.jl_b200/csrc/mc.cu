@@ -111,10 +111,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// At most `limit` polls and about one second; a thread that has given up once passes limit 0 from
-// then on, so a wait that cannot complete costs the kernel that second once, not once per slice.
+// At most `limit` polls and about one second (the clock starts after 256 polls, so a wait that
+// succeeds at once reads no timer); a thread that has given up once passes limit 0 from then on, so
+// a wait that cannot complete costs the kernel that second once, not once per slice.
 __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, long long limit) {
-  const unsigned long long t0 = limit > 0 ? global_ns() : 0;
+  unsigned long long t0 = 0;
   for (long long i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
@@ -124,7 +125,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, long lon
         : "r"(smem_addr(m)), "r"(parity)
         : "memory");
     if (ok) return true;
-    if ((i & 255) == 255 && global_ns() - t0 > 1000000000ull) return false;
+    if ((i & 255) == 255) {
+      if (t0 == 0) t0 = global_ns();
+      else if (global_ns() - t0 > 1000000000ull) return false;
+    }
   }
   return false;
 }

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, co
 constexpr int FZ_X = 32, FZ_Y = 8, FZ_KZ = 32;
 
 template <class T, bool MX>
-__global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 3 : (MX ? 4 : 5)) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
                                                             const T* __restrict__ normals,
                                                             const T* __restrict__ intercepts,
                                                             const uint8_t* __restrict__ valid) {
@@ -359,24 +359,54 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
     const int c = f >> 1;
     return (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
   };
-  auto frac_at = [&](long long ci, int f) {  // the one-sided fraction of cell ci's face f
-    return frac_of(face_area<T, 3, MX>(normals + 3 * ci, intercepts[ci], vf[ci], valid[ci] != 0, cs, f), full_of(f));
+  // One cell's stored plane, loaded a slice before its fractions are formed, so the loads' latency
+  // hides behind the slice in between instead of sitting in front of the slice barrier.
+  struct Plane {
+    T n[3], a, fr;
+    bool ok;
   };
-  auto own6 = [&](T (*buf)[NF][X], long long k) {  // this thread's cell of slice k: six one-sided fractions
+  auto load_plane = [&](long long ci) {
+    Plane p;
+    p.n[0] = normals[3 * ci]; p.n[1] = normals[3 * ci + 1]; p.n[2] = normals[3 * ci + 2];
+    p.a = intercepts[ci];
+    p.fr = vf[ci];
+    p.ok = valid[ci] != 0;
+    return p;
+  };
+  // a plane's one-sided fraction of face f; a plane that misses its cell gives every face 0 or 1
+  // without the clip (every area is then exactly 0 or the full face)
+  auto frac_from = [&](const Plane& p, int side, int f) {
+    if (side != 0) return side > 0 ? T(1) : T(0);
+    return frac_of(face_area<T, 3, MX>(p.n, p.a, p.fr, p.ok, cs, f), full_of(f));
+  };
+  auto side_of = [&](const Plane& p) { return p.ok ? plane_side<T>(p.n, p.a) : 0; };
+  auto own6 = [&](T (*buf)[NF][X], const Plane& p) {  // this thread's cell: six one-sided fractions
     if (!inxy) return;
-    const long long ci = ix + n[0] * (jy + n[1] * k);
-    const T nrm[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
-    const T a = intercepts[ci], fr = vf[ci];
-    const bool ok = valid[ci] != 0;
-    const int side = ok ? plane_side<T>(nrm, a) : 0;
-    if (side != 0) {  // a plane that misses the cell: every area 0 or the full face, so 0 or 1
+    const int side = side_of(p);
 #pragma unroll
-      for (int f = 0; f < NF; ++f) buf[ly][f][lx] = side > 0 ? T(1) : T(0);
-      return;
-    }
-#pragma unroll
-    for (int f = 0; f < NF; ++f) buf[ly][f][lx] = frac_of(face_area<T, 3, MX>(nrm, a, fr, ok, cs, f), full_of(f));
+    for (int f = 0; f < NF; ++f) buf[ly][f][lx] = frac_from(p, side, f);
   };
+  // The x and y halo of a slice: 2Y + 2X faces, one on every third thread (all eight warps share
+  // them). Item h: the cell beyond the tile's -x / +x edge at row h (h < 2Y), or beyond its -y / +y
+  // edge at column h - 2Y; the face it shows the tile.
+  constexpr int NH = 2 * Y + 2 * X;
+  static_assert(3 * (NH - 1) < NT, "one halo face per third thread");
+  const int hitem = (q % 3 == 0) ? q / 3 : NH;
+  long long hcell = -1;
+  int hface = 0;
+  if (hitem < 2 * Y) {
+    const int side = hitem / Y, y = hitem % Y;
+    const long long ii = side == 0 ? i0 - 1 : i0 + X, jj = j0 + y;
+    if (ii >= 0 && ii < n[0] && jj < n[1]) hcell = ii + n[0] * jj;
+    hface = side == 0 ? 1 : 0;
+  } else if (hitem < NH) {
+    const int side = (hitem - 2 * Y) / X, x = (hitem - 2 * Y) % X;
+    const long long ii = i0 + x, jj = side == 0 ? j0 - 1 : j0 + Y;
+    if (jj >= 0 && jj < n[1] && ii < n[0]) hcell = ii + n[0] * jj;
+    hface = side == 0 ? 3 : 2;
+  }
+  const long long nxy = n[0] * n[1];
+  const long long cxy = ix + n[0] * jy;
   // One barrier per slice. Slice k's fractions live in bufs[(k - k0) % 3]: the next slice's are
   // written (own slots) while this one's are read, and the buffer they overwrite was last read in
   // slice k - 2, whose readers all passed the previous barrier. The halo alternates by slice
@@ -384,8 +414,14 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
   // becomes slice k + 2's), takes each warp's resolved row in the warp's own block: only that
   // warp writes or reads its block until it fills it with slice k + 2's fractions itself, and it
   // copies the row out in between.
-  own6(bufs[0], k0);
-  if (inxy && k0 >= 1) prev5[q] = frac_at(ix + n[0] * (jy + n[1] * (k0 - 1)), 5);
+  Plane pnext{}, hnext{};
+  if (inxy) own6(bufs[0], load_plane(cxy + nxy * k0));
+  if (inxy && k0 >= 1) {
+    const Plane pb = load_plane(cxy + nxy * (k0 - 1));
+    prev5[q] = frac_from(pb, side_of(pb), 5);
+  }
+  if (inxy && k0 + 1 < n[2]) pnext = load_plane(cxy + nxy * (k0 + 1));
+  if (hcell >= 0) hnext = load_plane(hcell + nxy * k0);
   const int lane = q & 31, wrow = q >> 5;
   static_assert(X == 32, "a warp is one row of the slice");
   for (long long k = k0; k < k1; ++k) {
@@ -395,17 +431,15 @@ __global__ void __launch_bounds__(NT, 5) plic_face_z_kernel(const DevGrid<T> g, 
     T* const res = &bufs[r3 == 0 ? 2 : r3 - 1][wrow][0][0];  // this warp's row, cell-major
     T (*hxp)[Y] = hx[par];
     T (*hyp)[X] = hy[par];
-    if (k + 1 < n[2]) own6(nxt, k + 1);
-    for (int h = q; h < 2 * Y + 2 * X; h += NT) {
-      if (h < 2 * Y) {
-        const int side = h / Y, y = h % Y;
-        const long long ii = side == 0 ? i0 - 1 : i0 + X, jj = j0 + y;
-        if (ii >= 0 && ii < n[0] && jj < n[1]) hxp[side][y] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 1 : 0);
-      } else {
-        const int side = (h - 2 * Y) / X, x = (h - 2 * Y) % X;
-        const long long ii = i0 + x, jj = side == 0 ? j0 - 1 : j0 + Y;
-        if (jj >= 0 && jj < n[1] && ii < n[0]) hyp[side][x] = frac_at(ii + n[0] * (jj + n[1] * k), side == 0 ? 3 : 2);
-      }
+    const Plane pcur = pnext, hcur = hnext;
+    // the planes the next slice needs, loaded now
+    if (inxy && k + 2 < n[2]) pnext = load_plane(cxy + nxy * (k + 2));
+    if (hcell >= 0 && k + 1 < k1) hnext = load_plane(hcell + nxy * (k + 1));
+    if (k + 1 < n[2]) own6(nxt, pcur);
+    if (hcell >= 0) {
+      const T v = frac_from(hcur, side_of(hcur), hface);
+      if (hitem < 2 * Y) hxp[hitem / Y][hitem % Y] = v;
+      else hyp[(hitem - 2 * Y) / X][(hitem - 2 * Y) % X] = v;
     }
     __syncthreads();
     if (inxy) {
