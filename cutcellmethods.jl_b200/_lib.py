@@ -47,7 +47,6 @@ EXPORTS = {
     "cc_handle_create": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
     "cc_handle_destroy": [C.c_void_p],
     "cc_handle_set_mc_table": [C.c_void_p, C.c_void_p, C.c_size_t],
-    "cc_handle_status": [C.c_void_p],
     "cc_set_wait_limit": [C.c_int64],
     "cc_mc_update": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "cc_mc_cells_from_phi": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],

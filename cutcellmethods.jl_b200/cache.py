@@ -316,8 +316,6 @@ def update_cache(cache, geo, domain, stream=None, sync=True):
                 _check(fn(cache.handle.h, C.byref(gs), C.byref(tp.s), _ptr(cache.phi), C.byref(cells), s))
     if sync:
         torch.cuda.current_stream(dev).synchronize() if stream is None else torch.cuda.synchronize(dev)
-        # a kernel that gave up a bounded wait left its flag on the handle (host memory: no device call)
-        _check(L.cc_handle_status(cache.handle.h))
     return cache
 
 

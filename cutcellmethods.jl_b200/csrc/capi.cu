@@ -319,17 +319,6 @@ extern "C" {
 const char* cc_version(void) { return "cutcell_b200 0.1.0 (sm_100a)"; }
 const char* cc_last_error(void) { return g_last_error.c_str(); }
 
-cc_status cc_handle_status(cc_handle* h) {
-  if (!h) return fail(CC_BAD_ARG, "null handle");
-  if (h->status_host && *reinterpret_cast<volatile unsigned*>(h->status_host)) {
-    *reinterpret_cast<volatile unsigned*>(h->status_host) = 0;
-    return fail(CC_DEVICE_TIMEOUT,
-                "a marching-cubes fill CTA gave up waiting on its staging mbarriers; that update's columns are "
-                "not valid");
-  }
-  return CC_OK;
-}
-
 int64_t cc_set_wait_limit(int64_t polls) { return cci::set_wait_limit(polls); }
 
 cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t prec, const int64_t n[3],
@@ -360,11 +349,7 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->tape_copied, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&h->vol_scratch, (2 * cci::calc_volume_blocks() + 2) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->rep_scratch, 8 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaHostAlloc(&h->status_host, sizeof(unsigned), cudaHostAllocMapped);
-  if (e == cudaSuccess) {
-    *h->status_host = 0;
-    e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->status_dev), h->status_host, 0);
-  }
+
   if (e == cudaSuccess && method == CC_MARCHING_CUBES) {
     const int64_t ncell = h->n[0] * h->n[1] * h->n[2];
     e = cudaMalloc(&h->cut_list, size_t(ncell) * sizeof(unsigned));
@@ -387,7 +372,6 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->table_dev) cudaFree(h->table_dev);
   if (h->vol_scratch) cudaFree(h->vol_scratch);
   if (h->rep_scratch) cudaFree(h->rep_scratch);
-  if (h->status_host) cudaFreeHost(h->status_host);
   if (h->cut_list) cudaFree(h->cut_list);
   if (h->cut_count) cudaFree(h->cut_count);
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
@@ -436,15 +420,15 @@ static cc_status mc_common(cc_handle* h, const cc_grid* g, const cc_optape* body
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dev_grid<double>(g), tape, static_cast<const double*>(phi_in),
-                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count,
-                               h->status_dev, s, true, false, ps, ps ? pb : 0);
+                               static_cast<double*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s,
+                               true, false, ps, ps ? pb : 0);
   } else {
     if (body && (st = upload_tape<float>(h, body, 3, s, &tape)) != CC_OK) return st;
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dev_grid<float>(g), tape, static_cast<const float*>(phi_in),
-                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count,
-                              h->status_dev, s, true, h->prec == CC_MIXED, ps, ps ? pb : 0);
+                              static_cast<float*>(phi_out), cols_of(cells), h->tb, h->cut_list, h->cut_count, s, true,
+                              h->prec == CC_MIXED, ps, ps ? pb : 0);
   }
   if (e != cudaSuccess) return cuda_fail(e, "marching cubes launch");
   return CC_OK;

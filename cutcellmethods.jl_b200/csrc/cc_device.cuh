@@ -103,36 +103,12 @@ __device__ __forceinline__ Dual<T, D> operator/(const Dual<T, D>& a, T c) {
 #pragma unroll
   for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / c;
   return r; }
-// Quotients a_i / b of one denominator from one reciprocal (Markstein, "Computation of elementary
-// functions on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990): with
-// y = RN(1/b) and q0 = RN(a y), the residual r = a - b q0 is exact in one FMA and RN(q0 + r y) is
-// RN(a / b), the IEEE quotient, while a, b and the quotient stay far from overflow and underflow
-// (here |a|, |b| in [2^-60, 2^60] or a == 0; elsewhere the division itself). r == 0 means q0 is
-// exact, and keeps a's signed zero.
-__device__ __forceinline__ float rcp_rn(float b) { return __frcp_rn(b); }
-__device__ __forceinline__ double rcp_rn(double b) { return __drcp_rn(b); }
-__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
-template <class T>
-__device__ __forceinline__ bool quotient_in_range(T a, T b) {
-  const T lo = T(8.673617379884035e-19), hi = T(1.152921504606847e18);  // 2^-60, 2^60
-  const T ab = fabs(b), aa = fabs(a);
-  return ab >= lo && ab <= hi && (aa == T(0) || (aa >= lo && aa <= hi));
-}
-template <class T>
-__device__ __forceinline__ T div_by_rcp(T a, T b, T y) {
-  if (!quotient_in_range(a, b)) return a / b;
-  const T q0 = a * y;
-  const T r = fma_rn(-b, q0, a);
-  return r == T(0) ? q0 : fma_rn(r, y, q0);
-}
 template <class T, int D>
 __device__ __forceinline__ Dual<T, D> dsqrt(const Dual<T, D>& a) {
   Dual<T, D> r; r.v = sqrt(a.v);
   const T two_s = T(2) * r.v;
-  const T y = rcp_rn(two_s);
 #pragma unroll
-  for (int i = 0; i < D; ++i) r.g[i] = div_by_rcp(a.g[i], two_s, y);
+  for (int i = 0; i < D; ++i) r.g[i] = a.g[i] / two_s;
   return r; }
 template <class T, int D>
 __device__ __forceinline__ Dual<T, D> dabs(const Dual<T, D>& a) {

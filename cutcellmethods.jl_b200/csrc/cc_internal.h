@@ -56,16 +56,15 @@ struct Cols {
 // Marching cubes: sample (if phi_in == nullptr: sample from the tape into phi_out) and build
 // every cell. Returns the CUDA launch status.
 // `cut_list` (one slot per cell) and `cut_count` are scratch: the fill pass lists the cut band
-// there and the cut pass reads it back. `status` (host-mapped or device memory) is set to 1 by a
-// fill CTA whose bounded mbarrier wait ran out; the launch never clears it.
+// there and the cut pass reads it back.
 // With with_cut false only the fill pass runs (the cut band is listed, not built).
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      unsigned* status, cudaStream_t s, bool with_cut = true, bool mixed = false,
+                      cudaStream_t s, bool with_cut = true, bool mixed = false,
                       void* prune_scratch = nullptr, size_t prune_bytes = 0);
-// The mbarrier poll limit of the fill and learned kernels (cc_set_wait_limit): set returns the old
-// value; a negative argument restores the default.
+// The mbarrier poll limit of the learned kernels (cc_set_wait_limit): set returns the old value; a
+// negative argument restores the default.
 long long set_wait_limit(long long polls);
 long long wait_limit();
 // Scratch launch_mc needs to prune a union-of-spheres tape per fill CTA (n_ops ops per CTA).
@@ -166,8 +165,6 @@ struct cc_handle {
   cci::DevTable tb{};
   unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
   unsigned* cut_count = nullptr;
-  unsigned* status_host = nullptr;  // pinned, mapped: set by a kernel whose bounded wait ran out
-  unsigned* status_dev = nullptr;   // the device's view of status_host
   double* vol_scratch = nullptr;  // calc_volume partials + result
   unsigned long long* rep_scratch = nullptr;  // report counters + min
   unsigned* mesh_vbase = nullptr;  // generate_mesh: first vertex of each node's cut edges

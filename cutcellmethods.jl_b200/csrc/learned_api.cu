@@ -300,7 +300,7 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dg2, tape, nullptr, static_cast<double*>(phi), cols_of(cells), h->tb, h->cut_list,
-                               h->cut_count, h->status_dev, s, false, false, ps, ps ? pb : 0);
+                               h->cut_count, s, false, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<double>(dg2, static_cast<const double*>(phi), cols_of(cells), h->tb, h->cut_list,
                                              h->cut_count, m->P, bound, m->fallback, m->err, s);
@@ -311,7 +311,7 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dg2, tape, nullptr, static_cast<float*>(phi), cols_of(cells), h->tb, h->cut_list,
-                              h->cut_count, h->status_dev, s, false, false, ps, ps ? pb : 0);
+                              h->cut_count, s, false, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<float>(dg2, static_cast<const float*>(phi), cols_of(cells), h->tb, h->cut_list,
                                             h->cut_count, m->P, bound, m->fallback, m->err, s);
@@ -323,10 +323,7 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "cc_mc_update_learned");
     *n_fallback = (int64_t)fb;
-    // both flags are read (and cleared): the network's, then the fill pass's on the handle
-    const cc_status hs = cc_handle_status(h);
-    st = check_err(m, s);
-    return st != CC_OK ? st : hs;
+    return check_err(m, s);
   }
   return CC_OK;
 }

@@ -32,24 +32,19 @@ using cci::DevTable;
 using cci::DevTape;
 
 // Fill-kernel tile: TX cells along x (32 at Float32, 16 at Float64, so a staging buffer is about
-// 26 KB either way) by TY = 8 rows, one compute thread per cell, marching KZ slices along z. A slab
-// of (TX+1) x (TY+1) nodes serves TX x TY cells. A CTA is NT compute threads plus one store warp.
+// 26 KB either way) by TY = 8 rows, one thread per cell, marching KZ slices along z. A slab of
+// (TX+1) x (TY+1) nodes serves TX x TY cells: 1.16 node evaluations per cell at Float32.
 template <class T> struct Tile {
   static constexpr int TX = sizeof(T) == 4 ? 32 : 16;
   static constexpr int TY = 8;
   static constexpr int NT = TX * TY;
   static constexpr int NSX = TX + 1;
   static constexpr int NSLAB = (TX + 1) * (TY + 1);
-  static constexpr int MINB = sizeof(T) == 4 ? 2 : 3;  // resident CTAs per SM the registers are capped for
-  static constexpr int NSTAGE = 2;  // staging buffers between the compute warps and the store warp
-  static constexpr int NLAG = 1;    // tensor-store groups the store warp leaves in flight (< NSTAGE)
+  static constexpr int MINB = sizeof(T) == 4 ? 3 : 3;  // Float64 at 4 spills
 };
-// z slices marched per pencil: KZ + 1 = 32 node slabs, exactly 8 sampling rounds of NS slabs
-constexpr int KZ = 31;
+constexpr int KZ = 31;  // z slices marched per CTA: KZ + 1 = 32 node slabs, 8 sampling rounds of NS
 constexpr int NS = 4;   // node slabs sampled per round (one op-major tape pass per thread)
 constexpr int CUT_NT = 256;  // 512^3 CSG body, Float32 update: 2.73 ms at 128, 2.71-2.72 at 256, 2.75 at 64
-// mbarrier polls before a wait of the fill kernel gives up (the default of cc_set_wait_limit)
-constexpr long long FILL_WAIT_LIMIT = 1ll << 22;
 
 template <class T>
 struct McArgs {
@@ -61,11 +56,9 @@ struct McArgs {
   DevTable tb;
   unsigned* cut_list;
   unsigned* cut_count;
-  int n_itiles, n_jtiles, n_ktiles;
-  int tma_mask;  // bit c: output column c leaves through TMA tensor stores (its map below is valid)
-  int byte_words;  // kind/ambiguous rows start on 4-byte boundaries: the store warp copies them as words
-  unsigned* status;  // set to 1 by a fill CTA whose mbarrier wait ran out
-  long long wait_limit;  // mbarrier polls before a wait gives up
+  int n_itiles, n_jtiles;
+  int tma_mask;  // bit c: column c leaves through TMA tensor stores (its map below is valid)
+  int byte_words;  // kind/ambiguous rows start on 4-byte boundaries
   // a union of spheres: each CTA's kept ops (stride tape.n_ops) and their count, or null
   const cc_op* pruned_ops;
   const int* pruned_count;
@@ -96,48 +89,7 @@ __device__ __forceinline__ void tma_store4(const CUtensorMap* m, const void* ssr
                : "memory");
 }
 
-// mbarriers between the compute warps and the store warp. A wait polls at most `limit` times; a
-// wait that runs out returns false (the caller records it and goes on without the data it waited
-// for: the kernel still ends, and the host reports CC_DEVICE_TIMEOUT).
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* m, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* m) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(m)) : "memory");
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// At most `limit` polls and about one second (the clock starts after 256 polls, so a wait that
-// succeeds at once reads no timer); a thread that has given up once passes limit 0 from then on, so
-// a wait that cannot complete costs the kernel that second once, not once per slice.
-__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, long long limit) {
-  unsigned long long t0 = 0;
-  for (long long i = 0; i < limit; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.acquire.cta.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_addr(m)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((i & 255) == 255) {
-      if (t0 == 0) t0 = global_ns();
-      else if (global_ns() - t0 > 1000000000ull) return false;
-    }
-  }
-  return false;
-}
-// The compute warps' own barrier (named barrier 1; the store warp never joins it).
-template <int N>
-__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory"); }
-
-// Shared-memory byte layout of one fill CTA: NSTAGE staging buffers, the node-slab ring, the
-// full/empty mbarriers of the staging buffers, the tape.
+// Shared-memory byte layout of one fill CTA: two staging buffers, two node slabs, the tape.
 template <class T>
 struct Layout {
   using TL = Tile<T>;
@@ -151,14 +103,12 @@ struct Layout {
   static constexpr int ic = fcl + 12 * NC * int(sizeof(T));
   static constexpr int stage_bytes = ((ic + 3 * NC * int(sizeof(T)) + 127) / 128) * 128;
   static constexpr int slab_bytes = ((TL::NSLAB * int(sizeof(T)) + 15) / 16) * 16;
-  static constexpr int slab0 = TL::NSTAGE * stage_bytes;
-  static constexpr int bars = slab0 + (NS + 1) * slab_bytes;  // full[NSTAGE], empty[NSTAGE]
-  static constexpr int tape = bars + ((2 * TL::NSTAGE * 8 + 15) / 16) * 16;
+  static constexpr int slab0 = 2 * stage_bytes;
+  static constexpr int tape = slab0 + (NS + 1) * slab_bytes;
   // TMA tensor stores read each staged column from a 128-byte aligned base
   static_assert(amb % 128 == 0 && vf % 128 == 0 && c % 128 == 0 && ff % 128 == 0 && fcl % 128 == 0 &&
                     ic % 128 == 0 && stage_bytes % 128 == 0,
                 "staged columns must start on 128-byte boundaries");
-  static_assert(bars % 8 == 0 && tape % 16 == 0, "mbarriers 8-byte, the tape 16-byte aligned");
 };
 
 // bytes per staged row of output column `col` (kind, amb, vf, c, ff, fcl, ic) and its offset
@@ -195,7 +145,7 @@ __device__ __forceinline__ Stage<T> stage_at(unsigned char* base) {
 template <class T>
 __global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, cc_op* __restrict__ out,
                                                             int* __restrict__ count) {
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_count;
   using TL = Tile<T>;
   const STape<T> t = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem);
@@ -235,279 +185,229 @@ __device__ __forceinline__ void put_uncut_z(const Stage<float>& st, int lc, floa
   d4[1] = make_float4(hx, hz, hx, hz);
 }
 
-// Decode a pencil index (x tiles fastest, then y tiles, then z blocks) into its cell ranges.
-template <class T>
-__device__ __forceinline__ void pencil_of(const McArgs<T>& A, long long p, long long& i0, long long& j0, long long& k0,
-                                          long long& k1) {
-  const long long it = p % A.n_itiles;
-  p /= A.n_itiles;
-  const long long jt = p % A.n_jtiles;
-  p /= A.n_jtiles;
-  i0 = it * Tile<T>::TX;
-  j0 = jt * Tile<T>::TY;
-  k0 = p * KZ;
-  k1 = k0 + KZ < A.g.n[2] ? k0 + KZ : A.g.n[2];
-}
-
-// The store warp: for every slice the compute warps stage, wait until the buffer is full, send
-// the TMA-addressable columns as one tensor-store box each (one lane issues them), copy the others
-// (a `kind` row that is not a multiple of 16 bytes, ...) with the warp's lanes, and hand the
-// buffer back once the copy engine has read it. Up to NLAG + 1 copies are in flight.
-template <class T>
-__device__ __forceinline__ void fill_store_warp(const McArgs<T>& A, const ColumnMaps& maps, unsigned char* smem,
-                                                uint64_t* full, uint64_t* empty, int lane) {
+template <class T, bool SAMPLE, bool PRUNED>
+__global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
+                                                                            const __grid_constant__ ColumnMaps maps) {
   using TL = Tile<T>;
   using L = Layout<T>;
-  constexpr int S = TL::NSTAGE, LAG = TL::NLAG;
-  static_assert(LAG < S, "a buffer is handed back before the compute warps need it again");
-  const long long n0 = A.g.n[0], n1 = A.g.n[1];
-  const long long npencil = (long long)A.n_itiles * A.n_jtiles * A.n_ktiles;
+  constexpr int TX = TL::TX, TY = TL::TY, NT = TL::NT, NSX = TL::NSX, NSLAB = TL::NSLAB;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x;
+  const long long n0 = A.g.n[0], n1 = A.g.n[1], n2 = A.g.n[2];
+  const long long nx = n0 + 1, ny = n1 + 1;
+
+  int b = blockIdx.x;
+  const int it = b % A.n_itiles; b /= A.n_itiles;
+  const int jt = b % A.n_jtiles; b /= A.n_jtiles;
+  const long long i0 = (long long)it * TX, j0 = (long long)jt * TY;
+  const long long k0 = (long long)b * KZ;
+  const long long k1 = (k0 + KZ < n2) ? k0 + KZ : n2;
+
+  STape<T> tape;
+  if (SAMPLE) {
+    tape = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem + L::tape);
+    if (PRUNED) {  // this pencil's kept ops over the loaded ones (same places, fewer)
+      const int m = A.pruned_count[blockIdx.x];
+      cc_op* ops = reinterpret_cast<cc_op*>(smem + L::tape);
+      __syncthreads();
+      for (int q = tid; q < m; q += NT) ops[q] = A.pruned_ops[(long long)blockIdx.x * A.tape.n_ops + q];
+      tape.n_ops = m;
+    }
+  }
+  T* const ring = reinterpret_cast<T*>(smem + L::slab0);
+  constexpr int RS = L::slab_bytes / int(sizeof(T));  // ring slot stride, elements
+  if (SAMPLE) __syncthreads();
+
+  const T x0 = A.g.x0[0], y0 = A.g.x0[1], z0 = A.g.x0[2];
+  const T dx = A.g.d[0], dy = A.g.d[1], dz = A.g.d[2];
+  const long long nxy = nx * ny;
+
+  // This thread's node slots for one sampling round of NS slabs, fixed for the whole march:
+  // which of the round's slabs, the slab index, coordinates, the node index in the z = 0 plane,
+  // and whether this CTA owns (writes) the node.
+  constexpr int NSL = (NS * NSLAB + NT - 1) / NT;
+  int sl_s[NSL], sl_v[NSL];
+  T sl_x[NSL], sl_y[NSL];
+  long long sl_g[NSL];
+  bool sl_ok[NSL], sl_own[NSL];
+#pragma unroll
+  for (int q = 0; q < NSL; ++q) {
+    const int flat = tid + q * NT;
+    const int s = flat / NSLAB, v = flat - s * NSLAB;
+    const int tx = v % NSX, ty = v / NSX;
+    const long long i = i0 + tx, j = j0 + ty;
+    sl_s[q] = s;
+    sl_v[q] = v;
+    sl_ok[q] = s < NS && i <= n0 && j <= n1;
+    sl_own[q] = (tx < TX || i == n0) && (ty < TY || j == n1);
+    sl_x[q] = node_coord(x0, dx, i);
+    sl_y[q] = node_coord(y0, dy, j);
+    sl_g[q] = i + nx * j;
+  }
+
+  // One round: slabs zbase, zbase+1, ... (slot s samples slab zbase + s, for slabs <= zlast),
+  // into ring slot z % (NS + 1); phi written for owned nodes of owned slabs. `first` samples
+  // only slab zbase (the first slab of the march).
+  auto sample_round = [&](long long zbase, long long zlast, bool first) {
+    T pts[NSL][3];
+    T val[NSL];
+    bool use[NSL];
+#pragma unroll
+    for (int q = 0; q < NSL; ++q) {
+      const long long z = zbase + sl_s[q];
+      use[q] = sl_ok[q] && z <= zlast && (!first || sl_s[q] == 0);
+      pts[q][0] = sl_x[q];
+      pts[q][1] = sl_y[q];
+      pts[q][2] = node_coord(z0, dz, (long long)(int)z);
+    }
+    if (SAMPLE) {
+      tape_eval_multi<T, 3, NSL>(tape, pts, val);
+    }
+#pragma unroll
+    for (int q = 0; q < NSL; ++q) {
+      if (!use[q]) continue;
+      const long long z = zbase + sl_s[q];
+      const long long gi = sl_g[q] + nxy * z;
+      T v;
+      if (SAMPLE) {
+        v = val[q];
+        const bool own_slab = z < k1 || z == n2;
+        if (own_slab && sl_own[q]) A.phi_out[gi] = v;
+      } else {
+        v = A.phi_in[gi];
+      }
+      ring[(int)(z - k0) % (NS + 1) * RS + sl_v[q]] = v;
+    }
+  };
+
+
+  const int tx = tid % TX, ty = tid / TX;
+  const long long ci = i0 + tx, cj = j0 + ty;
+  const bool valid = ci < n0 && cj < n1;
+  const T xa = node_coord(x0, dx, ci), xb = node_coord(x0, dx, ci + 1);
+  const T ya = node_coord(y0, dy, cj), yb = node_coord(y0, dy, cj + 1);
+  const T hx = T(0.5) * (xb - xa), hy = T(0.5) * (yb - ya);
+  const T cx = xa + T(0.5) * dx, cy = ya + T(0.5) * dy;
+  const int lc = ty * TX + tx;
+  const int s00 = ty * NSX + tx;
+  const bool fast = A.tma_mask != 0;
+  const int rows = (int)((n1 - j0) < TY ? (n1 - j0) : TY);
+  const int cnt = (int)((n0 - i0) < TX ? (n0 - i0) : TX);
   unsigned char* gcol[7] = {reinterpret_cast<unsigned char*>(A.cols.kind), A.cols.amb,
                             reinterpret_cast<unsigned char*>(A.cols.vf), reinterpret_cast<unsigned char*>(A.cols.c),
                             reinterpret_cast<unsigned char*>(A.cols.ff), reinterpret_cast<unsigned char*>(A.cols.fcl),
                             reinterpret_cast<unsigned char*>(A.cols.ic)};
-  bool timed_out = false;
-  unsigned t = 0;  // slices staged so far by this CTA
-  for (long long p = blockIdx.x; p < npencil; p += gridDim.x) {
-    long long i0, j0, k0, k1;
-    pencil_of(A, p, i0, j0, k0, k1);
-    const int rows = (int)((n1 - j0) < TL::TY ? (n1 - j0) : TL::TY);
-    const int cnt = (int)((n0 - i0) < TL::TX ? (n0 - i0) : TL::TX);
-    for (long long k = k0; k < k1; ++k, ++t) {
-      const int sb = (int)(t % S);
-      unsigned char* sbase = smem + sb * L::stage_bytes;
-      if (!mbar_wait(&full[sb], (t / S) & 1, timed_out ? 0 : A.wait_limit)) timed_out = true;
-      if (lane == 0 && A.tma_mask) {
-        const int ci0 = (int)i0, cj0 = (int)j0, ck = (int)k;
-        if (A.tma_mask & 1) tma_store3(&maps.m[0], sbase + col_offset<T>(0), ci0, cj0, ck);
-        if (A.tma_mask & 2) tma_store3(&maps.m[1], sbase + col_offset<T>(1), ci0, cj0, ck);
-        if (A.tma_mask & 4) tma_store3(&maps.m[2], sbase + col_offset<T>(2), ci0, cj0, ck);
-        if (A.tma_mask & 8) tma_store3(&maps.m[3], sbase + col_offset<T>(3), 3 * ci0, cj0, ck);
-        if (A.tma_mask & 16) tma_store3(&maps.m[4], sbase + col_offset<T>(4), 6 * ci0, cj0, ck);
-        if (A.tma_mask & 32) tma_store4(&maps.m[5], sbase + col_offset<T>(5), 0, ci0, cj0, ck);
-        if (A.tma_mask & 64) tma_store3(&maps.m[6], sbase + col_offset<T>(6), 3 * ci0, cj0, ck);
-        bulk_commit();
+
+  // What this thread's slot of each staging buffer holds: 0 not known (first use, or a cut cell,
+  // whose slot the fill leaves alone), 1 an uncut cell outside, 2 inside (2 bits per buffer).
+  int slots = 0;
+  for (long long k = k0; k < k1; ++k) {
+    const int sb = (int)((k - k0) & 1);
+    unsigned char* sbase = smem + sb * L::stage_bytes;
+    {
+      // round r samples slabs k0 + NS r .. k0 + NS r + NS - 1 before the slice that first needs its
+      // first slab; the slabs it overwrites were last read before the previous slice's barriers
+      const int kk = (int)(k - k0);
+      if (kk == 0) sample_round(k0, k1, false);
+      else if (kk % NS == NS - 1) sample_round(k + 1, k1, false);
+    }
+    if (fast && tid == 0) bulk_wait_read<1>();  // staging buffer sb: its copy two slices ago has been read
+    __syncthreads();  // slabs k and k+1 ready; staging sb free
+
+    const T za = node_coord(z0, dz, (long long)(int)k), zb = node_coord(z0, dz, (long long)(int)(k + 1));
+    bool is_cut = false;
+    if (valid) {
+      const int rk = (int)(k - k0) % (NS + 1);
+      const T* sa = ring + rk * RS;
+      const T* sbb = ring + (rk == NS ? 0 : rk + 1) * RS;
+      const T ph[8] = {sa[s00], sa[s00 + 1], sa[s00 + NSX + 1], sa[s00 + NSX],
+                       sbb[s00], sbb[s00 + 1], sbb[s00 + NSX + 1], sbb[s00 + NSX]};
+      // nudge_zeros(v) >= 0  <=>  v > -eps  (and false for NaN, as there)
+      const T neps = -Eps<T>::v();
+      int nout = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) nout += ph[q] > neps ? 1 : 0;
+      const int state = nout == 8 ? 2 : (nout == 0 ? 1 : 0);
+      if (state != 0) {
+        const T hz = T(0.5) * (zb - za);
+        const T one = nout == 8 ? T(1) : T(0);
+        const T cen[3] = {cx, cy, za + T(0.5) * dz};
+        // (Float32 only: at Float64 the split cost more than the stores it saved, 4.91 vs 4.76 ms)
+        if (sizeof(T) == 4 && ((slots >> (2 * sb)) & 3) == state) {
+          if constexpr (sizeof(T) == 4) put_uncut_z(stage_at<T>(sbase), lc, cen[2], hx, hy, hz);
+        } else {
+          const T ff[6] = {one, one, one, one, one, one};
+          const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
+          put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+        }
+      } else {
+        is_cut = true;
       }
-      if (A.tma_mask != 0x7f) {
-        // the columns TMA cannot address, row by row: byte columns as 32-bit words when every row
-        // starts on a 4-byte boundary (x extent a multiple of 4, 4-byte aligned bases; the pencil's
-        // x offset is a multiple of 16), else bytes; T columns by element
-        const long long row0 = i0 + n0 * (j0 + n1 * k);
-#pragma unroll 1
+      slots = (slots & ~(3 << (2 * sb))) | (state << (2 * sb));
+    }
+    // Warp-ballot compaction of the cut band into the global work list. A cut cell's staged slot
+    // is left as it is: the span is copied out whole and the cut kernel, which runs after this
+    // one in stream order, overwrites the cell.
+    const unsigned m = __ballot_sync(0xffffffffu, is_cut);
+    if (m) {
+      const int lane = tid & 31;
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(A.cut_count, (unsigned)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (is_cut) A.cut_list[base + __popc(m & ((1u << lane) - 1))] = (unsigned)(ci + n0 * (cj + n1 * k));
+    }
+    if (fast) fence_proxy_async_smem();  // staged writes visible to the bulk-copy engine
+    __syncthreads();  // staging sb complete
+
+    const long long row0 = i0 + n0 * (j0 + n1 * k);
+    if (fast && tid == 0) {
+      // one thread stores the TMA-addressable columns: one box each (clipped at the grid's edge)
+      const int ci0 = (int)i0, cj0 = (int)j0, ck = (int)k;
+      if (A.tma_mask & 1) tma_store3(&maps.m[0], sbase + col_offset<T>(0), ci0, cj0, ck);
+      if (A.tma_mask & 2) tma_store3(&maps.m[1], sbase + col_offset<T>(1), ci0, cj0, ck);
+      if (A.tma_mask & 4) tma_store3(&maps.m[2], sbase + col_offset<T>(2), ci0, cj0, ck);
+      if (A.tma_mask & 8) tma_store3(&maps.m[3], sbase + col_offset<T>(3), 3 * ci0, cj0, ck);
+      if (A.tma_mask & 16) tma_store3(&maps.m[4], sbase + col_offset<T>(4), 6 * ci0, cj0, ck);
+      if (A.tma_mask & 32) tma_store4(&maps.m[5], sbase + col_offset<T>(5), 0, ci0, cj0, ck);
+      if (A.tma_mask & 64) tma_store3(&maps.m[6], sbase + col_offset<T>(6), 3 * ci0, cj0, ck);
+      bulk_commit();
+    }
+    if (A.tma_mask != 0x7f) {
+      // the columns TMA cannot address, copied by every thread: kind / ambiguous as one 32-bit word
+      // per thread where every row starts on a 4-byte boundary (rows x 2 columns x TX/4 words fit
+      // in the CTA), else bytes; T columns by element
+      static_assert(2 * TY * (TX / 4) <= NT, "one word of kind / ambiguous per thread");
+      if (A.byte_words) {
+        const int wpr = (cnt + 3) / 4;  // words per row (cnt is a multiple of 4 here)
+        const int w = tid % wpr, rest = tid / wpr, r = rest % TY, col = rest / TY;
+        if (col < 2 && r < rows && !(A.tma_mask & (1 << col))) {
+          const long long rowc = row0 + (long long)r * n0;
+          reinterpret_cast<uint32_t*>(gcol[col] + rowc)[w] =
+              reinterpret_cast<const uint32_t*>(sbase + col_offset<T>(col) + r * col_bytes<T>(col))[w];
+        }
+      }
+      for (int r = 0; r < rows; ++r) {
+        const long long rowc = row0 + (long long)r * n0;
+#pragma unroll
         for (int col = 0; col < 7; ++col) {
           if (A.tma_mask & (1 << col)) continue;
-          const int es = col_elem(col, int(sizeof(T)));  // bytes per cell
-          for (int r = 0; r < rows; ++r) {
-            const unsigned char* src = sbase + col_offset<T>(col) + r * col_bytes<T>(col);
-            unsigned char* dst = gcol[col] + (row0 + (long long)r * n0) * es;
-            if (col < 2 && A.byte_words) {
-              for (int v = lane; v < cnt / 4; v += 32)
-                reinterpret_cast<uint32_t*>(dst)[v] = reinterpret_cast<const uint32_t*>(src)[v];
-            } else if (col < 2) {
-              for (int v = lane; v < cnt; v += 32) dst[v] = src[v];
-            } else {
-              const int ne = cnt * es / int(sizeof(T));
-              for (int v = lane; v < ne; v += 32)
-                reinterpret_cast<T*>(dst)[v] = reinterpret_cast<const T*>(src)[v];
-            }
-          }
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
-        // the copy of slice t - LAG has been read out of its buffer: hand it back
-        if (A.tma_mask) bulk_wait_read<LAG>();
-        if (t >= LAG) mbar_arrive(&empty[(t - LAG) % S]);
-      }
-    }
-  }
-  if (lane == 0 && A.tma_mask) bulk_wait<0>();  // every tensor store complete before the CTA retires
-  if (timed_out && A.status) *reinterpret_cast<volatile unsigned*>(A.status) = 1u;  // plain store: may be host memory
-}
-
-// mc_fill_kernel: persistent CTAs of NT compute threads and one store warp take pencils of
-// TX x TY cells x KZ slices in turn (pencil blockIdx.x, then every gridDim.x-th). Per pencil the
-// compute threads sample the node slabs NS at a time into a ring of NS + 1 slabs (two compute-warp
-// barriers per round, none on the other slices), classify one cell each per slice, stage uncut
-// cells' fields, list cut cells through a warp ballot, and hand each staged slice to the store warp
-// through the full/empty mbarriers of NSTAGE buffers, so neither side waits on the other unless
-// the copies fall NSTAGE slices behind.
-template <class T, bool SAMPLE, bool PRUNED>
-__global__ void __launch_bounds__(Tile<T>::NT + 32, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
-                                                                                 const __grid_constant__ ColumnMaps maps) {
-  using TL = Tile<T>;
-  using L = Layout<T>;
-  constexpr int TX = TL::TX, TY = TL::TY, NT = TL::NT, NSX = TL::NSX, NSLAB = TL::NSLAB, S = TL::NSTAGE;
-  extern __shared__ __align__(128) unsigned char smem[];
-  const int tid = threadIdx.x;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::bars);
-  uint64_t* empty = full + S;
-  if (tid == 0) {
-    for (int q = 0; q < S; ++q) {
-      mbar_init(&full[q], NT / 32);  // one arrival per compute warp
-      mbar_init(&empty[q], 1);       // the store warp's
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  STape<T> tape;
-  if (SAMPLE) tape = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem + L::tape);
-  __syncthreads();  // mbarriers initialised, tape loaded
-  if (tid >= NT) {
-    fill_store_warp<T>(A, maps, smem, full, empty, tid - NT);
-    return;
-  }
-
-  const long long n0 = A.g.n[0], n1 = A.g.n[1], n2 = A.g.n[2];
-  const long long nx = n0 + 1, ny = n1 + 1;
-  const long long nxy = nx * ny;
-  const long long npencil = (long long)A.n_itiles * A.n_jtiles * A.n_ktiles;
-  T* const ring = reinterpret_cast<T*>(smem + L::slab0);
-  constexpr int RS = L::slab_bytes / int(sizeof(T));  // ring slot stride, elements
-  const T x0 = A.g.x0[0], y0 = A.g.x0[1], z0 = A.g.x0[2];
-  const T dx = A.g.d[0], dy = A.g.d[1], dz = A.g.d[2];
-  constexpr int NSL = (NS * NSLAB + NT - 1) / NT;
-  const int tx = tid % TX, ty = tid / TX;
-  const int lc = ty * TX + tx;
-  const int s00 = ty * NSX + tx;
-  const int lane = tid & 31;
-  bool timed_out = false;
-  unsigned t = 0;  // slices staged so far by this CTA
-
-  for (long long p = blockIdx.x; p < npencil; p += gridDim.x) {
-    long long i0, j0, k0, k1;
-    pencil_of(A, p, i0, j0, k0, k1);
-    compute_sync<NT>();  // the previous pencil's ring (and tape) reads are done
-    if (SAMPLE && PRUNED) {  // this pencil's kept ops over the loaded ones (same places, fewer)
-      const int m = A.pruned_count[p];
-      cc_op* ops = reinterpret_cast<cc_op*>(smem + L::tape);
-      for (int q = tid; q < m; q += NT) ops[q] = A.pruned_ops[p * A.tape.n_ops + q];
-      tape.n_ops = m;
-      compute_sync<NT>();
-    }
-
-    // This thread's node slots of one sampling round of NS slabs: which of the round's slabs, the
-    // slab index, coordinates, the node index in the z = 0 plane, and whether this CTA owns
-    // (writes) the node.
-    int sl_s[NSL], sl_v[NSL];
-    T sl_x[NSL], sl_y[NSL];
-    long long sl_g[NSL];
-    bool sl_ok[NSL], sl_own[NSL];
-#pragma unroll
-    for (int q = 0; q < NSL; ++q) {
-      const int flat = tid + q * NT;
-      const int s = flat / NSLAB, v = flat - s * NSLAB;
-      const int vx = v % NSX, vy = v / NSX;
-      const long long i = i0 + vx, j = j0 + vy;
-      sl_s[q] = s;
-      sl_v[q] = v;
-      sl_ok[q] = s < NS && i <= n0 && j <= n1;
-      sl_own[q] = (vx < TX || i == n0) && (vy < TY || j == n1);
-      sl_x[q] = node_coord(x0, dx, i);
-      sl_y[q] = node_coord(y0, dy, j);
-      sl_g[q] = i + nx * j;
-    }
-    // Round r: slabs k0 + NS r ... k0 + NS r + NS - 1 (those <= k1) into ring slot (z - k0) % (NS + 1);
-    // phi written for owned nodes of owned slabs (slab k1 belongs to the next pencil up, unless it
-    // is the grid's last).
-    auto sample_round = [&](long long zbase) {
-      T pts[NSL][3];
-      T val[NSL];
-#pragma unroll
-      for (int q = 0; q < NSL; ++q) {
-        pts[q][0] = sl_x[q];
-        pts[q][1] = sl_y[q];
-        pts[q][2] = node_coord(z0, dz, (long long)(int)(zbase + sl_s[q]));
-      }
-      if (SAMPLE) tape_eval_multi<T, 3, NSL>(tape, pts, val);
-#pragma unroll
-      for (int q = 0; q < NSL; ++q) {
-        const long long z = zbase + sl_s[q];
-        if (!sl_ok[q] || z > k1) continue;
-        const long long gi = sl_g[q] + nxy * z;
-        T v;
-        if (SAMPLE) {
-          v = val[q];
-          if ((z < k1 || z == n2) && sl_own[q]) A.phi_out[gi] = v;
-        } else {
-          v = A.phi_in[gi];
-        }
-        ring[(int)(z - k0) % (NS + 1) * RS + sl_v[q]] = v;
-      }
-    };
-
-    const long long ci = i0 + tx, cj = j0 + ty;
-    const bool valid = ci < n0 && cj < n1;
-    const T xa = node_coord(x0, dx, ci), xb = node_coord(x0, dx, ci + 1);
-    const T ya = node_coord(y0, dy, cj), yb = node_coord(y0, dy, cj + 1);
-    const T hx = T(0.5) * (xb - xa), hy = T(0.5) * (yb - ya);
-    const T cx = xa + T(0.5) * dx, cy = ya + T(0.5) * dy;
-
-    // What this thread's slot of each staging buffer holds from this pencil: 0 not known (first
-    // use, or a cut cell, whose slot the fill leaves alone), 1 an uncut cell outside, 2 inside
-    // (2 bits per buffer).
-    int slots = 0;
-    for (long long k = k0; k < k1; ++k, ++t) {
-      const int kk = (int)(k - k0);
-      if (kk == 0 || (kk % NS) == NS - 1) {
-        // slab k + 1 comes from the round starting there (slab k0 too, at the pencil's start);
-        // the round overwrites the ring slots of slabs the previous slice has finished reading
-        if (kk != 0) compute_sync<NT>();
-        sample_round(kk == 0 ? k0 : k + 1);
-        compute_sync<NT>();
-      }
-      const int sb = (int)(t % S);
-      unsigned char* sbase = smem + sb * L::stage_bytes;
-      // staging buffer sb: the store warp has finished with its previous slice
-      if (t >= S && !mbar_wait(&empty[sb], ((t / S) - 1) & 1, timed_out ? 0 : A.wait_limit)) timed_out = true;
-
-      const T za = node_coord(z0, dz, (long long)(int)k), zb = node_coord(z0, dz, (long long)(int)(k + 1));
-      bool is_cut = false;
-      if (valid) {
-        const int rk = kk % (NS + 1);
-        const T* sa = ring + rk * RS;
-        const T* sbb = ring + (rk == NS ? 0 : rk + 1) * RS;
-        const T ph[8] = {sa[s00], sa[s00 + 1], sa[s00 + NSX + 1], sa[s00 + NSX],
-                         sbb[s00], sbb[s00 + 1], sbb[s00 + NSX + 1], sbb[s00 + NSX]};
-        // nudge_zeros(v) >= 0  <=>  v > -eps  (and false for NaN, as there)
-        const T neps = -Eps<T>::v();
-        int nout = 0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) nout += ph[q] > neps ? 1 : 0;
-        const int state = nout == 8 ? 2 : (nout == 0 ? 1 : 0);
-        if (state != 0) {
-          const T hz = T(0.5) * (zb - za);
-          const T one = nout == 8 ? T(1) : T(0);
-          const T cen[3] = {cx, cy, za + T(0.5) * dz};
-          // (Float32 only: at Float64 the split cost more than the stores it saved, 4.91 vs 4.76 ms)
-          if (sizeof(T) == 4 && ((slots >> (2 * sb)) & 3) == state) {
-            if constexpr (sizeof(T) == 4) put_uncut_z(stage_at<T>(sbase), lc, cen[2], hx, hy, hz);
+          if (col < 2 && A.byte_words) continue;  // done above
+          const int es = col_elem(col, int(sizeof(T)));
+          const unsigned char* src = sbase + col_offset<T>(col) + r * col_bytes<T>(col);
+          unsigned char* dst = gcol[col] + rowc * es;
+          if (col >= 2) {
+            const T* s2 = reinterpret_cast<const T*>(src);
+            T* d2 = reinterpret_cast<T*>(dst);
+            const int ne = cnt * es / int(sizeof(T));
+            for (int v = tid; v < ne; v += NT) d2[v] = s2[v];
           } else {
-            const T ff[6] = {one, one, one, one, one, one};
-            const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
-            put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+            for (int v = tid; v < cnt; v += NT) dst[v] = src[v];
           }
-        } else {
-          is_cut = true;
         }
-        slots = (slots & ~(3 << (2 * sb))) | (state << (2 * sb));
-      }
-      // This warp's part of the slice is staged: make it visible to the copy engine and tell the
-      // store warp. A cut cell's staged slot is left as it is: the row is copied out whole and the
-      // cut kernel, which runs after this one in stream order, overwrites the cell.
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&full[sb]);
-      // Warp-ballot compaction of the cut band into the global work list.
-      const unsigned m = __ballot_sync(0xffffffffu, is_cut);
-      if (m) {
-        unsigned base = 0;
-        if (lane == 0) base = atomicAdd(A.cut_count, (unsigned)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (is_cut) A.cut_list[base + __popc(m & ((1u << lane) - 1))] = (unsigned)(ci + n0 * (cj + n1 * k));
       }
     }
   }
-  if (timed_out && A.status) *reinterpret_cast<volatile unsigned*>(A.status) = 1u;  // plain store: may be host memory
+  if (fast && tid == 0) bulk_wait<0>();  // all tensor stores complete before the CTA retires
 }
 
 template <class T, bool SAMPLE, bool MX>
@@ -612,51 +512,27 @@ int make_column_maps(const DevGrid<T>& g, const Cols& cols, ColumnMaps* maps) {
 
 namespace cci {
 
+namespace {
+constexpr long long DEFAULT_WAIT_LIMIT = 1ll << 22;  // mbarrier polls of the learned kernels' waits
+long long g_wait_limit = DEFAULT_WAIT_LIMIT;
+}  // namespace
+long long set_wait_limit(long long polls) {
+  const long long old = g_wait_limit;
+  g_wait_limit = polls < 0 ? DEFAULT_WAIT_LIMIT : polls;
+  return old;
+}
+long long wait_limit() { return g_wait_limit; }
+
 size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool f64) {
   const long long tx = f64 ? Tile<double>::TX : Tile<float>::TX, ty = Tile<float>::TY;
   const long long blocks = ((n0 + tx - 1) / tx) * ((n1 + ty - 1) / ty) * ((n2 + KZ - 1) / KZ);
   return size_t(((blocks * 4 + 15) / 16) * 16 + blocks * (long long)n_ops * (long long)sizeof(cc_op));
 }
 
-namespace {
-long long g_wait_limit = FILL_WAIT_LIMIT;
-
-// The persistent fill grid: resident CTAs per SM for this shared-memory size times the SM count,
-// at most one CTA per pencil.
-template <class K>
-int fill_grid(K kernel, int threads, int smem, long long pencils) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  const long long g = (long long)sms * per_sm;
-  return int(pencils < g ? pencils : g);
-}
-
-template <class T, bool SAMPLE, bool PRUNED>
-cudaError_t launch_fill(const McArgs<T>& a, const ColumnMaps& maps, int sm, long long pencils, cudaStream_t s) {
-  auto k = mc_fill_kernel<T, SAMPLE, PRUNED>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e != cudaSuccess) return e;
-  const int threads = Tile<T>::NT + 32;
-  k<<<fill_grid(k, threads, sm, pencils), threads, sm, s>>>(a, maps);
-  return cudaSuccess;
-}
-}  // namespace
-
-long long set_wait_limit(long long polls) {
-  const long long old = g_wait_limit;
-  g_wait_limit = polls < 0 ? FILL_WAIT_LIMIT : polls;
-  return old;
-}
-long long wait_limit() { return g_wait_limit; }
-
 template <class T>
 cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in, T* phi_out,
                       const Cols& cols, const DevTable& tb, unsigned* cut_list, unsigned* cut_count,
-                      unsigned* status, cudaStream_t s, bool with_cut, bool mixed, void* prune_scratch,
-                      size_t prune_bytes) {
+                      cudaStream_t s, bool with_cut, bool mixed, void* prune_scratch, size_t prune_bytes) {
   using TL = Tile<T>;
   McArgs<T> a;
   a.g = g;
@@ -667,8 +543,6 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   a.tb = tb;
   a.cut_list = cut_list;
   a.cut_count = cut_count;
-  a.status = status;
-  a.wait_limit = g_wait_limit;
   ColumnMaps maps;
   std::memset(&maps, 0, sizeof maps);
   a.tma_mask = make_column_maps<T>(g, cols, &maps);
@@ -677,7 +551,6 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   a.n_itiles = int((g.n[0] + TL::TX - 1) / TL::TX);
   a.n_jtiles = int((g.n[1] + TL::TY - 1) / TL::TY);
   const long long nk = (g.n[2] + KZ - 1) / KZ;
-  a.n_ktiles = int(nk);
   const long long blocks = (long long)a.n_itiles * a.n_jtiles * nk;
   if (blocks <= 0 || blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   cudaError_t e = cudaMemsetAsync(cut_count, 0, sizeof(unsigned), s);
@@ -701,22 +574,33 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   const int cut_blocks = 148 * 8;
   // the FP64 islands of mixed precision exist for Float32 caches only
   const bool mx = mixed && sizeof(T) == 4;
-  if (sample && a.pruned_ops) e = launch_fill<T, true, true>(a, maps, sm, blocks, s);
-  else if (sample) e = launch_fill<T, true, false>(a, maps, sm, blocks, s);
-  else e = launch_fill<T, false, false>(a, maps, sm, blocks, s);
-  if (e != cudaSuccess) return e;
-  if (with_cut && sample && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
-  else if (with_cut && sample) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
-  else if (with_cut && mx) mc_cut_kernel<T, false, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
-  else if (with_cut) mc_cut_kernel<T, false, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+  if (sample && a.pruned_ops) {
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_fill_kernel<T, true, true><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    if (with_cut && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+  } else if (sample) {
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_fill_kernel<T, true, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    if (with_cut && mx) mc_cut_kernel<T, true, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, true, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+  } else {
+    e = cudaFuncSetAttribute(mc_fill_kernel<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_fill_kernel<T, false, false><<<unsigned(blocks), TL::NT, sm, s>>>(a, maps);
+    if (with_cut && mx) mc_cut_kernel<T, false, true><<<cut_blocks, CUT_NT, 0, s>>>(a);
+    else if (with_cut) mc_cut_kernel<T, false, false><<<cut_blocks, CUT_NT, 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
 template cudaError_t launch_mc<float>(const DevGrid<float>&, const DevTape&, const float*, float*,
-                                      const Cols&, const DevTable&, unsigned*, unsigned*, unsigned*, cudaStream_t,
-                                      bool, bool, void*, size_t);
+                                      const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool,
+                                      void*, size_t);
 template cudaError_t launch_mc<double>(const DevGrid<double>&, const DevTape&, const double*, double*,
-                                       const Cols&, const DevTable&, unsigned*, unsigned*, unsigned*, cudaStream_t,
-                                       bool, bool, void*, size_t);
+                                       const Cols&, const DevTable&, unsigned*, unsigned*, cudaStream_t, bool, bool,
+                                       void*, size_t);
 
 }  // namespace cci

@@ -21,7 +21,7 @@ namespace {
 // Largest grid the static work list can serve: 2^23 cells (for example 203^3, or 512 x 128 x 128).
 constexpr long long kMaxCells = 8388608;
 constexpr size_t kTableBytes = 64 * 1024;    // the tiling table's device copy
-constexpr size_t kCountOffset = kTableBytes;  // the work list's counter, then the fill's wait-limit flag
+constexpr size_t kCountOffset = kTableBytes;  // the work list's counter
 constexpr size_t kListOffset = kTableBytes + 256;
 constexpr size_t kScratchBytes = kListOffset + size_t(kMaxCells) * sizeof(unsigned);  // 32 MiB + 64.25 KiB
 
@@ -130,8 +130,7 @@ extern "C" cc_status cc_mc_cells_from_phi_noalloc(int32_t device, int32_t prec, 
       }
     }
     if (e == cudaSuccess) {
-      // the launch clears the work list's counter on the stream before the fill pass; the word
-      // after it takes the fill's wait-limit flag, which this entry point does not report
+      // the launch clears the work list's counter on the stream before the fill pass
       unsigned* count = reinterpret_cast<unsigned*>(b + kCountOffset);
       unsigned* list = reinterpret_cast<unsigned*>(b + kListOffset);
       const cci::DevTable tb = lay.at(b);
@@ -141,13 +140,11 @@ extern "C" cc_status cc_mc_cells_from_phi_noalloc(int32_t device, int32_t prec, 
       if (prec == CC_F64) {
         cci::DevGrid<double> dg;
         for (int a = 0; a < 3; ++a) { dg.x0[a] = g->x0[a]; dg.d[a] = g->d[a]; dg.n[a] = g->n[a]; }
-        e = cci::launch_mc<double>(dg, none, static_cast<const double*>(phi), nullptr, cols, tb, list, count,
-                                   count + 1, s);
+        e = cci::launch_mc<double>(dg, none, static_cast<const double*>(phi), nullptr, cols, tb, list, count, s);
       } else {
         cci::DevGrid<float> dg;
         for (int a = 0; a < 3; ++a) { dg.x0[a] = float(g->x0[a]); dg.d[a] = float(g->d[a]); dg.n[a] = g->n[a]; }
-        e = cci::launch_mc<float>(dg, none, static_cast<const float*>(phi), nullptr, cols, tb, list, count,
-                                  count + 1, s);
+        e = cci::launch_mc<float>(dg, none, static_cast<const float*>(phi), nullptr, cols, tb, list, count, s);
       }
     }
     if (e != cudaSuccess) status = fail(CC_CUDA_ERR, std::string("marching cubes launch: ") + cudaGetErrorString(e));

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, co
 constexpr int FZ_X = 32, FZ_Y = 8, FZ_KZ = 32;
 
 template <class T, bool MX>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 3 : (MX ? 4 : 5)) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
+__global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
                                                             const T* __restrict__ normals,
                                                             const T* __restrict__ intercepts,
                                                             const uint8_t* __restrict__ valid) {
@@ -359,8 +359,11 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 3 : (MX ? 4 : 5)) plic_fa
     const int c = f >> 1;
     return (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
   };
-  // One cell's stored plane, loaded a slice before its fractions are formed, so the loads' latency
-  // hides behind the slice in between instead of sitting in front of the slice barrier.
+  // One cell's stored plane. At Float32 it is loaded a slice before its fractions are formed, so the
+  // loads' latency hides behind the slice in between instead of sitting in front of the slice
+  // barrier (512^3, 64 spheres: 4.36 -> 4.29 ms); at Float64 the registers that takes cost more
+  // occupancy than it saves (6.22 -> 6.63 ms), so there it is loaded when used.
+  constexpr bool PREFETCH = sizeof(T) == 4;
   struct Plane {
     T n[3], a, fr;
     bool ok;
@@ -420,8 +423,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 3 : (MX ? 4 : 5)) plic_fa
     const Plane pb = load_plane(cxy + nxy * (k0 - 1));
     prev5[q] = frac_from(pb, side_of(pb), 5);
   }
-  if (inxy && k0 + 1 < n[2]) pnext = load_plane(cxy + nxy * (k0 + 1));
-  if (hcell >= 0) hnext = load_plane(hcell + nxy * k0);
+  if (PREFETCH && inxy && k0 + 1 < n[2]) pnext = load_plane(cxy + nxy * (k0 + 1));
+  if (PREFETCH && hcell >= 0) hnext = load_plane(hcell + nxy * k0);
   const int lane = q & 31, wrow = q >> 5;
   static_assert(X == 32, "a warp is one row of the slice");
   for (long long k = k0; k < k1; ++k) {
@@ -431,10 +434,17 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 3 : (MX ? 4 : 5)) plic_fa
     T* const res = &bufs[r3 == 0 ? 2 : r3 - 1][wrow][0][0];  // this warp's row, cell-major
     T (*hxp)[Y] = hx[par];
     T (*hyp)[X] = hy[par];
-    const Plane pcur = pnext, hcur = hnext;
-    // the planes the next slice needs, loaded now
-    if (inxy && k + 2 < n[2]) pnext = load_plane(cxy + nxy * (k + 2));
-    if (hcell >= 0 && k + 1 < k1) hnext = load_plane(hcell + nxy * (k + 1));
+    Plane pcur{}, hcur{};
+    if constexpr (PREFETCH) {
+      pcur = pnext;
+      hcur = hnext;
+      // the planes the next slice needs, loaded now
+      if (inxy && k + 2 < n[2]) pnext = load_plane(cxy + nxy * (k + 2));
+      if (hcell >= 0 && k + 1 < k1) hnext = load_plane(hcell + nxy * (k + 1));
+    } else {
+      if (inxy && k + 1 < n[2]) pcur = load_plane(cxy + nxy * (k + 1));
+      if (hcell >= 0) hcur = load_plane(hcell + nxy * k);
+    }
     if (k + 1 < n[2]) own6(nxt, pcur);
     if (hcell >= 0) {
       const T v = frac_from(hcur, side_of(hcur), hface);

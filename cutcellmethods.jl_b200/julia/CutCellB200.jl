@@ -163,12 +163,8 @@ function handle!(a::B200Array, method::Int32, dim::Integer, ::Type{T}, n) where 
     return a.handle
 end
 
-# Block on the cache's stream, as update_cache! does (src/marching_squares/cache.jl:62), then ask
-# the handle whether a kernel gave up one of its bounded waits.
-function finish(h::Handle)
-    CUDA.synchronize()
-    check(ccall((:cc_handle_status, LIB), Cint, (Ptr{Cvoid},), h.h))
-end
+# Block on the cache's stream, as update_cache! does (src/marching_squares/cache.jl:62).
+finish(::Handle) = CUDA.synchronize()
 
 # ---- bodies: SDFLibrary geometry flattened to the op-tape ------------------------------------
 # Opcodes and combine modes of include/cutcell_b200.h.

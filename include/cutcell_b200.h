@@ -202,17 +202,10 @@ typedef struct cc_handle cc_handle;
 cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t prec,
                            const int64_t n[3], cc_handle** out);
 cc_status cc_handle_destroy(cc_handle* h);
-/* Whether a kernel of an earlier call on this handle gave up a bounded wait (CC_DEVICE_TIMEOUT,
- * then cleared) or not (CC_OK). The marching-cubes fill kernel hands staged slices between its
- * compute warps and its store warp through mbarriers; every wait polls a limited number of times
- * (cc_set_wait_limit) and, when the limit runs out, the kernel records it here and finishes without
- * the data it waited for. Read it after the update's stream has synchronized: update_cache! blocks
- * on the stream (src/marching_squares/cache.jl:62) and then asks. No device call; does not block. */
-cc_status cc_handle_status(cc_handle* h);
-/* The number of mbarrier polls after which a wait of the fill and learned kernels gives up, for
- * later launches; returns the previous value. A negative value restores the default (2^22).
- * Lowering it to 0 makes every such wait give up at once: a way to exercise the timeout path
- * (the fill then writes unspecified values and reports CC_DEVICE_TIMEOUT). */
+/* The number of mbarrier polls after which a wait of the learned kernels (for a CTA's own
+ * tensor-core MMAs) gives up, for later launches; returns the previous value. A negative value
+ * restores the default (2^22). Lowering it to 0 makes every such wait give up at once: a way to
+ * exercise the timeout path, which then reports CC_DEVICE_TIMEOUT. */
 int64_t cc_set_wait_limit(int64_t polls);
 /* Upload a marching-cubes tiling table blob (validated) into the handle. */
 cc_status cc_handle_set_mc_table(cc_handle* h, const void* blob, size_t nbytes);
@@ -467,7 +460,6 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
  *     that first call before any stream capture.
  *   - The table is copied from the host only when the device does not already hold the same
  *     blob (compared by size and hash) from an earlier call in the same context.
- *   - A fill wait that runs out of polls (cc_handle_status) is not reported by this entry point.
  *   - Every call reuses the same array: calls that overlap on the GPU (other streams, other host
  *     threads) race. Serialize them, e.g. on one stream.
  * Calls no cudaMalloc, cudaFree or other allocating routine. */

@@ -1,10 +1,9 @@
 """The bounded waits' failure path, made to run out on purpose and safely: with the poll limit at
-0 (cc_set_wait_limit), every mbarrier wait of the marching-cubes fill and of the learned kernels
-gives up at once. Nothing is left hanging: the fill finishes without the data it waited for, a
-learned CTA first lets its committed MMAs drain and then frees its tensor memory, and the host
-reports CC_DEVICE_TIMEOUT. With the default limit restored, the same kernels run again and give
-the normal results bit for bit (a CTA that had kept its tensor memory would leave the next
-allocation short)."""
+0 (cc_set_wait_limit), every mbarrier wait of the learned kernels (a CTA's wait for its own
+tensor-core MMAs) gives up at once. Nothing is left hanging: the CTA first lets its committed MMAs
+drain with the default limit, then frees its tensor memory, and the host reports
+CC_DEVICE_TIMEOUT. With the default limit restored, the same kernels run again and give the normal
+results bit for bit (a CTA that had kept its tensor memory would leave the next allocation short)."""
 import numpy as np
 import pytest
 import torch
@@ -25,20 +24,6 @@ class wait_limit:
 
     def __exit__(self, *a):
         _lib.load().cc_set_wait_limit(-1)
-
-
-def test_fill_wait_timeout_is_reported_and_recovers():
-    g = cc.workloads.csg_grid(64)
-    body = cc.workloads.csg_body(0)
-    ref = cc.update_cache(cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32), body, g).to_host()
-    c = cc.allocate_cache(g, cc.MarchingCubesCutCell(), dtype=torch.float32)
-    with wait_limit(0):
-        with pytest.raises(cc.CCError) as e:
-            cc.update_cache(c, body, g)
-    assert e.value.status == _lib.CC_DEVICE_TIMEOUT
-    assert _lib.load().cc_handle_status(c.handle.h) == _lib.CC_OK  # reported once, then cleared
-    cc.update_cache(c, body, g)
-    assert_cells_bitwise(c.to_host(), ref, label="after a timeout")
 
 
 def test_learned_wait_timeout_frees_tensor_memory_and_recovers():
