@@ -408,6 +408,33 @@ def near_zero_cells(c):
     return (F.max_pool3d(near, 2, stride=1) > 0).reshape(-1)
 
 
+def decider_threshold_cells(c, chunk=32):
+    """Per cell: does one of its faces have alternating corner signs and an asymptotic-decider
+    determinant |A C - B D| below eps(Float32) (src/marching_cubes/marching_cubes.jl:401-406)? There
+    a Float32 or mixed update decides by the threshold, face >= 0, where Float64, whose threshold is
+    eps(Float64), decides by the determinant's sign: the two tile the cell differently. Computed in
+    Float64 on the cache's phi nudged as Float32 nudges it."""
+    import torch
+    n0, n1, n2 = c.n
+    phi = c.phi.reshape(n2 + 1, n1 + 1, n0 + 1)
+    e = float(torch.finfo(torch.float32).eps)
+    out = torch.zeros(n2, n1, n0, dtype=torch.bool, device=phi.device)
+
+    def amb(a, b, cc_, d):
+        pa, pb, pc, pd = a >= 0, b >= 0, cc_ >= 0, d >= 0
+        return (pa == pc) & (pb == pd) & (pa != pb) & ((a * cc_ - b * d).abs() < e)
+    for k0 in range(0, n2, chunk):
+        k1 = min(k0 + chunk, n2)
+        v = phi[k0:k1 + 1].double()
+        v = torch.where(v.abs() < e, torch.full_like(v, e), v)
+        fx = amb(v[:-1, :-1, :], v[:-1, 1:, :], v[1:, 1:, :], v[1:, :-1, :])    # faces normal to x
+        fy = amb(v[:-1, :, :-1], v[:-1, :, 1:], v[1:, :, 1:], v[1:, :, :-1])    # normal to y
+        fz = amb(v[:, :-1, :-1], v[:, :-1, 1:], v[:, 1:, 1:], v[:, 1:, :-1])    # normal to z
+        out[k0:k1] = (fx[:, :, :-1] | fx[:, :, 1:]) | (fy[:, :-1, :] | fy[:, 1:, :]) | (fz[:-1] | fz[1:])
+        del v, fx, fy, fz
+    return out.reshape(-1)
+
+
 def precision_report(cc, g, c32, c64, cm, dev):
     """Every column's error of the Float32 and mixed updates against Float64, split into its
     sources. ``c64_on_32`` is the Float64 cell construction run on the Float32 update's phi: against
@@ -422,22 +449,28 @@ def precision_report(cc, g, c32, c64, cm, dev):
     cc.update_cache(c64on32, cc.NodalField(c32.phi.double()), g)
     flips = cells_differ(c32, cm)
     near = near_zero_cells(c32)
+    thresh = decider_threshold_cells(c32)
     out = {"reference": "the Float64 update of the same body and grid",
            "float32": field_errors(c32, c64), "mixed": field_errors(cm, c64),
            "input_rounding": {"what": "Float64 cells from the Float32 phi, against the Float64 update",
                               **field_errors(c64on32, c64)},
            "float32_decider_flip_cells": int(flips.sum().item()),
            "near_zero_corner_cells": int(near.sum().item()),
+           "decider_threshold_cells": int(thresh.sum().item()),
+           "decider_threshold": {"what": "Float32 against Float64 cells on the same Float32 phi, cells with a "
+                                         "face decided by the eps(Float32) threshold, not the determinant's sign",
+                                 **field_errors(c32, c64on32, keep=thresh)},
            "near_zero": {"what": "Float32 against Float64 cells on the same Float32 phi, cells with a corner "
                                  "within eps(Float32) of zero (nudged in Float32 only)",
                          **field_errors(c32, c64on32, keep=near)},
            "float32_arithmetic": {"what": "Float32 against Float64 cells on the same Float32 phi, cells with the "
-                                          "same decisions as mixed and no corner within eps(Float32) of zero",
-                                  **field_errors(c32, c64on32, keep=~flips & ~near)},
+                                          "same decisions as mixed, no corner within eps(Float32) of zero and no "
+                                          "face at the decider threshold",
+                                  **field_errors(c32, c64on32, keep=~flips & ~near & ~thresh)},
            "mixed_arithmetic": {"what": "mixed against Float64 cells on the same Float32 phi, no corner within "
-                                        "eps(Float32) of zero",
-                                **field_errors(cm, c64on32, keep=~near)}}
-    del c64on32, flips, near
+                                        "eps(Float32) of zero, no face at the decider threshold",
+                                **field_errors(cm, c64on32, keep=~near & ~thresh)}}
+    del c64on32, flips, near, thresh
     torch.cuda.empty_cache()
     return out
 
