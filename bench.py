@@ -543,6 +543,31 @@ def traffic_per_update(n):
     return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
 
 
+# Per-cell counts of the PLIC Float32 update (fit + face pass) on the 64-sphere union, from one ncu
+# capture at 256^3 (sm__inst_executed.sum; FADD + FMUL + 2 FFMA thread instructions): 316.2 M +
+# 305.6 M warp instructions and 2415 M + 468 M FP32 flops over 16,777,216 cells. At 512^3 the
+# pruned union keeps fewer spheres per slab, so these overstate the 512^3 work a little.
+PLIC_F32_WARP_INSTS_PER_CELL = (316.16e6 + 305.55e6) / 16777216
+PLIC_F32_FLOPS_PER_CELL = ((1076.08 + 424.43 + 2 * 914.97) + (313.19 + 129.37 + 2 * 25.52)) * 1e6 / 16777216
+B200_SMS, B200_MHZ = 148, 1965.0
+
+
+def plic_rooflines(cells, ms, peak_gbs, bytes_per_cell=46):
+    """The PLIC update against the three rooflines that could bound it: HBM (the bytes it must
+    write), the FP32 pipe (128 lanes per SM, FFMA two flops) and instruction issue (4 warp
+    instructions per SM per cycle), at B200's 148 SMs and 1965 MHz."""
+    t = ms * 1e-3
+    fp32_peak = B200_SMS * 128 * 2 * B200_MHZ * 1e6
+    issue_peak = B200_SMS * 4 * B200_MHZ * 1e6
+    hbm = cells * bytes_per_cell / t / 1e9 / peak_gbs
+    fp32 = cells * PLIC_F32_FLOPS_PER_CELL / t / fp32_peak
+    issue = cells * PLIC_F32_WARP_INSTS_PER_CELL / t / issue_peak
+    return {"hbm_frac": hbm, "fp32_pipe_frac": fp32, "issue_frac": issue,
+            "bound": max((("hbm", hbm), ("fp32 pipe", fp32), ("instruction issue", issue)), key=lambda x: x[1])[0],
+            "fp32_flops_per_cell": PLIC_F32_FLOPS_PER_CELL, "warp_instructions_per_cell": PLIC_F32_WARP_INSTS_PER_CELL,
+            "counts_source": "ncu at 256^3 (fit + face pass), profiles/plic_fit_face_f32_256_fp.md"}
+
+
 def plic_block(args, dev, cc):
     """PLIC over [0,1]^3 at n^3, a union of 64 seeded spheres: update times (Float32, Float64,
     mixed), the resolved face fractions' single-valuedness, every precision's error against
@@ -588,6 +613,7 @@ def plic_block(args, dev, cc):
         fd = (c.cells.face_fraction.double() - ref.cells.face_fraction).abs()
         out[name] = {"ms": ms, "cells_per_s": n ** 3 / (ms * 1e-3),
                      "roofline_frac": n ** 3 * 46 / (ms * 1e-3) / 1e9 / measured_peak()[0],
+                     "rooflines": plic_rooflines(n ** 3, ms, measured_peak()[0]),
                      "shared_face_mismatches": faces_single_valued(c),
                      "is_valid_differs_from_f64": int((c.is_valid != ref.is_valid).sum().item()),
                      "kind_differs_from_f64": int((c.cells.kind != ref.cells.kind).sum().item()),
