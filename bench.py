@@ -543,12 +543,14 @@ def traffic_per_update(n):
     return (1.7377e9 + 3.9e6) * s ** 3 + 21.3e6 * s ** 2
 
 
-# Per-cell counts of the PLIC Float32 update (fit + face pass) on the 64-sphere union, from one ncu
-# capture at 256^3 (sm__inst_executed.sum; FADD + FMUL + 2 FFMA thread instructions): 316.2 M +
-# 305.6 M warp instructions and 2415 M + 468 M FP32 flops over 16,777,216 cells. At 512^3 the
-# pruned union keeps fewer spheres per slab, so these overstate the 512^3 work a little.
-PLIC_F32_WARP_INSTS_PER_CELL = (316.16e6 + 305.55e6) / 16777216
-PLIC_F32_FLOPS_PER_CELL = ((1076.08 + 424.43 + 2 * 914.97) + (313.19 + 129.37 + 2 * 25.52)) * 1e6 / 16777216
+# Per-cell counts of the PLIC Float32 update (fit + face pass) on the 64-sphere union. Warp
+# instructions from one ncu capture at 512^3 (sm__inst_executed.sum, one pass: 1925.4 M + 2276.7 M
+# over 134,217,728 cells). FP32 flops (FADD + FMUL + 2 FFMA thread instructions) from a capture at
+# 256^3 (2415 M + 468 M over 16,777,216 cells), scaled to 512^3 by the two sizes' ratio of
+# instructions per cell (31.31 / 37.06).
+PLIC_F32_WARP_INSTS_PER_CELL = (1925.36e6 + 2276.66e6) / 134217728
+PLIC_F32_FLOPS_PER_CELL = (((1076.08 + 424.43 + 2 * 914.97) + (313.19 + 129.37 + 2 * 25.52)) * 1e6 / 16777216
+                           * PLIC_F32_WARP_INSTS_PER_CELL / ((316.16e6 + 305.55e6) / 16777216))
 B200_SMS, B200_MHZ = 148, 1965.0
 
 
@@ -565,7 +567,7 @@ def plic_rooflines(cells, ms, peak_gbs, bytes_per_cell=46):
     return {"hbm_frac": hbm, "fp32_pipe_frac": fp32, "issue_frac": issue,
             "bound": max((("hbm", hbm), ("fp32 pipe", fp32), ("instruction issue", issue)), key=lambda x: x[1])[0],
             "fp32_flops_per_cell": PLIC_F32_FLOPS_PER_CELL, "warp_instructions_per_cell": PLIC_F32_WARP_INSTS_PER_CELL,
-            "counts_source": "ncu at 256^3 (fit + face pass), profiles/plic_fit_face_f32_256_fp.md"}
+            "counts_source": "ncu: instructions at 512^3, flops at 256^3 scaled (profiles/plic_fit_face_f32_256_fp.md)"}
 
 
 def plic_block(args, dev, cc):

@@ -100,8 +100,10 @@ struct Layout {
   static constexpr int c = vf + NC * int(sizeof(T));
   static constexpr int ff = c + 3 * NC * int(sizeof(T));
   static constexpr int fcl = ff + 6 * NC * int(sizeof(T));
-  static constexpr int ic = fcl + 12 * NC * int(sizeof(T));
-  static constexpr int stage_bytes = ((ic + 3 * NC * int(sizeof(T)) + 127) / 128) * 128;
+  // an uncut cell's interface centroid is its centroid, and a cut cell's staged values are
+  // overwritten by the cut kernel: the interface_centroid box is sent from the centroid column
+  static constexpr int ic = c;
+  static constexpr int stage_bytes = ((fcl + 12 * NC * int(sizeof(T)) + 127) / 128) * 128;
   static constexpr int slab_bytes = ((TL::NSLAB * int(sizeof(T)) + 15) / 16) * 16;
   static constexpr int slab0 = 2 * stage_bytes;
   static constexpr int tape = slab0 + (NS + 1) * slab_bytes;
@@ -179,7 +181,6 @@ __global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, c
 // 512^3 CSG body: Float32 update 2.78 -> 2.74 ms.
 __device__ __forceinline__ void put_uncut_z(const Stage<float>& st, int lc, float cz, float hx, float hy, float hz) {
   st.c[3 * lc + 2] = cz;
-  st.ic[3 * lc + 2] = cz;
   float4* d4 = reinterpret_cast<float4*>(st.fcl + 12 * lc);
   d4[0] = make_float4(hy, hz, hy, hz);
   d4[1] = make_float4(hx, hz, hx, hz);
@@ -338,7 +339,13 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
         } else {
           const T ff[6] = {one, one, one, one, one, one};
           const T fcl[12] = {hy, hz, hy, hz, hx, hz, hx, hz, hx, hy, hx, hy};
-          put_cell<T>(stage_at<T>(sbase), lc, nout == 8 ? 1 : 0, 0, one, cen, ff, fcl, cen);
+          const Stage<T> st = stage_at<T>(sbase);
+          st.kind[lc] = int8_t(nout == 8 ? 1 : 0);
+          st.amb[lc] = 0;
+          st.vf[lc] = one;
+          st.c[3 * lc] = cen[0]; st.c[3 * lc + 1] = cen[1]; st.c[3 * lc + 2] = cen[2];
+          put_vec<T>(st.ff + 6 * lc, ff, 6);
+          put_vec<T>(st.fcl + 12 * lc, fcl, 12);
         }
       } else {
         is_cut = true;
