@@ -3,18 +3,18 @@
 // Two kernels replace the reference's two KernelAbstractions launches
 // (_sample_nodes_kernel! and _nodal_cells_kernel!, src/marching_squares/cache.jl:55-78):
 //
-//   * mc_fill_kernel: a CTA owns a pencil of TX x 4 cells in (x, y) and marches KZ slices along
-//     z. Each slice it samples one new slab of (TX+1) x 5 node values from the op-tape into shared
-//     memory (the slab below is kept from the previous slice), so a node is evaluated once per
-//     CTA and written to phi once, by the CTA that owns it. Every thread classifies one cell from
-//     its eight corners. Uncut cells (all corners of one sign) get their fields directly -- their
-//     face centroids are half the lattice edge lengths, a cheap affine fill -- into a
-//     double-buffered shared-memory staging tile that leaves as contiguous row spans of each
-//     StructArray column through the TMA bulk-copy engine (cp.async.bulk, shared -> global), so
-//     the SM's threads never issue the column stores. Cut cells are compacted with a warp ballot
-//     into a global work list.
+//   * mc_fill_kernel: a CTA owns a pencil of TX x TY cells in (x, y) and marches up to KZ slices
+//     along z. Node slabs of (TX+1) x (TY+1) values are sampled from the op-tape NS at a time into
+//     a shared-memory ring, so a node is evaluated once per CTA and written to phi once, by the
+//     CTA that owns it. Every thread classifies one cell from its eight corners. Uncut cells (all
+//     corners of one sign) get their fields directly -- their face centroids are half the lattice
+//     edge lengths, a cheap affine fill -- into a double-buffered shared-memory staging tile that
+//     leaves as one TMA tensor store per StructArray column (cp.async.bulk.tensor, shared ->
+//     global), so the SM's threads never issue the column stores. Cut cells are compacted with a
+//     warp ballot into a global work list.
 //   * mc_cut_kernel: one lane per listed cut cell runs the full construction of
 //     src/marching_cubes/moments.jl:275-346 densely and writes that cell's fields.
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <cuda.h>
@@ -42,8 +42,8 @@ template <class T> struct Tile {
   static constexpr int NSLAB = (TX + 1) * (TY + 1);
   static constexpr int MINB = sizeof(T) == 4 ? 3 : 3;  // Float64 at 4 spills
 };
-constexpr int KZ = 31;  // z slices marched per CTA: KZ + 1 = 32 node slabs, 8 sampling rounds of NS
 constexpr int NS = 4;   // node slabs sampled per round (one op-major tape pass per thread)
+constexpr int KZ = 31;  // most z slices marched per CTA: KZ + 1 = 32 node slabs, 8 sampling rounds
 constexpr int CUT_NT = 256;  // 512^3 CSG body, Float32 update: 2.73 ms at 128, 2.71-2.72 at 256, 2.75 at 64
 
 template <class T>
@@ -57,6 +57,7 @@ struct McArgs {
   unsigned* cut_list;
   unsigned* cut_count;
   int n_itiles, n_jtiles;
+  int kz;  // z slices per pencil (pencil_slices)
   int tma_mask;  // bit c: column c leaves through TMA tensor stores (its map below is valid)
   int byte_words;  // kind/ambiguous rows start on 4-byte boundaries
   // a union of spheres: each CTA's kept ops (stride tape.n_ops) and their count, or null
@@ -147,7 +148,7 @@ __device__ __forceinline__ Stage<T> stage_at(unsigned char* base) {
 template <class T>
 __global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, cc_op* __restrict__ out,
                                                             int* __restrict__ count) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];  // one alignment for every extern declaration
   __shared__ int s_count;
   using TL = Tile<T>;
   const STape<T> t = load_tape<T>(A.tape.bytes, A.tape.n_ops, A.tape.n_params, smem);
@@ -157,9 +158,9 @@ __global__ void __launch_bounds__(256) prune_pencils_kernel(const McArgs<T> A, c
   const int it = b % A.n_itiles; b /= A.n_itiles;
   const int jt = b % A.n_jtiles; b /= A.n_jtiles;
   const long long n0 = A.g.n[0], n1 = A.g.n[1], n2 = A.g.n[2];
-  const long long i0 = (long long)it * TL::TX, j0 = (long long)jt * TL::TY, k0 = (long long)b * KZ;
+  const long long i0 = (long long)it * TL::TX, j0 = (long long)jt * TL::TY, k0 = (long long)b * A.kz;
   const long long i1 = i0 + TL::TX < n0 ? i0 + TL::TX : n0, j1 = j0 + TL::TY < n1 ? j0 + TL::TY : n1;
-  const long long k1 = k0 + KZ < n2 ? k0 + KZ : n2;
+  const long long k1 = k0 + A.kz < n2 ? k0 + A.kz : n2;
   const double lo[3] = {double(A.g.x0[0]) + double(i0) * double(A.g.d[0]),
                         double(A.g.x0[1]) + double(j0) * double(A.g.d[1]),
                         double(A.g.x0[2]) + double(k0) * double(A.g.d[2])};
@@ -201,8 +202,8 @@ __global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(con
   const int it = b % A.n_itiles; b /= A.n_itiles;
   const int jt = b % A.n_jtiles; b /= A.n_jtiles;
   const long long i0 = (long long)it * TX, j0 = (long long)jt * TY;
-  const long long k0 = (long long)b * KZ;
-  const long long k1 = (k0 + KZ < n2) ? k0 + KZ : n2;
+  const long long k0 = (long long)b * A.kz;
+  const long long k1 = (k0 + A.kz < n2) ? k0 + A.kz : n2;
 
   STape<T> tape;
   if (SAMPLE) {
@@ -477,7 +478,7 @@ EncodeTiledFn encode_fn() {
 // The column maps of a marching-cubes cache: bit c of the result is set when column c (kind,
 // ambiguous, volume_fraction, centroid, face_fraction, face_centroid_local, interface_centroid) can
 // be written by TMA tensor stores -- its base 16-byte aligned, its row pitch (x extent x bytes per
-// cell) a multiple of 16 bytes, every dimension below 2^31. The store warp copies the others.
+// cell) a multiple of 16 bytes, every dimension below 2^31. The CTA's threads copy the others.
 template <class T>
 int make_column_maps(const DevGrid<T>& g, const Cols& cols, ColumnMaps* maps) {
   using TL = Tile<T>;
@@ -530,9 +531,89 @@ long long set_wait_limit(long long polls) {
 }
 long long wait_limit() { return g_wait_limit; }
 
+namespace {
+// SMs of the current device (read once per device).
+long long device_sms() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::atomic<int>* c = dev >= 0 && dev < 64 ? &cache[dev] : nullptr;
+  int v = c ? c->load(std::memory_order_relaxed) : 0;
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    if (c) c->store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+}  // namespace
+
+// Slices per fill pencil for an n0 x n1 x n2 grid. The CTAs are launched x-tile fastest and
+// z-layer slowest, so every layer of pencils but the last is kz slices deep and the last is the
+// remainder. Each candidate depth (kz + 1 a whole number of NS-slab sampling rounds) is scored by
+// list-scheduling the launch on the resident CTAs (each pencil to the earliest free one, in launch
+// order), a pencil taking its slices plus PENCIL_OVERHEAD slice-times (its tape load, first
+// sampling round and last drain). Few waves of deep pencils leave SMs idle in the last wave: at
+// 256^3, 31-slice pencils make 5.2 waves of the 444 resident CTAs; 27-slice pencils fill 5.8.
+int pencil_slices(long long n0, long long n1, long long n2, bool f64) {
+  const long long tx = f64 ? Tile<double>::TX : Tile<float>::TX, ty = Tile<float>::TY;
+  const long long tiles = ((n0 + tx - 1) / tx) * ((n1 + ty - 1) / ty);
+  const long long slots = device_sms() * (f64 ? Tile<double>::MINB : Tile<float>::MINB);
+  constexpr double PENCIL_OVERHEAD = 2.0;
+  int best = KZ;
+  double best_t = 0;
+  for (int kz = KZ; kz >= NS - 1; kz -= NS) {
+    const long long layers = (n2 + kz - 1) / kz;
+    const long long rem = n2 - (layers - 1) * kz;
+    // groups of resident CTAs that become free at the same time: (time, count), times increasing
+    double gt[8];
+    long long gc[8];
+    int ng = 1;
+    gt[0] = 0;
+    gc[0] = slots;
+    double end = 0;
+    const long long batch[2] = {tiles * (layers - 1), tiles};
+    const double dur[2] = {kz + PENCIL_OVERHEAD, rem + PENCIL_OVERHEAD};
+    for (int bi = 0; bi < 2; ++bi) {
+      long long m = batch[bi];
+      while (m > 0) {
+        // the earliest group takes as many pencils as it has CTAs; they free up dur later
+        const long long k = gc[0] < m ? gc[0] : m;
+        const double t = gt[0] + dur[bi];
+        end = t > end ? t : end;
+        m -= k;
+        if (k == gc[0]) {
+          for (int q = 1; q < ng; ++q) { gt[q - 1] = gt[q]; gc[q - 1] = gc[q]; }
+          --ng;
+        } else {
+          gc[0] -= k;
+        }
+        int q = 0;
+        while (q < ng && gt[q] < t) ++q;
+        if (q < ng && gt[q] == t) {
+          gc[q] += k;
+        } else if (ng < 8) {
+          for (int r = ng; r > q; --r) { gt[r] = gt[r - 1]; gc[r] = gc[r - 1]; }
+          gt[q] = t;
+          gc[q] = k;
+          ++ng;
+        } else {
+          gc[ng - 1] += k;  // out of groups: merge into the latest (a later free time, never earlier)
+          gt[ng - 1] = t > gt[ng - 1] ? t : gt[ng - 1];
+        }
+      }
+    }
+    if (kz == KZ || end < best_t * 0.995) {  // a shallower pencil only for a clear gain
+      best = kz;
+      best_t = end;
+    }
+  }
+  return best;
+}
+
 size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool f64) {
   const long long tx = f64 ? Tile<double>::TX : Tile<float>::TX, ty = Tile<float>::TY;
-  const long long blocks = ((n0 + tx - 1) / tx) * ((n1 + ty - 1) / ty) * ((n2 + KZ - 1) / KZ);
+  const long long kz = pencil_slices(n0, n1, n2, f64);
+  const long long blocks = ((n0 + tx - 1) / tx) * ((n1 + ty - 1) / ty) * ((n2 + kz - 1) / kz);
   return size_t(((blocks * 4 + 15) / 16) * 16 + blocks * (long long)n_ops * (long long)sizeof(cc_op));
 }
 
@@ -557,7 +638,8 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
                   (reinterpret_cast<uintptr_t>(cols.amb) & 3u) == 0) ? 1 : 0;
   a.n_itiles = int((g.n[0] + TL::TX - 1) / TL::TX);
   a.n_jtiles = int((g.n[1] + TL::TY - 1) / TL::TY);
-  const long long nk = (g.n[2] + KZ - 1) / KZ;
+  a.kz = pencil_slices(g.n[0], g.n[1], g.n[2], sizeof(T) == 8);
+  const long long nk = (g.n[2] + a.kz - 1) / a.kz;
   const long long blocks = (long long)a.n_itiles * a.n_jtiles * nk;
   if (blocks <= 0 || blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   cudaError_t e = cudaMemsetAsync(cut_count, 0, sizeof(unsigned), s);
