@@ -355,6 +355,8 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
     e = cudaMalloc(&h->cut_list, size_t(ncell) * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&h->cut_count, sizeof(unsigned));
   }
+  if (e == cudaSuccess && method == CC_PLIC && dim == 3 && !tree)
+    e = cudaMalloc(&h->plic_sides, size_t(h->n[0] * h->n[1] * h->n[2]));
   if (e != cudaSuccess) {
     cc_handle_destroy(h);
     return cuda_fail(e, "cc_handle_create");
@@ -374,6 +376,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->rep_scratch) cudaFree(h->rep_scratch);
   if (h->cut_list) cudaFree(h->cut_list);
   if (h->cut_count) cudaFree(h->cut_count);
+  if (h->plic_sides) cudaFree(h->plic_sides);
   if (h->mesh_vbase) cudaFree(h->mesh_vbase);
   if (h->mesh_scan) cudaFree(h->mesh_scan);
   if (h->mesh_list) cudaFree(h->mesh_list);
@@ -529,16 +532,16 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   if (h->prec == CC_F64) {
     if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     e = g->dim == 3 ? cci::launch_plic<double, 3>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
-                                                  static_cast<double*>(intercepts), is_valid, s)
+                                                  static_cast<double*>(intercepts), is_valid, h->plic_sides, s)
                     : cci::launch_plic<double, 2>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
-                                                  static_cast<double*>(intercepts), is_valid, s);
+                                                  static_cast<double*>(intercepts), is_valid, h->plic_sides, s);
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
     const bool mx = h->prec == CC_MIXED;
     e = g->dim == 3 ? cci::launch_plic<float, 3>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
-                                                 static_cast<float*>(intercepts), is_valid, s, mx)
+                                                 static_cast<float*>(intercepts), is_valid, h->plic_sides, s, mx)
                     : cci::launch_plic<float, 2>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
-                                                 static_cast<float*>(intercepts), is_valid, s, mx);
+                                                 static_cast<float*>(intercepts), is_valid, h->plic_sides, s, mx);
   }
   if (e != cudaSuccess) return cuda_fail(e, "PLIC launch");
   return CC_OK;

@@ -99,9 +99,12 @@ cudaError_t launch_ms_tree(const T x0[2], const double base_d[2], long long nlea
                            const int32_t* level, const int32_t* coord, const DevTape& tape,
                            T* phi4, const Cols& cols, cudaStream_t s, bool mixed = false);
 
+// PLIC update: the fit pass, then the face pass. In 3D the fit records each cell's side (whether
+// its plane crosses the cell, or every face is empty or full) in `sides`, one byte per cell, for
+// the face pass; 2D takes null.
 template <class T, int D>
 cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals,
-                        T* intercepts, uint8_t* valid, cudaStream_t s, bool mixed = false);
+                        T* intercepts, uint8_t* valid, int8_t* sides, cudaStream_t s, bool mixed = false);
 
 // calc_volume partial sums: nblocks (sum, compensation) pairs into `partial`, then a final
 // single-block pass into out[0..1]. `partial` holds 2 * calc_volume_blocks() doubles.
@@ -165,6 +168,7 @@ struct cc_handle {
   cci::DevTable tb{};
   unsigned* cut_list = nullptr;   // marching cubes: the cut band's cell indices (one slot per cell)
   unsigned* cut_count = nullptr;
+  int8_t* plic_sides = nullptr;  // 3D PLIC: the fit's per-cell side bytes for the face pass
   double* vol_scratch = nullptr;  // calc_volume partials + result
   unsigned long long* rep_scratch = nullptr;  // report counters + min
   unsigned* mesh_vbase = nullptr;  // generate_mesh: first vertex of each node's cut edges

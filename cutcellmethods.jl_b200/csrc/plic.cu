@@ -317,21 +317,32 @@ __global__ void __launch_bounds__(NT, 6) plic_face_kernel(const DevGrid<T> g, co
   }
 }
 
+// What the fit records per cell for the 3D face pass (cell_side): -1 when every face_area of the
+// cell's plane is 0, +1 when every one is the full face, 0 when they must be clipped. A valid plane
+// is classified by plane_side; an invalid one has face areas 0 (fraction < 1/2) or full (any other
+// fraction, NaN included), _face_area's rule for an invalid plane.
+template <class T>
+__device__ __forceinline__ int8_t cell_side(bool valid, const T n[3], T a, T frac) {
+  if (!valid) return frac < T(0.5) ? int8_t(-1) : int8_t(1);
+  return int8_t(plane_side<T>(n, a));
+}
+
 // The resolved faces in 3D, marching z: a CTA owns a column of FZ_X x FZ_Y cells and FZ_KZ slices.
-// Per slice it computes the next slice's one-sided fractions (area / full face, frac_of; whose
-// -z face is this slice's +z neighbour), this slice's x and y halo, then resolves the slice and
-// writes its rows; this slice's +z fractions are kept as the next slice's -z neighbours. So every
-// plane is read once (the column's first slice also reads the plane below it), with no z-halo,
-// in two barriers per slice, and each one-sided fraction is formed once rather than by both
-// cells of its face. The areas, fractions and resolve expression are plic_face_kernel's, so the
-// faces are the same bits.
+// Per slice it forms the next slice's one-sided fractions (area / full face, frac_of; whose -z face
+// is this slice's +z neighbour) and this slice's x and y halo, then resolves the slice and writes
+// its rows; this slice's +z fractions are kept as the next slice's -z neighbours. A cell's six
+// one-sided fractions come from its side byte alone (all 0 or all 1) unless the fit marked its
+// plane as crossing the cell, and only then is the plane read and clipped. Every side byte is read
+// once (the column's first slice also reads the one below it), in one barrier per slice, and each
+// one-sided fraction is formed once rather than by both cells of its face. The areas, fractions
+// and resolve expression are plic_face_kernel's, so the faces are the same bits.
 constexpr int FZ_X = 32, FZ_Y = 8, FZ_KZ = 32;
 
 template <class T, bool MX>
 __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGrid<T> g, const Cols cols,
                                                             const T* __restrict__ normals,
                                                             const T* __restrict__ intercepts,
-                                                            const uint8_t* __restrict__ valid) {
+                                                            const int8_t* __restrict__ sides) {
   constexpr int X = FZ_X, Y = FZ_Y, NF = 6;
   static_assert(X * Y == NT, "one cell of the slice per thread");
   // One-sided fractions of the slices k % 3, warp-blocked: row w (one warp) keeps its six faces
@@ -340,7 +351,6 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
   __shared__ T prev5[NT];                    // the slice below's +z fractions (own slot only)
   __shared__ T hx[2][2][Y], hy[2][2][X];     // the x and y halo of slices of each parity
   const long long n[3] = {g.n[0], g.n[1], g.n[2]};
-  const T* vf = static_cast<const T*>(cols.vf);
   T* ff = static_cast<T*>(cols.ff);
   const T cs[3] = {g.d[0], g.d[1], g.d[2]};
   const unsigned ntx = unsigned((n[0] + X - 1) / X), nty = unsigned((n[1] + Y - 1) / Y);
@@ -354,40 +364,26 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
   const int q = threadIdx.x, lx = q % X, ly = q / X;
   const long long ix = i0 + lx, jy = j0 + ly;
   const bool inxy = ix < n[0] && jy < n[1];
-  // the full area of a face of direction f, and the fraction m / full of an area m (frac_of)
+  // the full area of a face of direction f
   auto full_of = [&](int f) {
     const int c = f >> 1;
     return (T(1) * cs[c == 0 ? 1 : 0]) * cs[c == 2 ? 1 : 2];
   };
-  // One cell's stored plane. At Float32 it is loaded a slice before its fractions are formed, so the
-  // loads' latency hides behind the slice in between instead of sitting in front of the slice
-  // barrier (512^3, 64 spheres: 4.36 -> 4.29 ms); at Float64 the registers that takes cost more
-  // occupancy than it saves (6.22 -> 6.63 ms), so there it is loaded when used.
-  constexpr bool PREFETCH = sizeof(T) == 4;
-  struct Plane {
-    T n[3], a, fr;
-    bool ok;
+  // the clipped one-sided fraction of face f of cell ci, whose plane crosses it (side 0, so valid)
+  auto clip_frac = [&](const T nn[3], T a, int f) {
+    return frac_of(face_area<T, 3, MX>(nn, a, T(0), true, cs, f), full_of(f));
   };
-  auto load_plane = [&](long long ci) {
-    Plane p;
-    p.n[0] = normals[3 * ci]; p.n[1] = normals[3 * ci + 1]; p.n[2] = normals[3 * ci + 2];
-    p.a = intercepts[ci];
-    p.fr = vf[ci];
-    p.ok = valid[ci] != 0;
-    return p;
-  };
-  // a plane's one-sided fraction of face f; a plane that misses its cell gives every face 0 or 1
-  // without the clip (every area is then exactly 0 or the full face)
-  auto frac_from = [&](const Plane& p, int side, int f) {
-    if (side != 0) return side > 0 ? T(1) : T(0);
-    return frac_of(face_area<T, 3, MX>(p.n, p.a, p.fr, p.ok, cs, f), full_of(f));
-  };
-  auto side_of = [&](const Plane& p) { return p.ok ? plane_side<T>(p.n, p.a) : 0; };
-  auto own6 = [&](T (*buf)[NF][X], const Plane& p) {  // this thread's cell: six one-sided fractions
-    if (!inxy) return;
-    const int side = side_of(p);
+  auto own6 = [&](T (*buf)[NF][X], int side, long long ci) {  // this thread's cell: six one-sided fractions
+    if (side != 0) {
+      const T v = side > 0 ? T(1) : T(0);
 #pragma unroll
-    for (int f = 0; f < NF; ++f) buf[ly][f][lx] = frac_from(p, side, f);
+      for (int f = 0; f < NF; ++f) buf[ly][f][lx] = v;
+    } else {
+      const T nn[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
+      const T a = intercepts[ci];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) buf[ly][f][lx] = clip_frac(nn, a, f);
+    }
   };
   // The x and y halo of a slice: 2Y + 2X faces, one on every third thread (all eight warps share
   // them). Item h: the cell beyond the tile's -x / +x edge at row h (h < 2Y), or beyond its -y / +y
@@ -408,6 +404,18 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
     if (jj >= 0 && jj < n[1] && ii < n[0]) hcell = ii + n[0] * jj;
     hface = side == 0 ? 3 : 2;
   }
+  // a halo cell's face hface (one of the x and y directions), clipped with a constant direction
+  auto halo_frac = [&](int side, long long ci) -> T {
+    if (side != 0) return side > 0 ? T(1) : T(0);
+    const T nn[3] = {normals[3 * ci], normals[3 * ci + 1], normals[3 * ci + 2]};
+    const T a = intercepts[ci];
+    switch (hface) {
+      case 0: return clip_frac(nn, a, 0);
+      case 1: return clip_frac(nn, a, 1);
+      case 2: return clip_frac(nn, a, 2);
+      default: return clip_frac(nn, a, 3);
+    }
+  };
   const long long nxy = n[0] * n[1];
   const long long cxy = ix + n[0] * jy;
   // One barrier per slice. Slice k's fractions live in bufs[(k - k0) % 3]: the next slice's are
@@ -416,15 +424,22 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
   // parity on the same argument. The third buffer, free during slice k (it was slice k - 1's and
   // becomes slice k + 2's), takes each warp's resolved row in the warp's own block: only that
   // warp writes or reads its block until it fills it with slice k + 2's fractions itself, and it
-  // copies the row out in between.
-  Plane pnext{}, hnext{};
-  if (inxy) own6(bufs[0], load_plane(cxy + nxy * k0));
+  // copies the row out in between. Side bytes are read a slice ahead of their use.
+  if (inxy) own6(bufs[0], sides[cxy + nxy * k0], cxy + nxy * k0);
   if (inxy && k0 >= 1) {
-    const Plane pb = load_plane(cxy + nxy * (k0 - 1));
-    prev5[q] = frac_from(pb, side_of(pb), 5);
+    const long long cb = cxy + nxy * (k0 - 1);
+    const int sb = sides[cb];
+    T v;
+    if (sb != 0) {
+      v = sb > 0 ? T(1) : T(0);
+    } else {
+      const T nn[3] = {normals[3 * cb], normals[3 * cb + 1], normals[3 * cb + 2]};
+      v = clip_frac(nn, intercepts[cb], 5);
+    }
+    prev5[q] = v;
   }
-  if (PREFETCH && inxy && k0 + 1 < n[2]) pnext = load_plane(cxy + nxy * (k0 + 1));
-  if (PREFETCH && hcell >= 0) hnext = load_plane(hcell + nxy * k0);
+  int snext = (inxy && k0 + 1 < n[2]) ? sides[cxy + nxy * (k0 + 1)] : 0;
+  int hsnext = hcell >= 0 ? sides[hcell + nxy * k0] : 0;
   const int lane = q & 31, wrow = q >> 5;
   static_assert(X == 32, "a warp is one row of the slice");
   for (long long k = k0; k < k1; ++k) {
@@ -434,20 +449,12 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
     T* const res = &bufs[r3 == 0 ? 2 : r3 - 1][wrow][0][0];  // this warp's row, cell-major
     T (*hxp)[Y] = hx[par];
     T (*hyp)[X] = hy[par];
-    Plane pcur{}, hcur{};
-    if constexpr (PREFETCH) {
-      pcur = pnext;
-      hcur = hnext;
-      // the planes the next slice needs, loaded now
-      if (inxy && k + 2 < n[2]) pnext = load_plane(cxy + nxy * (k + 2));
-      if (hcell >= 0 && k + 1 < k1) hnext = load_plane(hcell + nxy * (k + 1));
-    } else {
-      if (inxy && k + 1 < n[2]) pcur = load_plane(cxy + nxy * (k + 1));
-      if (hcell >= 0) hcur = load_plane(hcell + nxy * k);
-    }
-    if (k + 1 < n[2]) own6(nxt, pcur);
+    const int scur = snext, hscur = hsnext;
+    if (inxy && k + 2 < n[2]) snext = sides[cxy + nxy * (k + 2)];
+    if (hcell >= 0 && k + 1 < k1) hsnext = sides[hcell + nxy * (k + 1)];
+    if (inxy && k + 1 < n[2]) own6(nxt, scur, cxy + nxy * (k + 1));
     if (hcell >= 0) {
-      const T v = frac_from(hcur, side_of(hcur), hface);
+      const T v = halo_frac(hscur, hcell + nxy * k);
       if (hitem < 2 * Y) hxp[hitem / Y][hitem % Y] = v;
       else hyp[(hitem - 2 * Y) / X][(hitem - 2 * Y) % X] = v;
     }
@@ -502,9 +509,12 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
 // strictly above the minimum over the box and keeps op order, so the planes are the same bits.
 constexpr int FIT_S = 4;
 
+// At Float32 a bound of 3 CTAs per SM lets the fit keep its values in registers (62, no spills;
+// 64-sphere cloud at 512^3: 3.64 -> 3.61 ms per update); Float64 keeps the compiler's own choice
+// (a bound of 1 CTA doubled its registers and cost 0.19 ms).
 template <class T, bool MX>
-__global__ void __launch_bounds__(NT) plic_fit_z_kernel(const DevGrid<T> g, const DevTape tape, const Cols cols,
-                                                        T* normals, T* intercepts, uint8_t* valid) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 0) plic_fit_z_kernel(const DevGrid<T> g, const DevTape tape, const Cols cols,
+                                                        T* normals, T* intercepts, uint8_t* valid, int8_t* sides) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_count;
   const STape<T> t = load_tape<T>(tape.bytes, tape.n_ops, tape.n_params, smem);
@@ -540,6 +550,7 @@ __global__ void __launch_bounds__(NT) plic_fit_z_kernel(const DevGrid<T> g, cons
       valid[ci] = pl.valid ? 1 : 0;
       vf[ci] = frac;
       cols.kind[ci] = frac == T(0) ? 0 : (frac == T(1) ? 1 : 2);
+      sides[ci] = cell_side<T>(pl.valid, pl.n, pl.a, frac);
     }
     __syncthreads();  // the next slab's pruning overwrites the ops this one read
   }
@@ -794,7 +805,8 @@ cudaError_t launch_monte_carlo(const DevTape& tape, const double lo[3], const do
 
 template <class T, int D>
 cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& cols, T* normals, T* intercepts,
-                        uint8_t* valid, cudaStream_t s, bool mixed) {
+                        uint8_t* valid, int8_t* sides, cudaStream_t s, bool mixed) {
+  if (D == 3 && !sides) return cudaErrorInvalidValue;
   const long long total = g.n[0] * g.n[1] * (D == 3 ? g.n[2] : 1);
   const int sm = CentroidSmem::of(tape).bytes;
   if (sm > 48 * 1024) {
@@ -814,16 +826,16 @@ cudaError_t launch_plic(const DevGrid<T>& g, const DevTape& tape, const Cols& co
   const long long zcols = ((g.n[0] + FZ_X - 1) / FZ_X) * ((g.n[1] + FZ_Y - 1) / FZ_Y) * ((g.n[2] + FZ_KZ - 1) / FZ_KZ);
   if (mixed && sizeof(T) == 4) {
     if constexpr (D == 3) {
-      plic_fit_z_kernel<T, true><<<unsigned(zcols), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
-      plic_face_z_kernel<T, true><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+      plic_fit_z_kernel<T, true><<<unsigned(zcols), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid, sides);
+      plic_face_z_kernel<T, true><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, sides);
     } else {
       plic_fit_kernel<T, D, true><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
       plic_face_kernel<T, D, true><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
     }
   } else {
     if constexpr (D == 3) {
-      plic_fit_z_kernel<T, false><<<unsigned(zcols), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
-      plic_face_z_kernel<T, false><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, valid);
+      plic_fit_z_kernel<T, false><<<unsigned(zcols), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid, sides);
+      plic_face_z_kernel<T, false><<<unsigned(zcols), NT, 0, s>>>(g, cols, normals, intercepts, sides);
     } else {
       plic_fit_kernel<T, D, false><<<blocks_for(total, 16), NT, sm, s>>>(g, tape, cols, normals, intercepts, valid);
       plic_face_kernel<T, D, false><<<blocks_for(total, 16), NT, 0, s>>>(g, cols, normals, intercepts, valid);
@@ -876,7 +888,7 @@ cudaError_t launch_report(long long ncell, const int8_t* kind, const uint8_t* am
 }
 
 #define INST(T, D)                                                                                      \
-  template cudaError_t launch_plic<T, D>(const DevGrid<T>&, const DevTape&, const Cols&, T*, T*, uint8_t*, \
+  template cudaError_t launch_plic<T, D>(const DevGrid<T>&, const DevTape&, const Cols&, T*, T*, uint8_t*, int8_t*, \
                                          cudaStream_t, bool);                                           \
   template cudaError_t launch_calc_volume<T, D>(const DevGrid<T>&, const DevTape&, double*, double*, cudaStream_t, \
                                                 bool);

@@ -66,6 +66,12 @@ def test_plic_bitwise(prec):
              (cc.CartesianGrid((-0.1, -0.05, 0.02), (37, 19, 45), (0.028,) * 3), cc.workloads.sphere_cloud(2, 16)),
              (cc.CartesianGrid((0.0, 0.0, 0.0), (33, 9, 70), (0.03,) * 3),
               cc.Sphere((0.5, 0.13, 1.05), 0.4)),
+             # a sphere centred on cell (8, 8, 8)'s centroid: that cell's gradient is 0 / 0, an
+             # invalid plane; the face pass takes its faces from the volume fraction
+             (cc.CartesianGrid((0.0, 0.0, 0.0), (16, 16, 16), (0.0625,) * 3),
+              cc.Sphere((0.53125, 0.53125, 0.53125), 0.3)),
+             # axis-aligned box faces: planes through cell faces, edges and corners
+             (cc.CartesianGrid((-1.0, -1.0, -1.0), (20, 20, 20), (0.1,) * 3), cc.Box((0.1, 0.0, 0.0), (0.5, 0.4, 0.3))),
              (cc.CartesianIsoGrid((-0.6, -0.6), (0.6, 0.6), 0.04),
               cc.SmoothUnion(cc.Circle((0.1, 0.0), 0.3), cc.Box((-0.2, 0.1), (0.15, 0.2)),
                              cc.Subtraction(cc.Circle((0.0, -0.2), 0.3), cc.Circle((0.0, -0.3), 0.1)), k=0.05))]
