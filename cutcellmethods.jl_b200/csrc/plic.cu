@@ -438,42 +438,54 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
     }
     prev5[q] = v;
   }
-  int snext = (inxy && k0 + 1 < n[2]) ? sides[cxy + nxy * (k0 + 1)] : 0;
-  int hsnext = hcell >= 0 ? sides[hcell + nxy * k0] : 0;
+  // Slice bookkeeping in 32-bit counters and running offsets: kk = k - k0, kn = n[2] - k0 slices
+  // to the grid's top; the offsets advance one slice (nxy cells) per step.
+  const int nk = int(k1 - k0), kn = int(n[2] - k0);
+  const bool x_lo = ix >= 1, x_hi = ix <= n[0] - 2, y_lo = jy >= 1, y_hi = jy <= n[1] - 2;
+  long long cn = cxy + nxy * (k0 + 1);  // the cell own6 builds next (slice k + 1)
+  long long hc = hcell + nxy * k0;      // this slice's halo cell
+  int snext = (inxy && kn > 1) ? sides[cn] : 0;
+  int hsnext = hcell >= 0 ? sides[hc] : 0;
   const int lane = q & 31, wrow = q >> 5;
   static_assert(X == 32, "a warp is one row of the slice");
-  for (long long k = k0; k < k1; ++k) {
-    const int r3 = int((k - k0) % 3), par = int((k - k0) & 1);
+  const int rowcells = (int)(n[0] - i0 < X ? n[0] - i0 : X);
+  T* frow = ff + NF * (i0 + n[0] * (jy + n[1] * k0));
+  const long long fstep = NF * nxy;
+  int r3 = 0;
+  for (int kk = 0; kk < nk; ++kk) {
+    const int par = kk & 1;
     T (*cur)[NF][X] = bufs[r3];
     T (*nxt)[NF][X] = bufs[r3 == 2 ? 0 : r3 + 1];
     T* const res = &bufs[r3 == 0 ? 2 : r3 - 1][wrow][0][0];  // this warp's row, cell-major
     T (*hxp)[Y] = hx[par];
     T (*hyp)[X] = hy[par];
     const int scur = snext, hscur = hsnext;
-    if (inxy && k + 2 < n[2]) snext = sides[cxy + nxy * (k + 2)];
-    if (hcell >= 0 && k + 1 < k1) hsnext = sides[hcell + nxy * (k + 1)];
-    if (inxy && k + 1 < n[2]) own6(nxt, scur, cxy + nxy * (k + 1));
+    if (inxy && kk + 2 < kn) snext = sides[cn + nxy];
+    if (hcell >= 0 && kk + 1 < nk) hsnext = sides[hc + nxy];
+    if (inxy && kk + 1 < kn) own6(nxt, scur, cn);
     if (hcell >= 0) {
-      const T v = halo_frac(hscur, hcell + nxy * k);
+      const T v = halo_frac(hscur, hc);
       if (hitem < 2 * Y) hxp[hitem / Y][hitem % Y] = v;
       else hyp[(hitem - 2 * Y) / X][(hitem - 2 * Y) % X] = v;
     }
+    cn += nxy;
+    hc += nxy;
     __syncthreads();
     if (inxy) {
-      const long long idx[3] = {ix, jy, k};
+      const bool lo[3] = {x_lo, y_lo, k0 + kk >= 1}, hi[3] = {x_hi, y_hi, kk + 1 < kn};
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
         const int c = f >> 1;
         const T mine = cur[ly][f][lx];
         T r;
         if ((f & 1) == 0) {
-          const bool has = idx[c] >= 1;
+          const bool has = lo[c];
           T below = T(0);
           if (has) below = c == 0 ? (lx > 0 ? cur[ly][1][lx - 1] : hxp[0][ly])
                                   : c == 1 ? (ly > 0 ? cur[ly - 1][3][lx] : hyp[0][lx]) : prev5[q];
           r = has ? (below + mine) * T(0.5) : mine;
         } else {
-          const bool has = idx[c] <= n[c] - 2;
+          const bool has = hi[c];
           T above = T(0);
           if (has) above = c == 0 ? (lx < X - 1 ? cur[ly][0][lx + 1] : hxp[1][ly])
                                   : c == 1 ? (ly < Y - 1 ? cur[ly + 1][2][lx] : hyp[1][lx]) : nxt[ly][4][lx];
@@ -484,30 +496,31 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
     }
     __syncwarp();
     // the warp's row leaves whole (16-byte vectors where the row is full and aligned)
-    const long long j = jy;
-    if (j < n[1]) {
-      const int rowcells = (int)(n[0] - i0 < X ? n[0] - i0 : X);
+    if (jy < n[1]) {
       constexpr int RV = X * NF * int(sizeof(T)) / 16;
-      const long long c0 = i0 + n[0] * (j + n[1] * k);
       const T* src = res;
-      if (rowcells == X && (reinterpret_cast<uintptr_t>(ff + NF * c0) & 15u) == 0) {
+      if (rowcells == X && (reinterpret_cast<uintptr_t>(frow) & 15u) == 0) {
         for (int v = lane; v < RV; v += 32)
-          reinterpret_cast<uint4*>(ff + NF * c0)[v] = reinterpret_cast<const uint4*>(src)[v];
+          reinterpret_cast<uint4*>(frow)[v] = reinterpret_cast<const uint4*>(src)[v];
       } else {
-        for (int e = lane; e < rowcells * NF; e += 32) ff[NF * c0 + e] = src[e];
+        for (int e = lane; e < rowcells * NF; e += 32) frow[e] = src[e];
       }
     }
+    frow += fstep;
     if (inxy) prev5[q] = cur[ly][5][lx];
     __syncwarp();  // every lane has copied the row out before any writes the next slice's fractions here
+    r3 = r3 == 2 ? 0 : r3 + 1;
   }
 }
 
 // The fit pass in 3D, marching z: a CTA owns a column of FZ_X x FZ_Y cells and FZ_KZ slices, and
 // prunes a union of spheres once per slab of FIT_S slices (the box of the slab's centroids)
-// instead of once per 256 cells: at 512^3 the 64-sphere union keeps 1.75 spheres per slab against
-// 1.62 per 32 x 4 x 2 tile, for a quarter of the bound work. The pruning drops only spheres
-// strictly above the minimum over the box and keeps op order, so the planes are the same bits.
-constexpr int FIT_S = 4;
+// instead of once per 256 cells. A deeper slab keeps a few more spheres per cell but bounds the
+// union less often; on the 64-sphere cloud (Float32 update, fit + faces) slabs of 4, 8, 16 and 32
+// slices took 3.55, 3.31, 3.27 and 3.50 ms at 512^3, and 8 was best at 256^3 (0.676 ms against
+// 0.696 for 16). The pruning drops only spheres strictly above the minimum over the box and keeps
+// op order, so the planes are the same bits.
+constexpr int FIT_S = 8;
 
 // At Float32 a bound of 3 CTAs per SM lets the fit keep its values in registers (62, no spills;
 // 64-sphere cloud at 512^3: 3.64 -> 3.61 ms per update); Float64 keeps the compiler's own choice
