@@ -748,13 +748,19 @@ def batch_block(args, dev, cc, k=256):
             b.add(c, t, g)
         cfg, tune_ms = b.autotune(reps=2)
         ms_graph = timed(lambda: b.run(sync=False), 5)
-        b.configure(use_graph=0)
+        # the tuned shape with band compaction switched the other way (off if tuned on, always on if off)
+        other_band = 0 if cfg["band_percent"] > 0 else 100
+        b.configure(band_percent=other_band)
+        ms_other_band = timed(lambda: b.run(sync=False), 5)
+        b.configure(band_percent=cfg["band_percent"], use_graph=0)
         ms_direct = timed(lambda: b.run(sync=False), 5)
         out[name] = {"updates": k, "cells": cells, "grids": "n x n, n ~ U{64..1024}, over [-1,1]^2",
                      "ms_per_update_launches": ms_single, "ms_batched_graph": ms_graph, "ms_batched_direct": ms_direct,
                      "speedup": ms_single / ms_graph, "cells_per_s_batched": cells / (ms_graph * 1e-3),
                      "roofline_frac": algo / (ms_graph * 1e-3) / 1e9 / measured_peak()[0],
-                     "algorithmic_bytes": algo, "autotuned": cfg}
+                     "algorithmic_bytes": algo, "autotuned": cfg,
+                     "band_compaction": {"tuned_percent": cfg["band_percent"], "other_percent": other_band,
+                                         "ms_batched_graph_other": ms_other_band}}
         del b, caches
         torch.cuda.empty_cache()
     tree, amp, ph = cc.star_curve_tree(0, 4, 12)

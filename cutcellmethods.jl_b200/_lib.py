@@ -19,7 +19,8 @@ CC_MARCHING_SQUARES, CC_MARCHING_CUBES, CC_PLIC = 0, 1, 2
 
 class BatchConfig(C.Structure):
     _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("threads", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("chunk", C.c_int32), ("use_graph", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("chunk", C.c_int32), ("use_graph", C.c_int32),
+                ("band_percent", C.c_int32)]
 
 
 class Grid(C.Structure):

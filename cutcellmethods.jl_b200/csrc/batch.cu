@@ -57,6 +57,7 @@ struct BatchArgs {
   unsigned long long* counter;
   long long total_tiles;
   int tape_smem;  // bytes reserved for one op-tape in shared memory
+  int band;       // band compaction: percent of a tile's cells (0 never, 100 always)
 };
 
 __device__ __forceinline__ int find_item(const BatchItem* items, int n, long long tile) {
@@ -69,11 +70,24 @@ __device__ __forceinline__ int find_item(const BatchItem* items, int n, long lon
   return lo;
 }
 
-template <class T, bool MX>
+// Whether a cell of corner values ph is cut: ms_cell's own test (not every corner on one side).
+template <class T>
+__device__ __forceinline__ bool ms_is_cut(const T* node, int nxn, int a, int b) {
+  const int nout = (node[a + nxn * b] >= T(0)) + (node[a + 1 + nxn * b] >= T(0)) +
+                   (node[a + 1 + nxn * (b + 1)] >= T(0)) + (node[a + nxn * (b + 1)] >= T(0));
+  return nout != 0 && nout != 4;
+}
+
+// BAND: the instantiation with band compaction (A.band > 0); without it the kernel carries none of
+// that code, so a batch that does not compact runs exactly as before the option existed.
+template <class T, bool MX, bool BAND>
 __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   T* node = reinterpret_cast<T*>(smem + A.tape_smem);
+  // band compaction: the tile's cut cells (a + tile_x * b), after the node values
+  uint16_t* band = reinterpret_cast<uint16_t*>(smem + A.tape_smem + ((A.tx + 1) * (A.ty + 1) * int(sizeof(T)) + 15) / 16 * 16);
   __shared__ long long s_first;
+  __shared__ int s_ncut, s_nlist;
   const int nt = blockDim.x;
   const int nxn = A.tx + 1, nyn = A.ty + 1;
   int cur = -1;
@@ -102,6 +116,10 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
         const unsigned ltu = unsigned(lt), row = ltu / unsigned(I.tiles_x);  // 32-bit: tiles of one grid
         const long long i0 = (long long)(ltu - row * unsigned(I.tiles_x)) * A.tx, j0 = (long long)row * A.ty;
         T* phi = static_cast<T*>(I.phi);
+        if (BAND && threadIdx.x == 0) {
+          s_ncut = 0;
+          s_nlist = 0;
+        }
         for (int v = threadIdx.x; v < nxn * nyn; v += nt) {
           const int a = v % nxn, b = v / nxn;
           const long long i = i0 + a, j = j0 + b;
@@ -125,13 +143,55 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
             ms_cell<T, MX>(nd, ph, cs, I.cols, i + n0 * j);
           }
         };
-        if (sizeof(T) == 4 && nt % A.tx == 0) {
-          // the block covers whole tile rows: a thread keeps its column and steps through rows
-          // (Float32 only: measured, the Float64 instantiation runs 6% slower this way)
-          const int a = threadIdx.x % A.tx, step = nt / A.tx;
-          for (int b = threadIdx.x / A.tx; b < A.ty; b += step) cell(a, b);
+        const bool rowwise = sizeof(T) == 4 && nt % A.tx == 0;
+        if constexpr (!BAND) {
+          if (rowwise) {
+            // the block covers whole tile rows: a thread keeps its column and steps through rows
+            // (Float32 only: measured, the Float64 instantiation runs 6% slower this way)
+            const int a = threadIdx.x % A.tx, step = nt / A.tx;
+            for (int b = threadIdx.x / A.tx; b < A.ty; b += step) cell(a, b);
+          } else {
+            for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) cell(c % A.tx, c / A.tx);
+          }
         } else {
-          for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) cell(c % A.tx, c / A.tx);
+          // Band compaction (A.band percent): when few enough of the tile's cells are cut, the
+          // threads fill the uncut cells and list the cut ones, then build the listed cells densely,
+          // so the long construction runs on full warps instead of on the few lanes whose cell
+          // happens to be cut. The same ms_cell runs for every cell either way: the same bits.
+          bool compact = A.band >= 100;
+          if (A.band < 100) {
+            int mine = 0;
+            if (rowwise) {
+              const int a = threadIdx.x % A.tx, step = nt / A.tx;
+              for (int b = threadIdx.x / A.tx; b < A.ty; b += step)
+                mine += (i0 + a < n0 && j0 + b < n1 && ms_is_cut(node, nxn, a, b)) ? 1 : 0;
+            } else {
+              for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) {
+                const int a = c % A.tx, b = c / A.tx;
+                mine += (i0 + a < n0 && j0 + b < n1 && ms_is_cut(node, nxn, a, b)) ? 1 : 0;
+              }
+            }
+            if (mine) atomicAdd(&s_ncut, mine);
+            __syncthreads();
+            compact = s_ncut * 100 <= A.band * A.tx * A.ty;
+          }
+          auto visit = [&](int a, int b) {
+            if (compact && i0 + a < n0 && j0 + b < n1 && ms_is_cut(node, nxn, a, b))
+              band[atomicAdd(&s_nlist, 1)] = uint16_t(a + A.tx * b);
+            else
+              cell(a, b);
+          };
+          if (rowwise) {
+            const int a = threadIdx.x % A.tx, step = nt / A.tx;
+            for (int b = threadIdx.x / A.tx; b < A.ty; b += step) visit(a, b);
+          } else {
+            for (int c = threadIdx.x; c < A.tx * A.ty; c += nt) visit(c % A.tx, c / A.tx);
+          }
+          if (compact) {
+            __syncthreads();
+            const int m = s_nlist;
+            for (int c = threadIdx.x; c < m; c += nt) cell(band[c] % A.tx, band[c] / A.tx);
+          }
         }
       } else {
         // one chunk of tree leaves, a leaf per thread (as ms_tree_kernel)
@@ -176,7 +236,7 @@ struct cc_batch {
   int device = 0;
   int prec = CC_F32;
   std::vector<HostItem> items;
-  cc_batch_config cfg{32, 8, 256, 4, 2, 1};
+  cc_batch_config cfg{32, 8, 256, 4, 2, 1, 0};
   bool layout_ok = false;  // device items and tapes match `items` and `cfg`
   bool graph_ok = false;   // `exec` replays the current layout
   BatchItem* items_dev = nullptr;
@@ -254,7 +314,9 @@ void drop_graph(cc_batch* b) {
 
 int tape_smem_of(const cc_batch* b) { return ((b->max_tape + 15) / 16) * 16; }
 int smem_of(const cc_batch* b) {
-  return tape_smem_of(b) + (b->cfg.tile_x + 1) * (b->cfg.tile_y + 1) * int(elem_size(b->prec));
+  const int nodes = (b->cfg.tile_x + 1) * (b->cfg.tile_y + 1) * int(elem_size(b->prec));
+  const int list = b->cfg.band_percent > 0 ? b->cfg.tile_x * b->cfg.tile_y * int(sizeof(uint16_t)) : 0;
+  return tape_smem_of(b) + (nodes + 15) / 16 * 16 + list;
 }
 
 // Pack every body into the staging buffer and lay the work list out for the current config.
@@ -367,23 +429,37 @@ cudaError_t issue(cc_batch* b, cudaStream_t s) {
   a.counter = b->counter;
   a.total_tiles = b->total_tiles;
   a.tape_smem = tape_smem_of(b);
+  a.band = b->cfg.band_percent;
   const int sm = smem_of(b);
   const int grid = 148 * b->cfg.ctas_per_sm;
   const int nt = b->cfg.threads;
-  if (b->prec == CC_F64) ms_batch_kernel<double, false><<<grid, nt, sm, s>>>(a);
-  else if (b->prec == CC_MIXED) ms_batch_kernel<float, true><<<grid, nt, sm, s>>>(a);
-  else ms_batch_kernel<float, false><<<grid, nt, sm, s>>>(a);
+  const bool bd = a.band > 0;
+  if (b->prec == CC_F64) {
+    if (bd) ms_batch_kernel<double, false, true><<<grid, nt, sm, s>>>(a);
+    else ms_batch_kernel<double, false, false><<<grid, nt, sm, s>>>(a);
+  } else if (b->prec == CC_MIXED) {
+    if (bd) ms_batch_kernel<float, true, true><<<grid, nt, sm, s>>>(a);
+    else ms_batch_kernel<float, true, false><<<grid, nt, sm, s>>>(a);
+  } else {
+    if (bd) ms_batch_kernel<float, false, true><<<grid, nt, sm, s>>>(a);
+    else ms_batch_kernel<float, false, false><<<grid, nt, sm, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
 // The kernel's dynamic shared-memory limit for the current layout (set outside any capture).
 cudaError_t prepare_kernel(const cc_batch* b) {
   const int sm = smem_of(b);
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  const bool bd = b->cfg.band_percent > 0;
   if (b->prec == CC_F64)
-    return cudaFuncSetAttribute(ms_batch_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return bd ? cudaFuncSetAttribute(ms_batch_kernel<double, false, true>, at, sm)
+              : cudaFuncSetAttribute(ms_batch_kernel<double, false, false>, at, sm);
   if (b->prec == CC_MIXED)
-    return cudaFuncSetAttribute(ms_batch_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  return cudaFuncSetAttribute(ms_batch_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return bd ? cudaFuncSetAttribute(ms_batch_kernel<float, true, true>, at, sm)
+              : cudaFuncSetAttribute(ms_batch_kernel<float, true, false>, at, sm);
+  return bd ? cudaFuncSetAttribute(ms_batch_kernel<float, false, true>, at, sm)
+            : cudaFuncSetAttribute(ms_batch_kernel<float, false, false>, at, sm);
 }
 
 cc_status check_config(const cc_batch_config* c) {
@@ -394,6 +470,7 @@ cc_status check_config(const cc_batch_config* c) {
     return fail(CC_BAD_ARG, "batch threads must be a multiple of 32 in 32..256");
   if (c->ctas_per_sm < 1 || c->ctas_per_sm > 32) return fail(CC_BAD_ARG, "batch ctas_per_sm must be 1..32");
   if (c->chunk < 1 || c->chunk > 1024) return fail(CC_BAD_ARG, "batch chunk must be 1..1024");
+  if (c->band_percent < 0 || c->band_percent > 100) return fail(CC_BAD_ARG, "batch band_percent must be 0..100");
   return CC_OK;
 }
 
@@ -585,6 +662,7 @@ cc_status cc_batch_autotune(cc_batch* b, int32_t reps, cc_batch_config* best, fl
   static const int threads[] = {128, 256};
   static const int ctas[] = {2, 4, 8};
   static const int chunks[] = {1, 4};
+  static const int bands[] = {0, 25, 100};
   const cudaStream_t user = static_cast<cudaStream_t>(stream);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
@@ -612,13 +690,15 @@ cc_status cc_batch_autotune(cc_batch* b, int32_t reps, cc_batch_config* best, fl
     for (int nt : threads) {
       for (int c : ctas) {
         for (int ch : chunks) {
-          if (st != CC_OK) break;
-          const cc_batch_config cand{tl[0], tl[1], nt, c, ch, use_graph};
-          float ms = 0.0f;
-          st = time_one(cand, &ms);
-          if (st == CC_OK && (top_ms < 0.0f || ms < top_ms)) {
-            top_ms = ms;
-            top = cand;
+          for (int bd : bands) {
+            if (st != CC_OK) break;
+            const cc_batch_config cand{tl[0], tl[1], nt, c, ch, use_graph, bd};
+            float ms = 0.0f;
+            st = time_one(cand, &ms);
+            if (st == CC_OK && (top_ms < 0.0f || ms < top_ms)) {
+              top_ms = ms;
+              top = cand;
+            }
           }
         }
       }

@@ -359,6 +359,9 @@ typedef struct {
   int32_t ctas_per_sm;    /* persistent CTAs per SM (148 SMs) */
   int32_t chunk;          /* tiles taken per atomic pop */
   int32_t use_graph;      /* replay a captured CUDA graph (1) or launch directly (0) */
+  int32_t band_percent;   /* band compaction, 0..100: a grid tile whose cut cells are at most this
+                           * percent of its cells fills its uncut cells first and then builds the
+                           * cut ones densely (0 never, 100 always); results are the same bits */
 } cc_batch_config;
 cc_status cc_batch_create(int32_t device, int32_t prec, cc_batch** out);
 cc_status cc_batch_destroy(cc_batch* b);
@@ -377,7 +380,8 @@ cc_status cc_batch_info(const cc_batch* b, int64_t* n_items, int64_t* total_tile
 /* Run every update, ordered after the work already on `stream` and before what follows it. */
 cc_status cc_batch_run(cc_batch* b, void* stream);
 /* Time every candidate launch shape (tiles 32x4..128x2, 128/256 threads, 2/4/8 CTAs per SM,
- * chunks 1/4) on the batch as it stands, `reps` timed runs each, and keep the fastest. */
+ * chunks 1/4, band compaction 0/25/100 percent) on the batch as it stands, `reps` timed runs
+ * each, and keep the fastest. */
 cc_status cc_batch_autotune(cc_batch* b, int32_t reps, cc_batch_config* best, float* best_ms, void* stream);
 
 /* ---- learned volume-fraction correction ----------------------------------------------------

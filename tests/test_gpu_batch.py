@@ -66,13 +66,19 @@ def test_batch_matches_single_updates(dtype, precision):
     assert_cells_bitwise(caches[-1].to_host(), ref)
 
 
-def test_launch_shapes_agree():
+@pytest.mark.parametrize("dtype,precision", [(torch.float32, "plain"), (torch.float64, "plain"),
+                                             (torch.float32, "mixed")])
+def test_launch_shapes_agree(dtype, precision):
     ups = updates()
-    _, ref = run_batch(ups, torch.float32, "plain")
-    for cfg in (dict(tile_x=16, tile_y=16, threads=128, ctas_per_sm=2, chunk=1, use_graph=0),
-                dict(tile_x=128, tile_y=2, threads=256, ctas_per_sm=8, chunk=4, use_graph=1),
-                dict(tile_x=5, tile_y=3, threads=32, ctas_per_sm=1, chunk=7, use_graph=1)):
-        _, got = run_batch(ups, torch.float32, "plain", **cfg)
+    _, ref = run_batch(ups, dtype, precision)
+    # band_percent: 0 builds every cell where it lies, 100 always lists a tile's cut cells and
+    # builds them densely, 30 decides per tile (some tiles of these bodies are mostly cut)
+    for cfg in (dict(tile_x=16, tile_y=16, threads=128, ctas_per_sm=2, chunk=1, use_graph=0, band_percent=0),
+                dict(tile_x=128, tile_y=2, threads=256, ctas_per_sm=8, chunk=4, use_graph=1, band_percent=100),
+                dict(tile_x=5, tile_y=3, threads=32, ctas_per_sm=1, chunk=7, use_graph=1, band_percent=30),
+                dict(tile_x=32, tile_y=8, threads=256, ctas_per_sm=4, chunk=2, use_graph=1, band_percent=100),
+                dict(tile_x=64, tile_y=64, threads=128, ctas_per_sm=2, chunk=1, use_graph=0, band_percent=30)):
+        _, got = run_batch(ups, dtype, precision, **cfg)
         for a, b in zip(got, ref):
             assert np.array_equal(bits(a.phi.cpu().numpy()), bits(b.phi.cpu().numpy()))
             assert_cells_bitwise(a.to_host(), b.to_host(), label=str(cfg))
