@@ -60,6 +60,7 @@ struct McArgs {
   int kz;  // z slices per pencil (pencil_slices)
   int tma_mask;  // bit c: column c leaves through TMA tensor stores (its map below is valid)
   int byte_words;  // kind/ambiguous rows start on 4-byte boundaries
+  int thread_cols;  // bit c: column c is copied element by element by the threads (no TMA, no words)
   // a union of spheres: each CTA's kept ops (stride tape.n_ops) and their count, or null
   const cc_op* pruned_ops;
   const int* pruned_count;
@@ -394,12 +395,14 @@ __global__ void __launch_bounds__(Tile<T>::NT, MB) mc_fill_kernel(const McArgs<T
               reinterpret_cast<const uint32_t*>(sbase + col_offset<T>(col) + r * col_bytes<T>(col))[w];
         }
       }
-      for (int r = 0; r < rows; ++r) {
+      // the rest element by element; most grids have none (every float column TMA-addressed and
+      // the byte columns copied as words), and the row loop is then skipped whole (200^3: 31.4 ->
+      // 18.3 warp instructions per cell, 0.383 -> 0.244 ms per update)
+      for (int r = 0; A.thread_cols && r < rows; ++r) {
         const long long rowc = row0 + (long long)r * n0;
 #pragma unroll
         for (int col = 0; col < 7; ++col) {
-          if (A.tma_mask & (1 << col)) continue;
-          if (col < 2 && A.byte_words) continue;  // done above
+          if (!(A.thread_cols & (1 << col))) continue;
           const int es = col_elem(col, int(sizeof(T)));
           const unsigned char* src = sbase + col_offset<T>(col) + r * col_bytes<T>(col);
           unsigned char* dst = gcol[col] + rowc * es;
@@ -660,6 +663,7 @@ cudaError_t launch_mc(const DevGrid<T>& g, const DevTape& tape, const T* phi_in,
   a.tma_mask = make_column_maps<T>(g, cols, &maps);
   a.byte_words = (g.n[0] % 4 == 0 && (reinterpret_cast<uintptr_t>(cols.kind) & 3u) == 0 &&
                   (reinterpret_cast<uintptr_t>(cols.amb) & 3u) == 0) ? 1 : 0;
+  a.thread_cols = ~a.tma_mask & 0x7f & ~(a.byte_words ? 3 : 0);
   a.n_itiles = int((g.n[0] + TL::TX - 1) / TL::TX);
   a.n_jtiles = int((g.n[1] + TL::TY - 1) / TL::TY);
   a.kz = pencil_slices(g.n[0], g.n[1], g.n[2], sizeof(T) == 8);
