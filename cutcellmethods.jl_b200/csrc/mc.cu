@@ -188,8 +188,8 @@ __device__ __forceinline__ void put_uncut_z(const Stage<float>& st, int lc, floa
   d4[1] = make_float4(hx, hz, hx, hz);
 }
 
-template <class T, bool SAMPLE, bool PRUNED, int MB = Tile<T>::MINB>
-__global__ void __launch_bounds__(Tile<T>::NT, MB) mc_fill_kernel(const McArgs<T> A,
+template <class T, bool SAMPLE, bool PRUNED>
+__global__ void __launch_bounds__(Tile<T>::NT, Tile<T>::MINB) mc_fill_kernel(const McArgs<T> A,
                                                                             const __grid_constant__ ColumnMaps maps) {
   using TL = Tile<T>;
   using L = Layout<T>;
@@ -621,23 +621,12 @@ size_t mc_prune_bytes(long long n0, long long n1, long long n2, int n_ops, bool 
 }
 
 namespace {
-// One fill launch. Float32 grids whose rows are not whole 32-byte sectors (x extent not a multiple
-// of 8 cells) run it at 4 CTAs per SM: neighbouring CTAs' boxes share partial sectors there, which
-// L2 merges, and the extra CTA hides that latency (260^3 0.774 -> 0.715 ms, 300^3 1.131 -> 1.057,
-// 500^3 4.63 -> 4.34). Grids of whole sectors are as fast or faster at 3 (200^3 0.385 against
-// 0.392 ms at 4; 512^3 2.66 against 2.79 with every column TMA-addressed).
+// One fill launch. (4 CTAs per SM at Float32 was measured too: faster only while grids whose x
+// extent is not a multiple of 16 still walked a per-row copy loop; without it 3 is faster at
+// every size: 500^3 2.85 against 3.18 ms, 260^3 0.468 against 0.496.)
 template <class T, bool SAMPLE, bool PRUNED>
 cudaError_t launch_fill(const McArgs<T>& a, const ColumnMaps& maps, unsigned blocks, int sm, cudaStream_t s) {
-  cudaError_t e;
-  if constexpr (sizeof(T) == 4) {
-    if ((a.g.n[0] * (long long)sizeof(T)) % 32 != 0) {
-      e = cudaFuncSetAttribute(mc_fill_kernel<T, SAMPLE, PRUNED, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-      if (e != cudaSuccess) return e;
-      mc_fill_kernel<T, SAMPLE, PRUNED, 4><<<blocks, Tile<T>::NT, sm, s>>>(a, maps);
-      return cudaSuccess;
-    }
-  }
-  e = cudaFuncSetAttribute(mc_fill_kernel<T, SAMPLE, PRUNED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaError_t e = cudaFuncSetAttribute(mc_fill_kernel<T, SAMPLE, PRUNED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e != cudaSuccess) return e;
   mc_fill_kernel<T, SAMPLE, PRUNED><<<blocks, Tile<T>::NT, sm, s>>>(a, maps);
   return cudaSuccess;
