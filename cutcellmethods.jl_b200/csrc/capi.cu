@@ -349,6 +349,7 @@ cc_status cc_handle_create(int32_t device, int32_t method, int32_t dim, int32_t 
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->tape_copied, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&h->vol_scratch, (2 * cci::calc_volume_blocks() + 2) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->rep_scratch, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(&h->rep_host, 8 * sizeof(unsigned long long));
 
   if (e == cudaSuccess && method == CC_MARCHING_CUBES) {
     const int64_t ncell = h->n[0] * h->n[1] * h->n[2];
@@ -374,6 +375,7 @@ cc_status cc_handle_destroy(cc_handle* h) {
   if (h->table_dev) cudaFree(h->table_dev);
   if (h->vol_scratch) cudaFree(h->vol_scratch);
   if (h->rep_scratch) cudaFree(h->rep_scratch);
+  if (h->rep_host) cudaFreeHost(h->rep_host);
   if (h->cut_list) cudaFree(h->cut_list);
   if (h->cut_count) cudaFree(h->cut_count);
   if (h->plic_sides) cudaFree(h->plic_sides);
@@ -618,17 +620,21 @@ cc_status cc_report(cc_handle* h, int64_t ncell, const int8_t* kind, const uint8
   if (ncell < 0) return fail(CC_BAD_ARG, "negative cell count");
   DeviceGuard dg(h->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
-  unsigned long long init[5] = {0, 0, 0, 0, 0};
-  const double one = 1.0;
-  std::memcpy(&init[4], &one, sizeof one);
-  cudaError_t e = cudaMemcpyAsync(h->rep_scratch, init, sizeof init, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && ncell > 0)
-    e = cci::launch_report(ncell, kind, ambiguous, volume_fraction, h->prec == CC_F64, h->rep_scratch,
-                           reinterpret_cast<double*>(h->rep_scratch + 4), s);
-  unsigned long long res[5];
-  if (e == cudaSuccess) e = cudaMemcpyAsync(res, h->rep_scratch, sizeof res, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  // four counters and the complement of the smallest fraction's bits (0: no cut fraction), zeroed
+  // on the device and read back through pinned memory
+  unsigned long long res[5] = {0, 0, 0, 0, 0};
+  cudaError_t e = cudaSuccess;
+  if (ncell > 0) {
+    e = cudaMemsetAsync(h->rep_scratch, 0, sizeof res, s);
+    if (e == cudaSuccess)
+      e = cci::launch_report(ncell, kind, ambiguous, volume_fraction, h->prec == CC_F64, h->rep_scratch,
+                             reinterpret_cast<double*>(h->rep_scratch + 4), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->rep_host, h->rep_scratch, sizeof res, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) std::memcpy(res, h->rep_host, sizeof res);
+  }
   if (e != cudaSuccess) return cuda_fail(e, "cc_report");
+  res[4] = res[4] == 0 ? 0x3FF0000000000000ull : ~res[4];  // no cut cell: 1.0
   counts[0] = ncell;
   counts[1] = (int64_t)res[0];
   counts[2] = (int64_t)res[1];

@@ -170,7 +170,8 @@ struct cc_handle {
   unsigned* cut_count = nullptr;
   int8_t* plic_sides = nullptr;  // 3D PLIC: the fit's per-cell side bytes for the face pass
   double* vol_scratch = nullptr;  // calc_volume partials + result
-  unsigned long long* rep_scratch = nullptr;  // report counters + min
+  unsigned long long* rep_scratch = nullptr;  // report counters + the complement of the min's bits
+  unsigned long long* rep_host = nullptr;     // pinned: the report's results read back
   unsigned* mesh_vbase = nullptr;  // generate_mesh: first vertex of each node's cut edges
   size_t mesh_vbase_n = 0;
   unsigned long long* mesh_scan = nullptr;  // generate_mesh: per-block counts and offsets

@@ -750,9 +750,10 @@ __global__ void __launch_bounds__(NT) report_kernel(long long ncell, const int8_
     atomicAdd(counts + 1, ins);
     atomicAdd(counts + 2, out);
     atomicAdd(counts + 3, am);
-    // non-negative floats order as their bit patterns
+    // non-negative floats order as their bit patterns; the slot keeps the complement's maximum, so
+    // it starts from 0 like the counters and the host zeroes all five with one memset
     const double dv = double(vmin);
-    atomicMin(vmin_bits, (unsigned long long)__double_as_longlong(dv));
+    atomicMax(vmin_bits, ~(unsigned long long)__double_as_longlong(dv));
   }
 }
 

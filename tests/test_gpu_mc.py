@@ -160,3 +160,9 @@ def test_report_on_arbitrary_columns(dtype):
         assert (rep["n"], rep["cut"], rep["inside"], rep["outside"], rep["ambiguous"]) == \
                (hr["n"], hr["cut"], hr["inside"], hr["outside"], hr["ambiguous"])
         assert rep["min_volume_fraction"] == float(hr["min_volume_fraction"])
+        # no cut cell with a positive fraction: the smallest fraction reported is 1, as on the host;
+        # the same handle reports twice in a row, so nothing carries over between calls
+        cache.cells.kind = torch.zeros_like(kb)
+        for _ in range(2):
+            rep = cc.cut_cell_report(cache)
+            assert (rep["cut"], rep["inside"], rep["min_volume_fraction"]) == (0, ncell, 1.0)
