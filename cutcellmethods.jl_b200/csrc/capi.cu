@@ -5,6 +5,8 @@
 // src/plic/surface.jl:41-45) and returns status codes the shims turn back into those exceptions.
 // The op-tape and tiling table are validated before they reach a kernel, so no device code ever
 // indexes outside them.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -201,6 +203,25 @@ int tape_prunable(const cc_optape* t) {
     if (i > 0 && t->ops[i].combine != mode) return 0;
   }
   return mode == CC_COMB_MIN ? 1 : 2;
+}
+
+// A deeper slab keeps a few more spheres per cell but bounds the union less often. On the 64-sphere
+// cloud (radii U[0.02, 0.08]) the Float32 update was fastest at 16 layers at 512^3 (3.27 ms; 8:
+// 3.31, 32: 3.50) and at 8 at 256^3 (0.676 ms; 16: 0.696, 4: 0.698): the same thickness in space,
+// about 0.6 of the median radius.
+int prune_slab(const cc_optape* t, double h) {
+  if (!t || t->n_ops < 1 || !(h > 0.0)) return 8;
+  std::vector<double> r;
+  for (int i = 0; i < t->n_ops; ++i)
+    if (t->ops[i].opcode == CC_OP_SPHERE && t->ops[i].poff + 3 < t->n_params)
+      r.push_back(std::fabs(t->params[t->ops[i].poff + 3]));  // a 3D sphere: centre, radius
+  if (r.empty()) return 8;
+  std::nth_element(r.begin(), r.begin() + r.size() / 2, r.end());
+  const double want = 0.6 * r[r.size() / 2] / h;
+  int best = 4;
+  for (int s = 8; s <= 32; s *= 2)
+    if (std::fabs(std::log2(want / s)) < std::fabs(std::log2(want / best))) best = s;
+  return best;
 }
 
 template size_t pack_tape<float>(const cc_optape*, int, unsigned char*, int*);
@@ -533,12 +554,14 @@ cc_status cc_plic_update(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   ++h->generation;
   if (h->prec == CC_F64) {
     if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
+    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     e = g->dim == 3 ? cci::launch_plic<double, 3>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
                                                   static_cast<double*>(intercepts), is_valid, h->plic_sides, s)
                     : cci::launch_plic<double, 2>(dev_grid<double>(g), tape, cols_of(cells), static_cast<double*>(normals),
                                                   static_cast<double*>(intercepts), is_valid, h->plic_sides, s);
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
+    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     const bool mx = h->prec == CC_MIXED;
     e = g->dim == 3 ? cci::launch_plic<float, 3>(dev_grid<float>(g), tape, cols_of(cells), static_cast<float*>(normals),
                                                  static_cast<float*>(intercepts), is_valid, h->plic_sides, s, mx)
@@ -566,6 +589,7 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   double pd;
   if (h->prec == CC_F64) {
     if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
+    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     const cci::DevGrid<double> dg2 = dev_grid<double>(g);
     e = g->dim == 3 ? cci::launch_calc_volume<double, 3>(dg2, tape, partial, res, s)
                     : cci::launch_calc_volume<double, 2>(dg2, tape, partial, res, s);
@@ -573,6 +597,7 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
     if (g->dim == 3) pd = pd * dg2.d[2];
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
+    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     const cci::DevGrid<float> dg2 = dev_grid<float>(g);
     const bool mx = h->prec == CC_MIXED;
     e = g->dim == 3 ? cci::launch_calc_volume<float, 3>(dg2, tape, partial, res, s, mx)

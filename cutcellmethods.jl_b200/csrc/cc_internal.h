@@ -41,7 +41,12 @@ struct DevTape {
   int n_params;
   int bytes_len;
   int prunable = 0;  // 1: a union (MIN) of spheres, 2: a smooth union (SMIN) of spheres; see prune_union
+  int slab = 8;      // the 3D PLIC passes' pruning slab in cell layers (prune_slab)
 };
+
+// The slab depth, in cell layers, over which the 3D PLIC fit and calc_volume prune a union of
+// spheres of cell size h: about 0.6 of the median radius, rounded to 4, 8, 16 or 32 layers.
+int prune_slab(const cc_optape* t, double h);
 
 struct Cols {
   int8_t* kind;

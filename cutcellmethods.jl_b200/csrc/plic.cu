@@ -514,13 +514,10 @@ __global__ void __launch_bounds__(NT, MX ? 4 : 5) plic_face_z_kernel(const DevGr
 }
 
 // The fit pass in 3D, marching z: a CTA owns a column of FZ_X x FZ_Y cells and FZ_KZ slices, and
-// prunes a union of spheres once per slab of FIT_S slices (the box of the slab's centroids)
-// instead of once per 256 cells. A deeper slab keeps a few more spheres per cell but bounds the
-// union less often; on the 64-sphere cloud (Float32 update, fit + faces) slabs of 4, 8, 16 and 32
-// slices took 3.55, 3.31, 3.27 and 3.50 ms at 512^3, and 8 was best at 256^3 (0.676 ms against
-// 0.696 for 16). The pruning drops only spheres strictly above the minimum over the box and keeps
-// op order, so the planes are the same bits.
-constexpr int FIT_S = 8;
+// prunes a union of spheres once per slab of tape.slab slices (the box of the slab's centroids;
+// the depth is chosen on the host from the spheres' radii, prune_slab) instead of once per 256
+// cells. The pruning drops only spheres strictly above the minimum over the box and keeps op
+// order, so the planes are the same bits whatever the depth.
 
 // At Float32 a bound of 3 CTAs per SM lets the fit keep its values in registers (62, no spills;
 // 64-sphere cloud at 512^3: 3.64 -> 3.61 ms per update); Float64 keeps the compiler's own choice
@@ -546,11 +543,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 0) plic_fit_z_kernel(
   const long long ix = i0 + q % X, jy = j0 + q / X;
   const bool inxy = ix < n[0] && jy < n[1];
   T* vf = static_cast<T*>(cols.vf);
-  for (long long ks = k0; ks < k1; ks += FIT_S) {
+  const int fit_s = tape.slab > 0 ? tape.slab : 8;
+  for (long long ks = k0; ks < k1; ks += fit_s) {
     const long long first[3] = {i0, j0, ks};
-    const int ext[3] = {X, Y, FIT_S};
+    const int ext[3] = {X, Y, fit_s};
     const STape<T> u = box_tape<T, 3>(t, tape, g, first, ext, smem, &s_count);
-    const long long ke = ks + FIT_S < k1 ? ks + FIT_S : k1;
+    const long long ke = ks + fit_s < k1 ? ks + fit_s : k1;
     for (long long k = ks; k < ke; ++k) {
       if (!inxy) continue;
       const long long idx[3] = {ix, jy, k};
@@ -615,7 +613,7 @@ __global__ void __launch_bounds__(NT) calc_volume_kernel(const DevGrid<T> g, con
 }
 
 // calc_volume in 3D, marching z: persistent CTAs take FZ_X x FZ_Y x FZ_KZ columns and prune a union
-// of spheres once per slab of FIT_S slices, as the 3D fit pass does (the same fractions; the sum
+// of spheres once per slab of tape.slab slices, as the 3D fit pass does (the same fractions; the sum
 // is the same compensated accumulation, in another order).
 template <class T, bool MX>
 __global__ void __launch_bounds__(NT) calc_volume_z_kernel(const DevGrid<T> g, const DevTape tape, double* partial) {
@@ -639,11 +637,12 @@ __global__ void __launch_bounds__(NT) calc_volume_z_kernel(const DevGrid<T> g, c
     const long long k1 = k0 + FZ_KZ < n[2] ? k0 + FZ_KZ : n[2];
     const long long ix = i0 + q % X, jy = j0 + q / X;
     const bool inxy = ix < n[0] && jy < n[1];
-    for (long long ks = k0; ks < k1; ks += FIT_S) {
+    const int fit_s = tape.slab > 0 ? tape.slab : 8;
+    for (long long ks = k0; ks < k1; ks += fit_s) {
       const long long first[3] = {i0, j0, ks};
-      const int ext[3] = {X, Y, FIT_S};
+      const int ext[3] = {X, Y, fit_s};
       const STape<T> u = box_tape<T, 3>(t, tape, g, first, ext, smem, &s_count);
-      const long long ke = ks + FIT_S < k1 ? ks + FIT_S : k1;
+      const long long ke = ks + fit_s < k1 ? ks + fit_s : k1;
       if (inxy)
         for (long long k = ks; k < ke; ++k) {
           const long long idx[3] = {ix, jy, k};
