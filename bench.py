@@ -544,13 +544,13 @@ def traffic_per_update(n):
 
 
 # Per-cell counts of the PLIC Float32 update (fit + face pass) on the 64-sphere union. Warp
-# instructions from one ncu capture at 512^3 (sm__inst_executed.sum, one pass: 1843.1 M + 1372.8 M
+# instructions from one ncu capture at 512^3 (sm__inst_executed.sum, one pass: 1812.4 M + 1372.8 M
 # over 134,217,728 cells). FP32 flops (FADD + FMUL + 2 FFMA thread instructions) from a capture at
 # 256^3 (3756 M + 266 M over 16,777,216 cells), scaled to 512^3 by the two sizes' ratio of
-# instructions per cell (23.96 / 30.38).
-PLIC_F32_WARP_INSTS_PER_CELL = (1843.09e6 + 1372.79e6) / 134217728
+# instructions per cell (23.73 / 30.37).
+PLIC_F32_WARP_INSTS_PER_CELL = (1812.37e6 + 1372.79e6) / 134217728
 PLIC_F32_FLOPS_PER_CELL = (((1307.33 + 475.00 + 2 * 986.78) + (109.12 + 105.61 + 2 * 25.52)) * 1e6 / 16777216
-                           * PLIC_F32_WARP_INSTS_PER_CELL / ((316.81e6 + 192.88e6) / 16777216))
+                           * PLIC_F32_WARP_INSTS_PER_CELL / ((316.58e6 + 192.88e6) / 16777216))
 B200_SMS, B200_MHZ = 148, 1965.0
 
 

@@ -582,6 +582,8 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   if (st != CC_OK) return st;
   DeviceGuard dg(h->device);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // calc_volume prunes over slabs of 8 layers whatever the body: deeper slabs, which the update's fit
+  // takes for small cells, made the Float64 sum slower (512^3 64-sphere cloud: 3.55 -> 6.37 ms at 16)
   cci::DevTape tape{nullptr, 0, 0, 0};
   double* partial = h->vol_scratch;
   double* res = h->vol_scratch + 2 * cci::calc_volume_blocks();
@@ -589,7 +591,6 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
   double pd;
   if (h->prec == CC_F64) {
     if ((st = upload_tape<double>(h, body, g->dim, s, &tape)) != CC_OK) return st;
-    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     const cci::DevGrid<double> dg2 = dev_grid<double>(g);
     e = g->dim == 3 ? cci::launch_calc_volume<double, 3>(dg2, tape, partial, res, s)
                     : cci::launch_calc_volume<double, 2>(dg2, tape, partial, res, s);
@@ -597,7 +598,6 @@ cc_status cc_calc_volume(cc_handle* h, const cc_grid* g, const cc_optape* body, 
     if (g->dim == 3) pd = pd * dg2.d[2];
   } else {
     if ((st = upload_tape<float>(h, body, g->dim, s, &tape)) != CC_OK) return st;
-    tape.slab = g->dim == 3 ? cci::prune_slab(body, g->d[0]) : 8;
     const cci::DevGrid<float> dg2 = dev_grid<float>(g);
     const bool mx = h->prec == CC_MIXED;
     e = g->dim == 3 ? cci::launch_calc_volume<float, 3>(dg2, tape, partial, res, s, mx)
