@@ -82,7 +82,7 @@ int mlp_nparam();
 template <class T>
 cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
                                   const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
-                                  unsigned long long* fallback, int* err, cudaStream_t s);
+                                  unsigned long long* fallback, int* err, cudaStream_t s, bool build);
 cudaError_t launch_mlp_grads(const float* P, const float* feats, const float* labels, const float* plain,
                              const float* weights, long long n, unsigned long long seed, int step, int tiles,
                              bool augment, float* grad, float* loss, int* err, cudaStream_t s);

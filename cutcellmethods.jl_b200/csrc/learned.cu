@@ -676,7 +676,10 @@ struct LearnedArgs {
   long long wait_limit;
 };
 
-template <class T>
+// BUILD: the kernel builds each listed cell's plain moments itself; without it the plain cut-band
+// kernel has already written them (mc_cut_kernel, the same construction at three times this
+// kernel's occupancy) and this kernel only reads the plain fraction back and corrects it.
+template <class T, bool BUILD>
 __global__ void __launch_bounds__(TILE) mc_cut_learned_kernel(const LearnedArgs<T> A) {
   extern __shared__ __align__(128) unsigned char smem[];
   const MlpShared s = mlp_shared(smem, false, A.wait_limit);
@@ -717,11 +720,14 @@ __global__ void __launch_bounds__(TILE) mc_cut_learned_kernel(const LearnedArgs<
       const long long bz = nx * ny;
       const T ph[8] = {A.phi[b0], A.phi[b0 + 1], A.phi[b0 + nx + 1], A.phi[b0 + nx],
                        A.phi[b0 + bz], A.phi[b0 + bz + 1], A.phi[b0 + bz + nx + 1], A.phi[b0 + bz + nx]};
-      const T org[3] = {node_coord(A.g.x0[0], A.g.d[0], i), node_coord(A.g.x0[1], A.g.d[1], j),
-                        node_coord(A.g.x0[2], A.g.d[2], k)};
-      const T l[3] = {node_coord(A.g.x0[0], A.g.d[0], i + 1) - org[0], node_coord(A.g.x0[1], A.g.d[1], j + 1) - org[1],
-                      node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
-      mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
+      if constexpr (BUILD) {
+        const T org[3] = {node_coord(A.g.x0[0], A.g.d[0], i), node_coord(A.g.x0[1], A.g.d[1], j),
+                          node_coord(A.g.x0[2], A.g.d[2], k)};
+        const T l[3] = {node_coord(A.g.x0[0], A.g.d[0], i + 1) - org[0],
+                        node_coord(A.g.x0[1], A.g.d[1], j + 1) - org[1],
+                        node_coord(A.g.x0[2], A.g.d[2], k + 1) - org[2]};
+        mc_cut_cell<T>(ph, l, org, cs, A.tb, st, ci);
+      }
       plain = st.vf[ci];
       float xr[8];
 #pragma unroll
@@ -843,20 +849,27 @@ int mlp_nparam() { return NPARAM; }
 template <class T>
 cudaError_t launch_mc_cut_learned(const DevGrid<T>& g, const T* phi, const Cols& cols, const DevTable& tb,
                                   const unsigned* cut_list, const unsigned* cut_count, const float* P, float bound,
-                                  unsigned long long* fallback, int* err, cudaStream_t s) {
+                                  unsigned long long* fallback, int* err, cudaStream_t s, bool build) {
   LearnedArgs<T> a{g, phi, cols, tb, cut_list, cut_count, P, bound, fallback, err, wait_limit()};
   const int sm = MlpLayout::INFER_SMEM;
-  cudaError_t e = cudaFuncSetAttribute(mc_cut_learned_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e != cudaSuccess) return e;
-  mc_cut_learned_kernel<T><<<148 * 3, TILE, sm, s>>>(a);
+  cudaError_t e;
+  if (build) {
+    e = cudaFuncSetAttribute(mc_cut_learned_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_cut_learned_kernel<T, true><<<148 * 3, TILE, sm, s>>>(a);
+  } else {
+    e = cudaFuncSetAttribute(mc_cut_learned_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    mc_cut_learned_kernel<T, false><<<148 * 3, TILE, sm, s>>>(a);
+  }
   return cudaGetLastError();
 }
 template cudaError_t launch_mc_cut_learned<float>(const DevGrid<float>&, const float*, const Cols&, const DevTable&,
                                                   const unsigned*, const unsigned*, const float*, float,
-                                                  unsigned long long*, int*, cudaStream_t);
+                                                  unsigned long long*, int*, cudaStream_t, bool);
 template cudaError_t launch_mc_cut_learned<double>(const DevGrid<double>&, const double*, const Cols&, const DevTable&,
                                                    const unsigned*, const unsigned*, const float*, float,
-                                                   unsigned long long*, int*, cudaStream_t);
+                                                   unsigned long long*, int*, cudaStream_t, bool);
 
 // One training step's gradients: per-CTA partials in grad[tiles][NPARAM], per-CTA squared-error
 // sums in loss[tiles].

@@ -292,7 +292,11 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
   ++h->generation;
   cudaError_t e = cudaMemsetAsync(m->fallback, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cc_mc_update_learned");
-  // the fill pass alone (cut band listed), then the fused cut + network pass
+  // The fill and the plain cut-band pass, then the network over the listed cells, reading their
+  // plain fractions back. (Building the cells inside the network kernel instead, one fused pass,
+  // runs the construction at a third of the plain kernel's occupancy: that kernel's 62 KB of
+  // shared memory allow 3 CTAs of 128 threads per SM.)
+  constexpr bool split = true;
   if (h->prec == CC_F64) {
     cci::DevTape tape{nullptr, 0, 0, 0};
     if ((st = cci::upload_body_f64(h, body, 3, s, &tape)) != CC_OK) return st;
@@ -300,10 +304,10 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, true) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<double>(dg2, tape, nullptr, static_cast<double*>(phi), cols_of(cells), h->tb, h->cut_list,
-                               h->cut_count, s, false, false, ps, ps ? pb : 0);
+                               h->cut_count, s, split, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<double>(dg2, static_cast<const double*>(phi), cols_of(cells), h->tb, h->cut_list,
-                                             h->cut_count, m->P, bound, m->fallback, m->err, s);
+                                             h->cut_count, m->P, bound, m->fallback, m->err, s, !split);
   } else {
     cci::DevTape tape{nullptr, 0, 0, 0};
     if ((st = cci::upload_body_f32(h, body, 3, s, &tape)) != CC_OK) return st;
@@ -311,10 +315,10 @@ cc_status cc_mc_update_learned(cc_handle* h, const cc_grid* g, const cc_optape* 
     const size_t pb = tape.prunable ? cci::mc_prune_bytes(g->n[0], g->n[1], g->n[2], tape.n_ops, false) : 0;
     void* ps = pb ? cci::prune_scratch(h, pb) : nullptr;
     e = cci::launch_mc<float>(dg2, tape, nullptr, static_cast<float*>(phi), cols_of(cells), h->tb, h->cut_list,
-                              h->cut_count, s, false, false, ps, ps ? pb : 0);
+                              h->cut_count, s, split, false, ps, ps ? pb : 0);
     if (e == cudaSuccess)
       e = cci::launch_mc_cut_learned<float>(dg2, static_cast<const float*>(phi), cols_of(cells), h->tb, h->cut_list,
-                                            h->cut_count, m->P, bound, m->fallback, m->err, s);
+                                            h->cut_count, m->P, bound, m->fallback, m->err, s, !split);
   }
   if (e != cudaSuccess) return cuda_fail(e, "cc_mc_update_learned");
   if (n_fallback) {
