@@ -32,6 +32,9 @@ namespace {
 
 using namespace ccd;
 using namespace ccms;
+
+// get_node's coordinate x0 + T(i) d from a 32-bit index: T(i) is the same value as from 64 bits.
+template <class T> __device__ __forceinline__ T node_coord_i(T x0, T d, int i) { return x0 + T(i) * d; }
 using cci::Cols;
 
 // One update as the kernel sees it.
@@ -111,10 +114,12 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
       const long long lt = tile - I.tile_begin;
       if (I.kind == 0) {
         // one grid tile: its nodes into shared memory (owned ones to phi), then its cells
-        const long long n0 = I.n0, n1 = I.n1;
+        // 32-bit node and cell coordinates (a batch grid has fewer than 2^31 cells per axis, checked
+        // when it is added); only the linear cell and node indices are 64-bit
+        const int n0 = int(I.n0), n1 = int(I.n1);
         const T gx0 = T(I.x0[0]), gy0 = T(I.x0[1]), dx = T(I.d[0]), dy = T(I.d[1]);
         const unsigned ltu = unsigned(lt), row = ltu / unsigned(I.tiles_x);  // 32-bit: tiles of one grid
-        const long long i0 = (long long)(ltu - row * unsigned(I.tiles_x)) * A.tx, j0 = (long long)row * A.ty;
+        const int i0 = int(ltu - row * unsigned(I.tiles_x)) * A.tx, j0 = int(row) * A.ty;
         T* phi = static_cast<T*>(I.phi);
         if (BAND && threadIdx.x == 0) {
           s_ncut = 0;
@@ -122,25 +127,25 @@ __global__ void __launch_bounds__(256) ms_batch_kernel(const BatchArgs A) {
         }
         for (int v = threadIdx.x; v < nxn * nyn; v += nt) {
           const int a = v % nxn, b = v / nxn;
-          const long long i = i0 + a, j = j0 + b;
+          const int i = i0 + a, j = j0 + b;
           if (i <= n0 && j <= n1) {
-            const T x[2] = {node_coord(gx0, dx, i), node_coord(gy0, dy, j)};
+            const T x[2] = {node_coord_i(gx0, dx, i), node_coord_i(gy0, dy, j)};
             const T val = tape_eval<T, 2, T>(tp, x);
             node[v] = val;
-            if ((a < A.tx || i == n0) && (b < A.ty || j == n1)) phi[i + (n0 + 1) * j] = val;
+            if ((a < A.tx || i == n0) && (b < A.ty || j == n1)) phi[(long long)i + (long long)(n0 + 1) * j] = val;
           }
         }
         __syncthreads();
         const T cs[2] = {dx, dy};
         auto cell = [&](int a, int b) {
-          const long long i = i0 + a, j = j0 + b;
+          const int i = i0 + a, j = j0 + b;
           if (i < n0 && j < n1) {
-            const T xa = node_coord(gx0, dx, i), xb = node_coord(gx0, dx, i + 1);
-            const T ya = node_coord(gy0, dy, j), yb = node_coord(gy0, dy, j + 1);
+            const T xa = node_coord_i(gx0, dx, i), xb = node_coord_i(gx0, dx, i + 1);
+            const T ya = node_coord_i(gy0, dy, j), yb = node_coord_i(gy0, dy, j + 1);
             const T nd[4][2] = {{xa, ya}, {xb, ya}, {xb, yb}, {xa, yb}};
             const T ph[4] = {node[a + nxn * b], node[a + 1 + nxn * b], node[a + 1 + nxn * (b + 1)],
                              node[a + nxn * (b + 1)]};
-            ms_cell<T, MX>(nd, ph, cs, I.cols, i + n0 * j);
+            ms_cell<T, MX>(nd, ph, cs, I.cols, (long long)i + (long long)n0 * j);
           }
         };
         const bool rowwise = sizeof(T) == 4 && nt % A.tx == 0;
@@ -545,6 +550,8 @@ cc_status cc_batch_add_ms_grid(cc_batch* b, const cc_grid* g, const cc_optape* b
   if (!b || !g || !phi || !cells_ok(cells)) return fail(CC_BAD_ARG, "null argument");
   if (g->dim != 2) return fail(CC_DIM_MISMATCH, "marching squares is 2D");
   if (g->n[0] < 1 || g->n[1] < 1) return fail(CC_BAD_ARG, "every axis needs at least one cell");
+  if (g->n[0] >= 0x7fffffffLL || g->n[1] >= 0x7fffffffLL)  // the kernel indexes an axis's nodes in 32 bits
+    return fail(CC_TOO_LARGE, "a batched grid has fewer than 2^31 - 1 cells per axis");
   cc_status st = cci::validate_body(body, 2);
   if (st != CC_OK) return st;
   HostItem it;
